@@ -1,0 +1,366 @@
+"""Benchmark of the CCSD(T) triples body on B200: one JSON line on rank 0.
+
+Default workload: the fused persistent FP64 kernel over every (i,j,k) triple of one `a` at
+nocc=40, nvir=300 (32,800 triples, 16.06 TFLOP per step), seeded synthetic inputs resident in HBM
+(1.52 GB > the 126 MB L2, so no L2 flush is needed between steps).
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+
+--impl b200 (default): `value` = triples/s of the fused kernel on device-resident inputs (CUDA events,
+  max over ranks); `e2e` = the same metric through the C ABI with host buffers (pinned host -> device
+  copy of every input tensor, execute, device -> host read of the energies inside the timed region);
+  `roofline` = FP64 tensor-pipe fraction of the fused kernel against the FP64 DMMA peak measured live
+  by the library's probe; `plain_gpu` = the plain per-triple GPU path (16 GEMMs + tengy per triple) on a
+  bounded sample; `cpu_baseline` = the reference's own CPU body (oracle/_ref, OpenBLAS) on a bounded
+  sample with all host threads (rank 0, N = 1 only).
+--impl reference: the reference's CPU path alone (oracle/_ref/libtrpdrv_ref.so: the reference
+  omp/ccsd_trpdrv_omp_cbody.c + omp/ccsd_tengy_c99.c compiled unmodified), each step a bounded sample of
+  the same workload's triples; rank 0 only.
+With torchrun (N > 1) the triples are split over ranks (strong scaling) and the two energies are summed
+with one NCCL all-reduce per step.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "nwchem-ccsd-trpdrv_b200"))
+
+METRIC = "(T) triples/s & FP64-equiv TFLOP/s, fused/emulated vs plain FP64 GPU"
+NOCC, NVIR, SEED = 40, 300, 2024
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--nocc", type=int, default=NOCC)
+    ap.add_argument("--nvir", type=int, default=NVIR)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-plain", action="store_true")
+    return ap.parse_args()
+
+
+def workload(nocc, nvir):
+    n = nocc * nocc * (nocc + 1) // 2
+    return {"workload": f"fused persistent FP64 triples body, nocc={nocc} nvir={nvir}, all {n} (i,j,k) triples of "
+                        f"one a per step", "nocc": nocc, "nvir": nvir, "triples_per_step": n,
+            "flop_per_triple": 16.0 * nvir * nvir * (nvir + nocc),
+            "l2": "inputs resident in HBM exceed the 126 MB L2; no flush between steps"}
+
+
+# ------------------------------------------------------------------------------------------------
+# CPU reference path (test infrastructure: oracle/_ref is the reference compiled unmodified)
+# ------------------------------------------------------------------------------------------------
+def time_reference_cpu(nocc, nvir, budget_s=12.0, max_triples=None):
+    """Times the reference body (omp/ccsd_trpdrv_omp_cbody.c + omp/ccsd_tengy_c99.c, unmodified, OpenBLAS)
+    over consecutive triples of the synthetic system, serially as omp/test.c calls it, each call using
+    every host thread (OpenMP + OpenBLAS).  Returns (triples/s, triples timed, seconds, threads)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import ctypes as C
+    import glob
+    import oracle as O
+    import trpdrv_b200 as T
+    ncpu = os.cpu_count() or 1
+    os.environ.setdefault("OMP_WAIT_POLICY", "passive")
+    R = O.ref()
+    for so in glob.glob(os.path.join(O._scipy_libs(), "libscipy_openblas-*.so")):
+        ob = C.CDLL(so)
+        ob.scipy_openblas_set_num_threads.argtypes = [C.c_int]
+        ob.scipy_openblas_set_num_threads(ncpu)
+    s = T.synth_system(nocc, nvir, seed=SEED)
+    O.run_system(s, "reference", t_begin=0, t_end=2, nthreads=1)  # warm-up (thread pools, pages)
+    n_all = nocc * nocc * (nocc + 1) // 2
+    done, t0, chunk = 0, time.perf_counter(), 8
+    while True:
+        hi = min(n_all, done + chunk)
+        O.run_system(s, "reference", t_begin=done, t_end=hi, nthreads=1)
+        done = hi
+        el = time.perf_counter() - t0
+        if done >= n_all or el >= budget_s or (max_triples and done >= max_triples):
+            break
+    del R
+    return done / el, done, el, ncpu
+
+
+def run_reference_arm(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    n_all = args.nocc * args.nocc * (args.nocc + 1) // 2
+    vals = []
+    per_step = None
+    for step in range(args.warmup + args.steps):
+        v, n, el, ncpu = time_reference_cpu(args.nocc, args.nvir, budget_s=8.0)
+        per_step = (n, el, ncpu)
+        if step >= args.warmup:
+            vals.append(v)
+    value = statistics.median(vals)
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "triples/s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * n_all / value,
+        "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded counter-based generator, reference config distributions)",
+        "config": workload(args.nocc, args.nvir),
+        "cpu_baseline": {"value": value, "unit": "triples/s", "cores": per_step[2], "kind": "reference",
+                         "sample": f"{per_step[0]} consecutive triples per step (of {n_all}), serial calls of the "
+                                   f"reference body with {per_step[2]} OpenMP + OpenBLAS threads, ~8 s per step; "
+                                   f"ms_per_step extrapolates to the full workload"},
+        "e2e": {"value": value, "unit": "triples/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "tflops_fp64_equiv": value * 16.0 * args.nvir ** 2 * (args.nvir + args.nocc) / 1e12,
+    }
+    print(json.dumps(line), flush=True)
+
+
+# ------------------------------------------------------------------------------------------------
+# B200 arm
+# ------------------------------------------------------------------------------------------------
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                                          "-lms", "200", "-i", str(self.device)], stdout=subprocess.PIPE,
+                                         stderr=subprocess.DEVNULL, text=True)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if not self.proc:
+            return None
+        self.proc.terminate()
+        try:
+            out, _ = self.proc.communicate(timeout=5)
+        except Exception:
+            self.proc.kill()
+            out, _ = self.proc.communicate()
+        rows = [[c.strip() for c in ln.split(",")] for ln in out.splitlines() if ln.count(",") >= 8]
+        if not rows:
+            return None
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        smax = max(float(r[2]) for r in rows if r[2].replace(".", "").isdigit())
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[q] for r in rows for q in range(4) if r[5 + q].lower() == "active"})
+        power = [float(r[3]) for r in rows if r[3].replace(".", "").isdigit()]
+        load = [v for v in sm if v > 0.5 * smax] or sm
+        return {"sm_mhz": statistics.median(load), "sm_max_mhz": smax, "reasons": reasons,
+                "samples": len(rows), "power_w_max": max(power) if power else None}
+
+
+def read_profile_traffic():
+    """DRAM bytes per fused launch from the committed ncu summary (profiles/), or None."""
+    path = os.path.join(ROOT, "profiles", "fused_nocc40_nvir300.md")
+    if not os.path.exists(path):
+        return None
+    for ln in open(path):
+        if ln.startswith("traffic_bytes_per_launch:"):
+            try:
+                return float(ln.split(":", 1)[1].split()[0])
+            except ValueError:
+                return None
+    return None
+
+
+def run_b200_arm(args):
+    import torch
+    import torch.distributed as dist
+    import trpdrv_b200 as T
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=torch.device("cuda", local))
+    dev = torch.device("cuda", local)
+    stream = torch.cuda.current_stream(dev)
+    sp = stream.cuda_stream
+
+    wl = workload(args.nocc, args.nvir)
+    n_all = wl["triples_per_step"]
+    flop_triple = wl["flop_per_triple"]
+
+    # inputs in pinned host memory (the e2e leg copies them every step)
+    pinned = []
+
+    def alloc(n):
+        t = torch.empty(n, dtype=torch.float64).pin_memory()
+        pinned.append(t)
+        return t.numpy()
+
+    s = T.synth_system(args.nocc, args.nvir, seed=SEED, alloc=alloc)
+    in_bytes = s.nbytes()
+
+    # FP64 peak of this device (library probe; best of the DMMA shapes) and cuBLAS DGEMM for context
+    probe = {k: T.probe_fp64_peak(k, local) for k in (1, 2, 3, 4)}
+    peak = max(probe[1], probe[2], probe[3])
+    a = torch.randn(8192, 8192, dtype=torch.float64, device=dev)
+    torch.matmul(a, a)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(3):
+        torch.matmul(a, a)
+    e1.record()
+    torch.cuda.synchronize()
+    cublas_dgemm = 3 * 2 * 8192 ** 3 / (e0.elapsed_time(e1) * 1e-3) / 1e12
+    del a
+
+    plan = T.Plan([s], mode=T.MODE_FUSED, rank=rank, world=world, device=local)
+    plan.upload(stream=sp)
+    my_triples = plan.num_triples(0)
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    def step():
+        plan.execute(stream=sp)
+        e4, e5 = plan.energies()
+        if world > 1:
+            t = torch.tensor([e4[0], e5[0]], dtype=torch.float64, device=dev)
+            dist.all_reduce(t)
+            return t
+        return None
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    barrier()
+    torch.cuda.synchronize()
+    clocks = ClockSampler(local)
+    clocks.start()
+    time.sleep(0.3)
+    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    kernel_ms, launches = [], 0
+    start.record(stream)
+    for _ in range(args.steps):
+        step()
+        kernel_ms.append(plan.last_kernel_ms())
+        launches += plan.last_launches()
+    end.record(stream)
+    torch.cuda.synchronize()
+    barrier()
+    torch.cuda.synchronize()
+    ck = clocks.stop()
+    elapsed = start.elapsed_time(end) * 1e-3
+    if world > 1:
+        t = torch.tensor([elapsed], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        elapsed = float(t.item())
+    value = n_all / (elapsed / args.steps)
+    e4, e5 = plan.energies()
+
+    # e2e through the C ABI with host buffers: H2D of every input + execute + D2H of the energies
+    e2e_times = []
+    for it in range(args.warmup + args.steps):
+        torch.cuda.synchronize()
+        barrier()
+        t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        t0.record(stream)
+        plan.upload(stream=sp)
+        step()
+        t1.record(stream)
+        torch.cuda.synchronize()
+        el = t0.elapsed_time(t1) * 1e-3
+        if world > 1:
+            tt = torch.tensor([el], dtype=torch.float64, device=dev)
+            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+            el = float(tt.item())
+        if it >= args.warmup:
+            e2e_times.append(el)
+    e2e_value = n_all / statistics.mean(e2e_times)
+    plan.close()
+
+    # plain per-triple GPU path on a bounded sample of the same workload (1/16 of the triples)
+    plain = None
+    if not args.no_plain and rank == 0:
+        with T.Plan([s], mode=T.MODE_PLAIN, rank=0, world=16, device=local) as pp:
+            pp.upload(stream=sp)
+            pp.execute(stream=sp)
+            pp.energies()
+            pe0, pe1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            pe0.record(stream)
+            pp.execute(stream=sp)
+            pe1.record(stream)
+            pp.energies()
+            pms = pe0.elapsed_time(pe1)
+            nplain = pp.num_triples(0)
+        plain = {"value": nplain / (pms * 1e-3), "unit": "triples/s", "sample": f"{nplain} triples (1/16 of the "
+                 f"workload, driver order), one grouped 16-GEMM launch + one tengy launch per triple",
+                 "tflops_fp64_equiv": nplain * flop_triple / (pms * 1e-3) / 1e12}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            v, n, el, ncpu = time_reference_cpu(args.nocc, args.nvir, budget_s=15.0)
+            cpu = {"value": v, "unit": "triples/s", "cores": ncpu, "kind": "reference",
+                   "sample": f"{n} consecutive triples of the same system, serial calls of the reference body "
+                             f"(oracle/_ref: omp/ccsd_trpdrv_omp_cbody.c + omp/ccsd_tengy_c99.c, OpenBLAS 0.3.30), "
+                             f"{ncpu} OpenMP + OpenBLAS threads, {el:.1f} s"}
+        except Exception as ex:  # the reference build is missing
+            cpu = {"value": None, "unit": "triples/s", "cores": os.cpu_count(), "kind": "reference",
+                   "sample": f"unavailable: {ex}"}
+
+    if rank != 0:
+        if world > 1:
+            dist.destroy_process_group()
+        return
+    kms = statistics.mean(kernel_ms)
+    achieved = my_triples * flop_triple / (kms * 1e-3) / 1e12
+    traffic = read_profile_traffic()
+    line = {
+        "metric": METRIC, "value": value, "unit": "triples/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": 1e3 * elapsed / args.steps, "higher_is_better": True,
+        "scaling": "strong", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded counter-based generator, reference config distributions)",
+        "config": dict(wl, parallelism=f"triples sharded over {world} rank(s), one 2-double all-reduce per step"),
+        "tflops_fp64_equiv": value * flop_triple / 1e12,
+        "emp4": e4[0], "emp5": e5[0],
+        "roofline": {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                     "frac": achieved / peak, "traffic": traffic,
+                     "peak_source": "measured live: library FP64 DMMA probe (best of m16n8k4/k8/k16, register "
+                                    "operands, 50 ms burst); MEASURED_PEAKS.json has no FP64 entry",
+                     "kernel_ms": kms},
+        "fp64_probe_tflops": {"dmma_m16n8k4": probe[1], "dmma_m16n8k8": probe[2], "dmma_m16n8k16": probe[3],
+                              "dfma": probe[4], "cublas_dgemm_8192": cublas_dgemm},
+        "e2e": {"value": e2e_value, "unit": "triples/s", "h2d_bytes_per_step": in_bytes,
+                "d2h_bytes_per_step": 16, "path": "trpdrv_plan_upload (pinned host) + trpdrv_plan_execute + "
+                                                  "trpdrv_plan_energies"},
+        "gpu_launches": launches,
+        "clocks": ck,
+        "plain_gpu": plain,
+        "speedup_vs_plain": (value / plain["value"]) if plain else None,
+        "cpu_baseline": cpu,
+    }
+    print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.destroy_process_group()
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference_arm(args)
+    else:
+        run_b200_arm(args)
+
+
+if __name__ == "__main__":
+    main()

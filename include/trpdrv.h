@@ -1,0 +1,251 @@
+/*
+ * trpdrv.h — C ABI of the B200 (sm_100a) CCSD(T) triples-driver library, libtrpdrv_b200.so.
+ *
+ * Part 1 exports the reference's own entry points with the reference's exact signatures, so the
+ * reference driver (omp/test.c) and Fortran/C callers link against this library unchanged.
+ * Part 2 is the batched interface: whole systems (every (i,j,k) triple of one `a`) resident on the
+ * device, run by one persistent fused kernel, by a plain per-triple path, or sharded over ranks.
+ *
+ * Conventions: all real data is IEEE double; integers are 32-bit unless typed otherwise; orbital
+ * indices in the reference entry points are 1-based (Fortran convention, as in the reference).
+ * Matrices are column-major: f(b,c) lives at f[b + c*nvir].  No function here takes or returns a
+ * framework type; streams are passed as `void *` holding a cudaStream_t (NULL = the library's own).
+ */
+#ifndef TRPDRV_B200_H
+#define TRPDRV_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ======================================================================================
+ * Part 1. Reference entry points (drop-in)
+ * ====================================================================================== */
+
+/* One triple (a,i,j,k): the 16 DGEMMs forming f1n..f4t, eaijk, the tengy reduction, and
+ * emp4 += emp4i (+ emp4k if i != k), emp5 likewise.
+ * Replaces ccsd_trpdrv_omp_cbody_ (omp/ccsd_trpdrv_omp_cbody.c:31-44; caller prototype
+ * omp/test.c:39-52).  All arguments by reference; every pointer is caller-owned HOST memory.
+ * tkj, jka, kka are offset by (k-klo)*nvir*nvir and tka, xka, jkj, kkj by (k-klo)*nocc*nvir, as in
+ * the reference.  f1n..f4t are scratch: they are written back only when TRPDRV_WRITE_F=1.
+ * Errors (bad sizes/indices, CUDA failure) print to stderr and abort, unless TRPDRV_ON_ERROR=return,
+ * in which case emp4/emp5 are left unchanged and trpdrv_last_error() reports the status. */
+void ccsd_trpdrv_omp_cbody_(double *f1n, double *f1t, double *f2n, double *f2t,
+                            double *f3n, double *f3t, double *f4n, double *f4t, double *eorb,
+                            int *ncor, int *nocc, int *nvir, double *emp4, double *emp5,
+                            int *a, int *i, int *j, int *k, int *klo,
+                            double *tij, double *tkj, double *tia, double *tka,
+                            double *xia, double *xka, double *jia, double *jka,
+                            double *kia, double *kka, double *jij, double *jkj,
+                            double *kij, double *kkj,
+                            double *dintc1, double *dintx1, double *t1v1,
+                            double *dintc2, double *dintx2, double *t1v2);
+
+/* Same contract; replaces the Fortran-77 body ccsd_trpdrv_omp_fbody (omp/ccsd_trpdrv_omp_f77.f:1-9),
+ * which omp/test.c calls under -DUSE_FORTRAN (omp/test.c:24-37, 167-171). */
+void ccsd_trpdrv_omp_fbody_(double *f1n, double *f1t, double *f2n, double *f2t,
+                            double *f3n, double *f3t, double *f4n, double *f4t, double *eorb,
+                            int *ncor, int *nocc, int *nvir, double *emp4, double *emp5,
+                            int *a, int *i, int *j, int *k, int *klo,
+                            double *tij, double *tkj, double *tia, double *tka,
+                            double *xia, double *xka, double *jia, double *jka,
+                            double *kia, double *kka, double *jij, double *jkj,
+                            double *kij, double *kkj,
+                            double *dintc1, double *dintx1, double *t1v1,
+                            double *dintc2, double *dintx2, double *t1v2);
+
+/* Same contract; replaces ccsd_trpdrv_cbody_ (ocl/ccsd_trpdrv_cbody.c:31; ocl/test.c:49-62). */
+void ccsd_trpdrv_cbody_(double *f1n, double *f1t, double *f2n, double *f2t,
+                        double *f3n, double *f3t, double *f4n, double *f4t, double *eorb,
+                        int *ncor, int *nocc, int *nvir, double *emp4, double *emp5,
+                        int *a, int *i, int *j, int *k, int *klo,
+                        double *tij, double *tkj, double *tia, double *tka,
+                        double *xia, double *xka, double *jia, double *jka,
+                        double *kia, double *kka, double *jij, double *jkj,
+                        double *kij, double *kkj,
+                        double *dintc1, double *dintx1, double *t1v1,
+                        double *dintc2, double *dintx2, double *t1v2);
+
+/* Same contract; replaces ccsd_trpdrv_opencl_ (ocl/ccsd_trpdrv_opencl.c:31; ocl/test.c:34-47).
+ * Unlike that reference body (whose tengy call is commented out, ocl/ccsd_trpdrv_opencl.c:128-131),
+ * this one computes the energies. */
+void ccsd_trpdrv_opencl_(double *f1n, double *f1t, double *f2n, double *f2t,
+                         double *f3n, double *f3t, double *f4n, double *f4t, double *eorb,
+                         int *ncor, int *nocc, int *nvir, double *emp4, double *emp5,
+                         int *a, int *i, int *j, int *k, int *klo,
+                         double *tij, double *tkj, double *tia, double *tka,
+                         double *xia, double *xka, double *jia, double *jka,
+                         double *kia, double *kka, double *jij, double *jkj,
+                         double *kij, double *kkj,
+                         double *dintc1, double *dintx1, double *t1v1,
+                         double *dintc2, double *dintx2, double *t1v2);
+
+/* The (b,c) energy reduction alone, on caller-provided host f arrays.  The four outputs are
+ * OVERWRITTEN (not accumulated).  Replaces ccsd_tengy_omp (omp/ccsd_tengy_c99.c:5-14): scalars
+ * by value, C argument order dintc1, dintx1, t1v1, dintc2, dintx2, t1v2. */
+void ccsd_tengy_omp(const double *f1n, const double *f1t, const double *f2n, const double *f2t,
+                    const double *f3n, const double *f3t, const double *f4n, const double *f4t,
+                    const double *dintc1, const double *dintx1, const double *t1v1,
+                    const double *dintc2, const double *dintx2, const double *t1v2,
+                    const double *eorb, const double eaijk,
+                    double *emp4i, double *emp5i, double *emp4k, double *emp5k,
+                    const int ncor, const int nocc, const int nvir);
+
+/* Same contract; replaces ccsd_tengy (ocl/ccsd_tengy.c:3-12). */
+void ccsd_tengy(const double *f1n, const double *f1t, const double *f2n, const double *f2t,
+                const double *f3n, const double *f3t, const double *f4n, const double *f4t,
+                const double *dintc1, const double *dintx1, const double *t1v1,
+                const double *dintc2, const double *dintx2, const double *t1v2,
+                const double *eorb, const double eaijk,
+                double *emp4i, double *emp5i, double *emp4k, double *emp5k,
+                const int ncor, const int nocc, const int nvir);
+
+/* Fortran binding of the same reduction; replaces the Fortran-77 ccsd_tengy_omp
+ * (omp/ccsd_tengy_f77.f:1-5): everything by reference, argument order
+ * dintc1, dintc2, dintx1, dintx2, t1v1, t1v2 (differs from the C order above). */
+void ccsd_tengy_omp_(const double *f1n, const double *f1t, const double *f2n, const double *f2t,
+                     const double *f3n, const double *f3t, const double *f4n, const double *f4t,
+                     const double *dintc1, const double *dintc2,
+                     const double *dintx1, const double *dintx2,
+                     const double *t1v1, const double *t1v2,
+                     const double *eorb, const double *eaijk,
+                     double *emp4i, double *emp5i, double *emp4k, double *emp5k,
+                     const int *ncor, const int *nocc, const int *nvir);
+
+/* ======================================================================================
+ * Part 2. Library interface (no reference counterpart unless stated)
+ * ====================================================================================== */
+
+/* Status codes. */
+enum {
+    TRPDRV_OK = 0,
+    TRPDRV_ERR_ARG = 1,          /* invalid argument (sizes, indices, NULL pointers) */
+    TRPDRV_ERR_CUDA = 2,         /* a CUDA runtime call failed */
+    TRPDRV_ERR_NOMEM = 3,        /* device or host allocation failed */
+    TRPDRV_ERR_NODEV = 4,        /* no usable sm_100 device */
+    TRPDRV_ERR_STATE = 5,        /* call out of order (e.g. execute before data is bound) */
+    TRPDRV_ERR_UNSUPPORTED = 6,  /* mode/shape not supported by the selected kernel */
+    TRPDRV_ERR_DEVICE = 7        /* a kernel reported an error through its status word */
+};
+
+int trpdrv_last_error(void);               /* status of the most recent failing call, this thread */
+const char *trpdrv_last_error_message(void);
+const char *trpdrv_status_string(int status);
+void trpdrv_clear_error(void);
+int trpdrv_version(void);                  /* major*10000 + minor*100 + patch */
+
+/* Execution modes. */
+enum {
+    TRPDRV_MODE_PLAIN = 0,  /* per triple: one grouped launch of the 16 FP64 GEMMs (f to HBM) + tengy */
+    TRPDRV_MODE_FUSED = 1   /* persistent kernel over (triple, tile-pair) work items; f stays on chip */
+};
+
+/* One system: all (i,j,k) triples of one fixed virtual `a`, every reference pointer a slice:
+ *   t2    [nocc j][nocc x][nvir][nvir]   tij = t2[j][i],  tkj = t2[j][k]
+ *   jvv   [nocc x][nvir][nvir]           jia = jvv[i],    jka = jvv[k]     (kvv likewise)
+ *   tov   [nocc x][nvir*nocc]            tia = tov[i],    tka = tov[k]     (xov likewise)
+ *   jov   [nocc j][nocc x][nocc*nvir]    jij = jov[j][i], jkj = jov[j][k]  (kov likewise)
+ *   dintc, dintx, t1v [nocc x][nvir]     dintc1 = dintc[i], dintc2 = dintc[k], ...
+ *   eorb  [ncor+nocc+nvir]
+ * `a` is the 1-based orbital index used for eaijk = eorb[a] - (eorb[ncor+i]+eorb[ncor+j]+eorb[ncor+k])
+ * (omp/ccsd_trpdrv_omp_cbody.c:126).  Pointers are host or device memory depending on the call. */
+typedef struct trpdrv_system {
+    int ncor, nocc, nvir, a;
+    const double *eorb;
+    const double *t2;
+    const double *jvv, *kvv;
+    const double *tov, *xov;
+    const double *jov, *kov;
+    const double *dintc, *dintx, *t1v;
+} trpdrv_system;
+
+typedef struct trpdrv_options {
+    int mode;         /* TRPDRV_MODE_*; default FUSED */
+    int nkpass;       /* triple order of the reference driver's k-chunking (omp/test.c:97); default 1 */
+    int rank, world;  /* process this rank's cost-balanced share of every system; default 0, 1 */
+    int device;       /* CUDA device ordinal; default -1 = current */
+    int tile;         /* fused tile width (32 is the only compiled width); 0 = default */
+    int ctas_per_sm;  /* fused persistent grid = ctas_per_sm * SM count; 0 = default */
+    int use_graph;    /* capture trpdrv_plan_execute's launch sequence in a CUDA graph; default 1 */
+    int reserved[8];
+} trpdrv_options;
+
+void trpdrv_options_default(trpdrv_options *opt);
+
+typedef struct trpdrv_plan trpdrv_plan;
+
+/* Allocates device storage and work queues for nsys systems (only ncor/nocc/nvir/a of `shape` are
+ * read).  Returns TRPDRV_OK and sets *plan. */
+int trpdrv_plan_create(trpdrv_plan **plan, const trpdrv_system *shape, int nsys,
+                       const trpdrv_options *opt);
+/* Copies every host tensor of `host` (nsys entries, same shapes) into the plan's device storage
+ * (host->device inside this call; pinned host memory makes it faster).  stream may be NULL. */
+int trpdrv_plan_upload(trpdrv_plan *plan, const trpdrv_system *host, void *stream);
+/* Uses caller-owned DEVICE tensors instead (no copy).  They must stay valid until the next
+ * upload/bind or destroy. */
+int trpdrv_plan_bind_device(trpdrv_plan *plan, const trpdrv_system *dev);
+/* Enqueues the whole job on `stream` (NULL = the plan's stream).  Asynchronous. */
+int trpdrv_plan_execute(trpdrv_plan *plan, void *stream);
+/* Waits for the job and returns this rank's per-system totals emp4[s], emp5[s] (compensated sums
+ * of emp4i + [i!=k] emp4k over the rank's triples).  Either output may be NULL. */
+int trpdrv_plan_energies(trpdrv_plan *plan, double *emp4, double *emp5);
+/* This rank's triples of system `sys`, in processing order: ijk[3*t..] = i, j, k (1-based). */
+int64_t trpdrv_plan_num_triples(const trpdrv_plan *plan, int sys);
+int trpdrv_plan_triples(const trpdrv_plan *plan, int sys, int32_t *ijk);
+/* Per-triple records of system `sys` after a job: rec[4*t..] = emp4i, emp5i, emp4k, emp5k. */
+int trpdrv_plan_triple_energies(trpdrv_plan *plan, int sys, double *rec);
+/* Kernel launches the last execute enqueued (for launch accounting). */
+int64_t trpdrv_plan_last_launches(const trpdrv_plan *plan);
+/* Device-time (ms) of the last execute's main kernel(s), measured with events on the plan stream. */
+int trpdrv_plan_last_kernel_ms(trpdrv_plan *plan, double *ms);
+int trpdrv_plan_destroy(trpdrv_plan *plan);
+
+/* One call from host tensors to totals: create, upload, execute, energies, destroy. */
+int trpdrv_run(const trpdrv_system *host, int nsys, const trpdrv_options *opt,
+               double *emp4, double *emp5);
+
+/* ---- host-side helpers (no device needed) ---- */
+
+/* Number of triples of the reference driver for one `a`: nocc*nocc*(nocc+1)/2 (omp/test.c:160-165). */
+int64_t trpdrv_count_triples(int nocc);
+/* The driver's triple order for a given nkpass (omp/test.c:97, 160-165): ijkl[4*t..] = i, j, k, klo. */
+int64_t trpdrv_enumerate_triples(int nocc, int nkpass, int32_t *ijkl);
+/* Splits n items with costs cost[] into `world` contiguous ranges of near-equal total cost:
+ * rank r gets [bounds[r], bounds[r+1]). */
+int trpdrv_partition(const double *cost, int64_t n, int world, int64_t *bounds);
+/* This rank's share of one system's triples, as plans assign them: the driver order for nkpass,
+ * split by trpdrv_partition into `world` contiguous ranges of equal count.  Writes ijk[3*t..] =
+ * i, j, k (1-based) when ijk is not NULL and returns the share's size (negative on bad arguments). */
+int64_t trpdrv_shard_triples(int nocc, int nkpass, int rank, int world, int32_t *ijk);
+/* Cost (FLOPs) of one triple of a system: 16*nvir*nvir*(nvir+nocc). */
+double trpdrv_triple_flops(int nocc, int nvir);
+
+/* Seeded synthetic inputs (counter-based, identical on every machine).  `tensor` selects which
+ * array of trpdrv_system to fill (TRPDRV_T_*); n must equal trpdrv_tensor_elems(tensor, ...).
+ * dist TRPDRV_DIST_UNIFORM: T2 in [-0.05,0.05]; tov, xov, t1v in [-0.02,0.02]; integrals
+ * (jvv, kvv, jov, kov, dintc, dintx) in [-0.1,0.1]; eorb: core sorted in [-20,-5], occupied sorted
+ * in [-2,-0.5], virtual sorted in [0.2,3].  TRPDRV_DIST_LOGUNIFORM: integrals instead have a
+ * log-uniform magnitude in [1e-6,1] with a random sign. */
+enum { TRPDRV_T_EORB = 0, TRPDRV_T_T2, TRPDRV_T_JVV, TRPDRV_T_KVV, TRPDRV_T_TOV, TRPDRV_T_XOV,
+       TRPDRV_T_JOV, TRPDRV_T_KOV, TRPDRV_T_DINTC, TRPDRV_T_DINTX, TRPDRV_T_T1V, TRPDRV_T_COUNT };
+enum { TRPDRV_DIST_UNIFORM = 0, TRPDRV_DIST_LOGUNIFORM = 1 };
+size_t trpdrv_tensor_elems(int tensor, int ncor, int nocc, int nvir);
+int trpdrv_synth_fill(int tensor, int ncor, int nocc, int nvir, uint64_t seed, int dist,
+                      double *out, size_t n);
+
+/* ---- device probes ---- */
+
+/* FP64 issue-rate microbenchmark on `device`: kind 0 = DMMA m8n8k4, 1 = m16n8k4, 2 = m16n8k8,
+ * 3 = m16n8k16, 4 = scalar DFMA.  Writes the achieved TFLOP/s. */
+int trpdrv_probe_fp64_peak(int device, int kind, double *tflops);
+
+/* Releases the drop-in entry points' device state (buffers, stream).  Safe to call repeatedly. */
+void trpdrv_finalize(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* TRPDRV_B200_H */

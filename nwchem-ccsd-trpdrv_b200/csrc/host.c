@@ -1,0 +1,1053 @@
+/*
+ * C host layer of libtrpdrv_b200.so: argument validation, device context, plans (device storage,
+ * work queues, CUDA-graph capture of the fused launch sequence), and the reference's drop-in entry
+ * points.  All device work is enqueued through the extern "C" launchers of launch.h.
+ */
+#include "trpdrv.h"
+#include "launch.h"
+
+#include <cuda_runtime_api.h>
+#include <pthread.h>
+#include <stdarg.h>
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+
+int trpdrv_fused_init(void);
+int trpdrv_plain_init(void);
+
+/* ------------------------------------------------------------------------------------------ */
+/* errors                                                                                       */
+/* ------------------------------------------------------------------------------------------ */
+
+static _Thread_local int t_status = TRPDRV_OK;
+static _Thread_local char t_message[512];
+
+static int fail(int status, const char *fmt, ...)
+{
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(t_message, sizeof t_message, fmt, ap);
+    va_end(ap);
+    t_status = status;
+    return status;
+}
+
+int trpdrv_last_error(void) { return t_status; }
+const char *trpdrv_last_error_message(void) { return t_message; }
+void trpdrv_clear_error(void)
+{
+    t_status = TRPDRV_OK;
+    t_message[0] = '\0';
+}
+
+const char *trpdrv_status_string(int status)
+{
+    switch (status) {
+    case TRPDRV_OK: return "ok";
+    case TRPDRV_ERR_ARG: return "invalid argument";
+    case TRPDRV_ERR_CUDA: return "CUDA runtime error";
+    case TRPDRV_ERR_NOMEM: return "out of memory";
+    case TRPDRV_ERR_NODEV: return "no usable sm_100 device";
+    case TRPDRV_ERR_STATE: return "call out of order";
+    case TRPDRV_ERR_UNSUPPORTED: return "unsupported";
+    case TRPDRV_ERR_DEVICE: return "device-side check failed";
+    default: return "unknown status";
+    }
+}
+
+#define CUDA_TRY(call)                                                                              \
+    do {                                                                                            \
+        cudaError_t e_ = (call);                                                                    \
+        if (e_ != cudaSuccess)                                                                      \
+            return fail(e_ == cudaErrorMemoryAllocation ? TRPDRV_ERR_NOMEM : TRPDRV_ERR_CUDA,       \
+                        "%s: %s (%s:%d)", #call, cudaGetErrorString(e_), __FILE__, __LINE__);       \
+    } while (0)
+
+#define LAUNCH_TRY(call)                                                                            \
+    do {                                                                                            \
+        int e_ = (call);                                                                            \
+        if (e_ != 0)                                                                                \
+            return fail(TRPDRV_ERR_CUDA, "%s: %s (%s:%d)", #call, cudaGetErrorString((cudaError_t)e_), \
+                        __FILE__, __LINE__);                                                        \
+    } while (0)
+
+#define TRY(call)                                                                                   \
+    do {                                                                                            \
+        int s_ = (call);                                                                            \
+        if (s_ != TRPDRV_OK) return s_;                                                             \
+    } while (0)
+
+/* ------------------------------------------------------------------------------------------ */
+/* device                                                                                       */
+/* ------------------------------------------------------------------------------------------ */
+
+#define TRPDRV_MAX_DEVICES 64
+static pthread_mutex_t g_init_mu = PTHREAD_MUTEX_INITIALIZER;
+static int g_init_done[TRPDRV_MAX_DEVICES];
+
+/* Selects `device` (-1 = current), checks that it is an sm_100 part, and sets the kernels'
+ * shared-memory limits once per device. */
+static int ensure_device(int device, int *out_dev, int *out_nsm)
+{
+    int count = 0;
+    cudaError_t e = cudaGetDeviceCount(&count);
+    if (e != cudaSuccess || count == 0)
+        return fail(TRPDRV_ERR_NODEV, "no CUDA device available (%s)", cudaGetErrorString(e));
+    int dev = device;
+    if (dev < 0) CUDA_TRY(cudaGetDevice(&dev));
+    if (dev >= count || dev >= TRPDRV_MAX_DEVICES) return fail(TRPDRV_ERR_ARG, "device %d out of range", dev);
+    CUDA_TRY(cudaSetDevice(dev));
+    int major = 0, minor = 0, nsm = 0;
+    CUDA_TRY(cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, dev));
+    CUDA_TRY(cudaDeviceGetAttribute(&minor, cudaDevAttrComputeCapabilityMinor, dev));
+    CUDA_TRY(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+    if (major != 10 || minor != 0)
+        return fail(TRPDRV_ERR_NODEV, "device %d is sm_%d%d; libtrpdrv_b200 is built for sm_100a only", dev,
+                    major, minor);
+    pthread_mutex_lock(&g_init_mu);
+    int rc = 0;
+    if (!g_init_done[dev]) {
+        rc = trpdrv_fused_init();
+        if (!rc) rc = trpdrv_plain_init();
+        if (!rc) g_init_done[dev] = 1;
+    }
+    pthread_mutex_unlock(&g_init_mu);
+    if (rc) return fail(TRPDRV_ERR_CUDA, "kernel attribute setup failed: %s", cudaGetErrorString((cudaError_t)rc));
+    if (out_dev) *out_dev = dev;
+    if (out_nsm) *out_nsm = nsm;
+    return TRPDRV_OK;
+}
+
+static int check_shape(const trpdrv_system *s, int idx)
+{
+    if (!s) return fail(TRPDRV_ERR_ARG, "system %d: NULL descriptor", idx);
+    if (s->nocc < 1 || s->nocc > TRPDRV_MAX_NOCC)
+        return fail(TRPDRV_ERR_ARG, "system %d: nocc=%d outside [1,%d]", idx, s->nocc, TRPDRV_MAX_NOCC);
+    if (s->nvir < 1 || s->nvir > TRPDRV_MAX_NVIR)
+        return fail(TRPDRV_ERR_ARG, "system %d: nvir=%d outside [1,%d]", idx, s->nvir, TRPDRV_MAX_NVIR);
+    if (s->ncor < 0) return fail(TRPDRV_ERR_ARG, "system %d: ncor=%d < 0", idx, s->ncor);
+    const int nbf = s->ncor + s->nocc + s->nvir;
+    if (s->a < 1 || s->a > nbf) return fail(TRPDRV_ERR_ARG, "system %d: a=%d outside [1,%d]", idx, s->a, nbf);
+    return TRPDRV_OK;
+}
+
+static const double *sys_tensor(const trpdrv_system *s, int w)
+{
+    switch (w) {
+    case TRPDRV_T_EORB: return s->eorb;
+    case TRPDRV_T_T2: return s->t2;
+    case TRPDRV_T_JVV: return s->jvv;
+    case TRPDRV_T_KVV: return s->kvv;
+    case TRPDRV_T_TOV: return s->tov;
+    case TRPDRV_T_XOV: return s->xov;
+    case TRPDRV_T_JOV: return s->jov;
+    case TRPDRV_T_KOV: return s->kov;
+    case TRPDRV_T_DINTC: return s->dintc;
+    case TRPDRV_T_DINTX: return s->dintx;
+    case TRPDRV_T_T1V: return s->t1v;
+    default: return NULL;
+    }
+}
+
+static int pack_triple(int i, int j, int k) { return (i - 1) | ((j - 1) << 10) | ((k - 1) << 20); }
+
+/* ------------------------------------------------------------------------------------------ */
+/* plans                                                                                        */
+/* ------------------------------------------------------------------------------------------ */
+
+typedef struct sysbuf {
+    trpdrv_system shape;
+    const double *t[TRPDRV_T_COUNT]; /* device tensors in use (owned or bound) */
+    double *own[TRPDRV_T_COUNT];     /* owned device copies made by upload */
+    double *ntov, *nxov;             /* -tov, -xov */
+    int32_t *d_triples, *h_triples;
+    int64_t ntriples;
+    double *partial, *rec;
+    int nb, npairs;
+} sysbuf;
+
+struct trpdrv_plan {
+    int nsys, device, nsm, grid, vec2, bound;
+    trpdrv_options opt;
+    cudaStream_t stream;
+    sysbuf *s;
+    trpdrv_dev_system *h_dev, *d_dev;
+    unsigned long long *d_counter;
+    int *d_status;
+    double *d_tot;
+    int64_t total_items;
+    double *d_f, *d_bpart;
+    unsigned *d_tcount;
+    cudaGraph_t graph;
+    cudaGraphExec_t gexec;
+    int graph_ready;
+    cudaEvent_t ev0, ev1;
+    int events_valid;
+    int64_t last_launches;
+    cudaStream_t last_stream;
+};
+
+void trpdrv_options_default(trpdrv_options *opt)
+{
+    if (!opt) return;
+    memset(opt, 0, sizeof *opt);
+    opt->mode = TRPDRV_MODE_FUSED;
+    opt->nkpass = 1;
+    opt->rank = 0;
+    opt->world = 1;
+    opt->device = -1;
+    opt->tile = 0;
+    opt->ctas_per_sm = 0;
+    opt->use_graph = 1;
+}
+
+static void plan_free(trpdrv_plan *p)
+{
+    if (!p) return;
+    if (p->gexec) cudaGraphExecDestroy(p->gexec);
+    if (p->graph) cudaGraphDestroy(p->graph);
+    if (p->s) {
+        for (int q = 0; q < p->nsys; ++q) {
+            sysbuf *b = &p->s[q];
+            for (int w = 0; w < TRPDRV_T_COUNT; ++w)
+                if (b->own[w]) cudaFree(b->own[w]);
+            if (b->ntov) cudaFree(b->ntov);
+            if (b->nxov) cudaFree(b->nxov);
+            if (b->d_triples) cudaFree(b->d_triples);
+            if (b->partial) cudaFree(b->partial);
+            if (b->rec) cudaFree(b->rec);
+            free(b->h_triples);
+        }
+        free(p->s);
+    }
+    free(p->h_dev);
+    if (p->d_dev) cudaFree(p->d_dev);
+    if (p->d_counter) cudaFree(p->d_counter);
+    if (p->d_status) cudaFree(p->d_status);
+    if (p->d_tot) cudaFree(p->d_tot);
+    if (p->d_f) cudaFree(p->d_f);
+    if (p->d_bpart) cudaFree(p->d_bpart);
+    if (p->d_tcount) cudaFree(p->d_tcount);
+    if (p->ev0) cudaEventDestroy(p->ev0);
+    if (p->ev1) cudaEventDestroy(p->ev1);
+    if (p->stream) cudaStreamDestroy(p->stream);
+    free(p);
+}
+
+static int plan_build(trpdrv_plan *p, const trpdrv_system *shape)
+{
+    const trpdrv_options *o = &p->opt;
+    CUDA_TRY(cudaStreamCreateWithFlags(&p->stream, cudaStreamNonBlocking));
+    CUDA_TRY(cudaEventCreate(&p->ev0));
+    CUDA_TRY(cudaEventCreate(&p->ev1));
+    p->s = (sysbuf *)calloc((size_t)p->nsys, sizeof(sysbuf));
+    p->h_dev = (trpdrv_dev_system *)calloc((size_t)p->nsys, sizeof(trpdrv_dev_system));
+    if (!p->s || !p->h_dev) return fail(TRPDRV_ERR_NOMEM, "host allocation failed");
+
+    int64_t item = 0;
+    int maxv = 0, maxpairs = 0;
+    int even = 1;
+    for (int q = 0; q < p->nsys; ++q) {
+        sysbuf *b = &p->s[q];
+        b->shape = shape[q];
+        const int nocc = shape[q].nocc, nvir = shape[q].nvir;
+        if ((nocc & 1) || (nvir & 1)) even = 0;
+        b->nb = (nvir + TRPDRV_TILE - 1) / TRPDRV_TILE;
+        b->npairs = b->nb * (b->nb + 1) / 2;
+        if (nvir > maxv) maxv = nvir;
+        if (b->npairs > maxpairs) maxpairs = b->npairs;
+
+        /* the reference driver's order, then this rank's contiguous share (uniform cost per system) */
+        const int64_t n = trpdrv_shard_triples(nocc, o->nkpass, o->rank, o->world, NULL);
+        if (n < 0) return fail(TRPDRV_ERR_ARG, "system %d: cannot shard triples", q);
+        b->ntriples = n;
+        int32_t *ijk = (int32_t *)malloc(sizeof(int32_t) * 3 * (size_t)(n > 0 ? n : 1));
+        b->h_triples = (int32_t *)malloc(sizeof(int32_t) * (size_t)(n > 0 ? n : 1));
+        if (!ijk || !b->h_triples) {
+            free(ijk);
+            return fail(TRPDRV_ERR_NOMEM, "host allocation failed");
+        }
+        trpdrv_shard_triples(nocc, o->nkpass, o->rank, o->world, ijk);
+        for (int64_t t = 0; t < n; ++t) b->h_triples[t] = pack_triple(ijk[3 * t], ijk[3 * t + 1], ijk[3 * t + 2]);
+        free(ijk);
+
+        if (b->ntriples > 0) {
+            CUDA_TRY(cudaMalloc((void **)&b->d_triples, sizeof(int32_t) * (size_t)b->ntriples));
+            CUDA_TRY(cudaMemcpy(b->d_triples, b->h_triples, sizeof(int32_t) * (size_t)b->ntriples,
+                                cudaMemcpyHostToDevice));
+            CUDA_TRY(cudaMalloc((void **)&b->rec, sizeof(double) * 4 * (size_t)b->ntriples));
+            CUDA_TRY(cudaMemset(b->rec, 0, sizeof(double) * 4 * (size_t)b->ntriples));
+            if (o->mode == TRPDRV_MODE_FUSED)
+                CUDA_TRY(cudaMalloc((void **)&b->partial, sizeof(double) * 4 * (size_t)b->ntriples * b->npairs));
+        }
+        const size_t ov = (size_t)nocc * nocc * nvir;
+        CUDA_TRY(cudaMalloc((void **)&b->ntov, sizeof(double) * ov));
+        CUDA_TRY(cudaMalloc((void **)&b->nxov, sizeof(double) * ov));
+
+        trpdrv_dev_system *d = &p->h_dev[q];
+        d->ncor = shape[q].ncor;
+        d->nocc = nocc;
+        d->nvir = nvir;
+        d->a = shape[q].a;
+        d->nb = b->nb;
+        d->npairs = b->npairs;
+        d->ntriples = b->ntriples;
+        d->item_begin = item;
+        d->triples = b->d_triples;
+        d->partial = b->partial;
+        d->rec = b->rec;
+        d->ntov = b->ntov;
+        d->nxov = b->nxov;
+        item += b->ntriples * b->npairs;
+    }
+    p->total_items = item;
+    p->vec2 = even;
+    CUDA_TRY(cudaMalloc((void **)&p->d_dev, sizeof(trpdrv_dev_system) * (size_t)p->nsys));
+    CUDA_TRY(cudaMalloc((void **)&p->d_counter, sizeof(unsigned long long)));
+    CUDA_TRY(cudaMalloc((void **)&p->d_status, sizeof(int)));
+    CUDA_TRY(cudaMemset(p->d_status, 0, sizeof(int)));
+    CUDA_TRY(cudaMalloc((void **)&p->d_tot, sizeof(double) * 4 * (size_t)p->nsys));
+    CUDA_TRY(cudaMemset(p->d_tot, 0, sizeof(double) * 4 * (size_t)p->nsys));
+    if (o->mode == TRPDRV_MODE_PLAIN) {
+        CUDA_TRY(cudaMalloc((void **)&p->d_f, sizeof(double) * 8 * (size_t)maxv * maxv));
+        CUDA_TRY(cudaMalloc((void **)&p->d_bpart, sizeof(double) * 4 * (size_t)maxpairs));
+        CUDA_TRY(cudaMalloc((void **)&p->d_tcount, sizeof(unsigned)));
+        CUDA_TRY(cudaMemset(p->d_tcount, 0, sizeof(unsigned)));
+    }
+
+    int per_sm = o->ctas_per_sm;
+    if (per_sm <= 0) {
+        int occ = 1;
+        if (trpdrv_fused_max_ctas_per_sm(&occ) != 0 || occ < 1) occ = 1;
+        per_sm = occ;
+    }
+    int64_t grid = (int64_t)per_sm * p->nsm;
+    if (grid > p->total_items) grid = p->total_items;
+    p->grid = (int)(grid > 0 ? grid : 0);
+    return TRPDRV_OK;
+}
+
+int trpdrv_plan_create(trpdrv_plan **plan, const trpdrv_system *shape, int nsys, const trpdrv_options *opt)
+{
+    if (!plan) return fail(TRPDRV_ERR_ARG, "plan output pointer is NULL");
+    *plan = NULL;
+    if (nsys < 1 || !shape) return fail(TRPDRV_ERR_ARG, "nsys=%d / shape=%p", nsys, (const void *)shape);
+    trpdrv_options o;
+    if (opt)
+        o = *opt;
+    else
+        trpdrv_options_default(&o);
+    if (o.mode != TRPDRV_MODE_PLAIN && o.mode != TRPDRV_MODE_FUSED)
+        return fail(TRPDRV_ERR_ARG, "unknown mode %d", o.mode);
+    if (o.world < 1 || o.rank < 0 || o.rank >= o.world)
+        return fail(TRPDRV_ERR_ARG, "rank %d / world %d", o.rank, o.world);
+    if (o.tile != 0 && o.tile != TRPDRV_TILE)
+        return fail(TRPDRV_ERR_UNSUPPORTED, "tile %d: only %d is compiled", o.tile, TRPDRV_TILE);
+    if (o.nkpass < 1) o.nkpass = 1;
+    for (int q = 0; q < nsys; ++q) TRY(check_shape(&shape[q], q));
+
+    int dev = 0, nsm = 0;
+    TRY(ensure_device(o.device, &dev, &nsm));
+    trpdrv_plan *p = (trpdrv_plan *)calloc(1, sizeof(trpdrv_plan));
+    if (!p) return fail(TRPDRV_ERR_NOMEM, "host allocation failed");
+    p->nsys = nsys;
+    p->opt = o;
+    p->device = dev;
+    p->nsm = nsm;
+    int rc = plan_build(p, shape);
+    if (rc != TRPDRV_OK) {
+        const int st = t_status;
+        char msg[sizeof t_message];
+        memcpy(msg, t_message, sizeof msg);
+        plan_free(p);
+        t_status = st;
+        memcpy(t_message, msg, sizeof msg);
+        return rc;
+    }
+    *plan = p;
+    return TRPDRV_OK;
+}
+
+static int plan_publish(trpdrv_plan *p)
+{
+    for (int q = 0; q < p->nsys; ++q) {
+        sysbuf *b = &p->s[q];
+        trpdrv_dev_system *d = &p->h_dev[q];
+        d->eorb = b->t[TRPDRV_T_EORB];
+        d->t2 = b->t[TRPDRV_T_T2];
+        d->jvv = b->t[TRPDRV_T_JVV];
+        d->kvv = b->t[TRPDRV_T_KVV];
+        d->jov = b->t[TRPDRV_T_JOV];
+        d->kov = b->t[TRPDRV_T_KOV];
+        d->dintc = b->t[TRPDRV_T_DINTC];
+        d->dintx = b->t[TRPDRV_T_DINTX];
+        d->t1v = b->t[TRPDRV_T_T1V];
+        const size_t ov = (size_t)b->shape.nocc * b->shape.nocc * b->shape.nvir;
+        LAUNCH_TRY(trpdrv_launch_negate(b->t[TRPDRV_T_TOV], b->ntov, ov, p->stream));
+        LAUNCH_TRY(trpdrv_launch_negate(b->t[TRPDRV_T_XOV], b->nxov, ov, p->stream));
+    }
+    CUDA_TRY(cudaMemcpyAsync(p->d_dev, p->h_dev, sizeof(trpdrv_dev_system) * (size_t)p->nsys,
+                             cudaMemcpyHostToDevice, p->stream));
+    CUDA_TRY(cudaStreamSynchronize(p->stream));
+    p->bound = 1;
+    return TRPDRV_OK;
+}
+
+int trpdrv_plan_upload(trpdrv_plan *p, const trpdrv_system *host, void *stream)
+{
+    if (!p || !host) return fail(TRPDRV_ERR_ARG, "NULL plan or systems");
+    CUDA_TRY(cudaSetDevice(p->device));
+    cudaStream_t st = stream ? (cudaStream_t)stream : p->stream;
+    for (int q = 0; q < p->nsys; ++q) {
+        sysbuf *b = &p->s[q];
+        const trpdrv_system *h = &host[q];
+        if (h->ncor != b->shape.ncor || h->nocc != b->shape.nocc || h->nvir != b->shape.nvir || h->a != b->shape.a)
+            return fail(TRPDRV_ERR_ARG, "system %d: shape differs from the plan's", q);
+        for (int w = 0; w < TRPDRV_T_COUNT; ++w) {
+            const double *src = sys_tensor(h, w);
+            if (!src) return fail(TRPDRV_ERR_ARG, "system %d: tensor %d is NULL", q, w);
+            const size_t n = trpdrv_tensor_elems(w, b->shape.ncor, b->shape.nocc, b->shape.nvir);
+            if (!b->own[w]) CUDA_TRY(cudaMalloc((void **)&b->own[w], sizeof(double) * n));
+            CUDA_TRY(cudaMemcpyAsync(b->own[w], src, sizeof(double) * n, cudaMemcpyHostToDevice, st));
+            b->t[w] = b->own[w];
+        }
+    }
+    if (st != p->stream) CUDA_TRY(cudaStreamSynchronize(st));
+    return plan_publish(p);
+}
+
+int trpdrv_plan_bind_device(trpdrv_plan *p, const trpdrv_system *dev)
+{
+    if (!p || !dev) return fail(TRPDRV_ERR_ARG, "NULL plan or systems");
+    CUDA_TRY(cudaSetDevice(p->device));
+    int aligned16 = 1;
+    for (int q = 0; q < p->nsys; ++q) {
+        sysbuf *b = &p->s[q];
+        const trpdrv_system *h = &dev[q];
+        if (h->ncor != b->shape.ncor || h->nocc != b->shape.nocc || h->nvir != b->shape.nvir || h->a != b->shape.a)
+            return fail(TRPDRV_ERR_ARG, "system %d: shape differs from the plan's", q);
+        for (int w = 0; w < TRPDRV_T_COUNT; ++w) {
+            const double *src = sys_tensor(h, w);
+            if (!src) return fail(TRPDRV_ERR_ARG, "system %d: tensor %d is NULL", q, w);
+            if (((uintptr_t)src) & 7u) return fail(TRPDRV_ERR_ARG, "system %d: tensor %d not 8-byte aligned", q, w);
+            if (((uintptr_t)src) & 15u) aligned16 = 0;
+            struct cudaPointerAttributes at;
+            if (cudaPointerGetAttributes(&at, src) != cudaSuccess ||
+                (at.type != cudaMemoryTypeDevice && at.type != cudaMemoryTypeManaged)) {
+                cudaGetLastError();
+                return fail(TRPDRV_ERR_ARG, "system %d: tensor %d is not device memory", q, w);
+            }
+            b->t[w] = src;
+        }
+    }
+    if (!aligned16) p->vec2 = 0;
+    return plan_publish(p);
+}
+
+static int enqueue_fused(trpdrv_plan *p, cudaStream_t st, int capturing)
+{
+    int64_t launches = 0;
+    CUDA_TRY(cudaMemsetAsync(p->d_counter, 0, sizeof(unsigned long long), st));
+    CUDA_TRY(cudaMemsetAsync(p->d_status, 0, sizeof(int), st));
+    CUDA_TRY(cudaMemsetAsync(p->d_tot, 0, sizeof(double) * 4 * (size_t)p->nsys, st));
+    CUDA_TRY(cudaEventRecordWithFlags(p->ev0, st, capturing ? cudaEventRecordExternal : cudaEventRecordDefault));
+    if (p->total_items > 0) {
+        LAUNCH_TRY(trpdrv_launch_fused(p->d_dev, p->nsys, p->total_items, p->d_counter, p->d_status, p->grid,
+                                       p->vec2, st));
+        ++launches;
+    }
+    CUDA_TRY(cudaEventRecordWithFlags(p->ev1, st, capturing ? cudaEventRecordExternal : cudaEventRecordDefault));
+    for (int q = 0; q < p->nsys; ++q) {
+        if (p->h_dev[q].ntriples <= 0) continue;
+        LAUNCH_TRY(trpdrv_launch_item_reduce(&p->h_dev[q], st));
+        LAUNCH_TRY(trpdrv_launch_system_reduce(p->s[q].rec, p->s[q].d_triples, p->s[q].ntriples, p->d_tot + 4 * q, st));
+        launches += 2;
+    }
+    p->last_launches = launches;
+    return TRPDRV_OK;
+}
+
+static int enqueue_plain(trpdrv_plan *p, cudaStream_t st)
+{
+    int64_t launches = 0;
+    CUDA_TRY(cudaMemsetAsync(p->d_tot, 0, sizeof(double) * 4 * (size_t)p->nsys, st));
+    CUDA_TRY(cudaEventRecord(p->ev0, st));
+    for (int q = 0; q < p->nsys; ++q) {
+        const sysbuf *b = &p->s[q];
+        const int O = b->shape.nocc, V = b->shape.nvir;
+        const size_t lnvv = (size_t)V * V, lnov = (size_t)O * V;
+        trpdrv_plain_args ga;
+        trpdrv_tengy_args ta;
+        memset(&ga, 0, sizeof ga);
+        memset(&ta, 0, sizeof ta);
+        ga.nocc = O;
+        ga.nvir = V;
+        ga.f = p->d_f;
+        ta.ncor = b->shape.ncor;
+        ta.nocc = O;
+        ta.nvir = V;
+        ta.use_eaijk = 0;
+        ta.a = b->shape.a;
+        ta.f = p->d_f;
+        ta.eorb = b->t[TRPDRV_T_EORB];
+        ta.block_partial = p->d_bpart;
+        ta.counter = p->d_tcount;
+        for (int64_t t = 0; t < b->ntriples; ++t) {
+            const int pk = b->h_triples[t];
+            const int i = pk & 1023, j = (pk >> 10) & 1023, k = (pk >> 20) & 1023; /* 0-based */
+            const size_t jo = (size_t)j * O;
+            const double *jia = b->t[TRPDRV_T_JVV] + i * lnvv, *kia = b->t[TRPDRV_T_KVV] + i * lnvv;
+            const double *jka = b->t[TRPDRV_T_JVV] + k * lnvv, *kka = b->t[TRPDRV_T_KVV] + k * lnvv;
+            const double *tij = b->t[TRPDRV_T_T2] + (jo + i) * lnvv, *tkj = b->t[TRPDRV_T_T2] + (jo + k) * lnvv;
+            const double *ntia = b->ntov + i * lnov, *nxia = b->nxov + i * lnov;
+            const double *ntka = b->ntov + k * lnov, *nxka = b->nxov + k * lnov;
+            const double *jij = b->t[TRPDRV_T_JOV] + (jo + i) * lnov, *kij = b->t[TRPDRV_T_KOV] + (jo + i) * lnov;
+            const double *jkj = b->t[TRPDRV_T_JOV] + (jo + k) * lnov, *kkj = b->t[TRPDRV_T_KOV] + (jo + k) * lnov;
+            /* f1n f2n f3n f4n f1t f2t f3t f4t: omp/ccsd_trpdrv_omp_cbody.c:70-117 */
+            const double *a1[8] = {jia, kia, jia, kia, jka, kka, jka, kka};
+            const double *b1[8] = {tkj, tkj, tkj, tkj, tij, tij, tij, tij};
+            const int nt[8] = {1, 1, 0, 0, 1, 1, 0, 0};
+            const double *a2[8] = {ntia, nxia, ntia, nxia, ntka, nxka, ntka, nxka};
+            const double *b2[8] = {kkj, kkj, jkj, jkj, kij, kij, jij, jij};
+            for (int x = 0; x < 8; ++x) {
+                ga.a1[x] = a1[x];
+                ga.b1[x] = b1[x];
+                ga.b1_nt[x] = nt[x];
+                ga.a2[x] = a2[x];
+                ga.b2[x] = b2[x];
+            }
+            LAUNCH_TRY(trpdrv_launch_plain_gemm(&ga, p->vec2, st));
+            ta.i = i + 1;
+            ta.j = j + 1;
+            ta.k = k + 1;
+            ta.dintc1 = b->t[TRPDRV_T_DINTC] + (size_t)i * V;
+            ta.dintx1 = b->t[TRPDRV_T_DINTX] + (size_t)i * V;
+            ta.t1v1 = b->t[TRPDRV_T_T1V] + (size_t)i * V;
+            ta.dintc2 = b->t[TRPDRV_T_DINTC] + (size_t)k * V;
+            ta.dintx2 = b->t[TRPDRV_T_DINTX] + (size_t)k * V;
+            ta.t1v2 = b->t[TRPDRV_T_T1V] + (size_t)k * V;
+            ta.out4 = b->rec + 4 * t;
+            LAUNCH_TRY(trpdrv_launch_tengy(&ta, st));
+            launches += 2;
+        }
+    }
+    CUDA_TRY(cudaEventRecord(p->ev1, st));
+    for (int q = 0; q < p->nsys; ++q) {
+        if (p->s[q].ntriples <= 0) continue;
+        LAUNCH_TRY(trpdrv_launch_system_reduce(p->s[q].rec, p->s[q].d_triples, p->s[q].ntriples, p->d_tot + 4 * q, st));
+        ++launches;
+    }
+    p->last_launches = launches;
+    return TRPDRV_OK;
+}
+
+int trpdrv_plan_execute(trpdrv_plan *p, void *stream)
+{
+    if (!p) return fail(TRPDRV_ERR_ARG, "NULL plan");
+    if (!p->bound) return fail(TRPDRV_ERR_STATE, "execute before upload/bind");
+    CUDA_TRY(cudaSetDevice(p->device));
+    cudaStream_t st = stream ? (cudaStream_t)stream : p->stream;
+    p->last_stream = st;
+    p->events_valid = 0;
+    if (p->opt.mode == TRPDRV_MODE_PLAIN) {
+        TRY(enqueue_plain(p, st));
+    } else if (p->opt.use_graph) {
+        if (!p->graph_ready) {
+            CUDA_TRY(cudaStreamBeginCapture(p->stream, cudaStreamCaptureModeThreadLocal));
+            const int rc = enqueue_fused(p, p->stream, 1);
+            cudaGraph_t g = NULL;
+            const cudaError_t ce = cudaStreamEndCapture(p->stream, &g);
+            if (rc != TRPDRV_OK) {
+                if (g) cudaGraphDestroy(g);
+                return rc;
+            }
+            CUDA_TRY(ce);
+            p->graph = g;
+            CUDA_TRY(cudaGraphInstantiate(&p->gexec, p->graph, 0));
+            p->graph_ready = 1;
+        }
+        CUDA_TRY(cudaGraphLaunch(p->gexec, st));
+    } else {
+        TRY(enqueue_fused(p, st, 0));
+    }
+    p->events_valid = 1;
+    return TRPDRV_OK;
+}
+
+static int plan_wait(trpdrv_plan *p)
+{
+    CUDA_TRY(cudaSetDevice(p->device));
+    CUDA_TRY(cudaStreamSynchronize(p->last_stream ? p->last_stream : p->stream));
+    int status = 0;
+    CUDA_TRY(cudaMemcpy(&status, p->d_status, sizeof(int), cudaMemcpyDeviceToHost));
+    if (status) return fail(TRPDRV_ERR_DEVICE, "the fused kernel rejected a malformed work-queue entry");
+    return TRPDRV_OK;
+}
+
+int trpdrv_plan_energies(trpdrv_plan *p, double *emp4, double *emp5)
+{
+    if (!p) return fail(TRPDRV_ERR_ARG, "NULL plan");
+    TRY(plan_wait(p));
+    double *tot = (double *)malloc(sizeof(double) * 4 * (size_t)p->nsys);
+    if (!tot) return fail(TRPDRV_ERR_NOMEM, "host allocation failed");
+    cudaError_t e = cudaMemcpy(tot, p->d_tot, sizeof(double) * 4 * (size_t)p->nsys, cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) {
+        free(tot);
+        return fail(TRPDRV_ERR_CUDA, "energy copy: %s", cudaGetErrorString(e));
+    }
+    for (int q = 0; q < p->nsys; ++q) {
+        if (emp4) emp4[q] = tot[4 * q + 0] + tot[4 * q + 1];
+        if (emp5) emp5[q] = tot[4 * q + 2] + tot[4 * q + 3];
+    }
+    free(tot);
+    return TRPDRV_OK;
+}
+
+int64_t trpdrv_plan_num_triples(const trpdrv_plan *p, int sys)
+{
+    if (!p || sys < 0 || sys >= p->nsys) return -1;
+    return p->s[sys].ntriples;
+}
+
+int trpdrv_plan_triples(const trpdrv_plan *p, int sys, int32_t *ijk)
+{
+    if (!p || sys < 0 || sys >= p->nsys || !ijk) return fail(TRPDRV_ERR_ARG, "bad plan/sys/output");
+    const sysbuf *b = &p->s[sys];
+    for (int64_t t = 0; t < b->ntriples; ++t) {
+        const int pk = b->h_triples[t];
+        ijk[3 * t + 0] = (pk & 1023) + 1;
+        ijk[3 * t + 1] = ((pk >> 10) & 1023) + 1;
+        ijk[3 * t + 2] = ((pk >> 20) & 1023) + 1;
+    }
+    return TRPDRV_OK;
+}
+
+int trpdrv_plan_triple_energies(trpdrv_plan *p, int sys, double *rec)
+{
+    if (!p || sys < 0 || sys >= p->nsys || !rec) return fail(TRPDRV_ERR_ARG, "bad plan/sys/output");
+    TRY(plan_wait(p));
+    const sysbuf *b = &p->s[sys];
+    if (b->ntriples > 0)
+        CUDA_TRY(cudaMemcpy(rec, b->rec, sizeof(double) * 4 * (size_t)b->ntriples, cudaMemcpyDeviceToHost));
+    return TRPDRV_OK;
+}
+
+int64_t trpdrv_plan_last_launches(const trpdrv_plan *p) { return p ? p->last_launches : -1; }
+
+int trpdrv_plan_last_kernel_ms(trpdrv_plan *p, double *ms)
+{
+    if (!p || !ms) return fail(TRPDRV_ERR_ARG, "NULL plan/output");
+    if (!p->events_valid) return fail(TRPDRV_ERR_STATE, "no execute to time");
+    TRY(plan_wait(p));
+    float f = 0.0f;
+    CUDA_TRY(cudaEventElapsedTime(&f, p->ev0, p->ev1));
+    *ms = (double)f;
+    return TRPDRV_OK;
+}
+
+int trpdrv_plan_destroy(trpdrv_plan *p)
+{
+    if (!p) return TRPDRV_OK;
+    cudaSetDevice(p->device);
+    cudaStreamSynchronize(p->stream);
+    plan_free(p);
+    return TRPDRV_OK;
+}
+
+int trpdrv_run(const trpdrv_system *host, int nsys, const trpdrv_options *opt, double *emp4, double *emp5)
+{
+    trpdrv_plan *p = NULL;
+    TRY(trpdrv_plan_create(&p, host, nsys, opt));
+    int rc = trpdrv_plan_upload(p, host, NULL);
+    if (rc == TRPDRV_OK) rc = trpdrv_plan_execute(p, NULL);
+    if (rc == TRPDRV_OK) rc = trpdrv_plan_energies(p, emp4, emp5);
+    trpdrv_plan_destroy(p);
+    return rc;
+}
+
+/* ------------------------------------------------------------------------------------------ */
+/* FP64 probe                                                                                   */
+/* ------------------------------------------------------------------------------------------ */
+
+int trpdrv_probe_fp64_peak(int device, int kind, double *tflops)
+{
+    if (!tflops || kind < 0 || kind > 4) return fail(TRPDRV_ERR_ARG, "bad probe arguments");
+    int dev = 0, nsm = 0;
+    TRY(ensure_device(device, &dev, &nsm));
+    const int grid = nsm * 4;
+    double *sink = NULL;
+    CUDA_TRY(cudaMalloc((void **)&sink, sizeof(double) * (size_t)grid * 256));
+    cudaEvent_t e0, e1;
+    CUDA_TRY(cudaEventCreate(&e0));
+    CUDA_TRY(cudaEventCreate(&e1));
+    double flops = 0.0;
+    int iters = 256;
+    float ms = 0.0f;
+    int rc = TRPDRV_OK;
+    /* warm up, then grow the loop until one launch takes >= 50 ms */
+    for (int attempt = 0; attempt < 12; ++attempt) {
+        if (trpdrv_launch_probe(kind, grid, iters, sink, &flops, NULL) != 0) {
+            rc = fail(TRPDRV_ERR_CUDA, "probe launch failed");
+            break;
+        }
+        cudaEventRecord(e0, NULL);
+        if (trpdrv_launch_probe(kind, grid, iters, sink, &flops, NULL) != 0) {
+            rc = fail(TRPDRV_ERR_CUDA, "probe launch failed");
+            break;
+        }
+        cudaEventRecord(e1, NULL);
+        if (cudaEventSynchronize(e1) != cudaSuccess) {
+            rc = fail(TRPDRV_ERR_CUDA, "probe sync failed");
+            break;
+        }
+        cudaEventElapsedTime(&ms, e0, e1);
+        if (ms >= 50.0f) break;
+        iters *= 2;
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    cudaFree(sink);
+    if (rc != TRPDRV_OK) return rc;
+    *tflops = flops / (ms * 1e-3) / 1e12;
+    return TRPDRV_OK;
+}
+
+/* ------------------------------------------------------------------------------------------ */
+/* drop-in entry points                                                                         */
+/* ------------------------------------------------------------------------------------------ */
+
+enum { DI_JIA, DI_KIA, DI_JKA, DI_KKA, DI_TIJ, DI_TKJ, DI_NVV };
+enum { DO_TIA, DO_XIA, DO_TKA, DO_XKA, DO_JIJ, DO_JKJ, DO_KIJ, DO_KKJ, DO_NOV };
+
+static struct dropin_state {
+    int ready, device;
+    cudaStream_t stream;
+    size_t cap_vv, cap_ov, cap_v, cap_bf, cap_pairs;
+    double *vv[DI_NVV];
+    double *ov[DO_NOV];
+    double *nov[4];
+    double *vec[6];
+    double *eorb, *f, *bpart, *out4;
+    unsigned *tcount;
+    double *h_out4; /* pinned */
+} g_di;
+static pthread_mutex_t g_di_mu = PTHREAD_MUTEX_INITIALIZER;
+
+static int env_flag(const char *name, const char *value)
+{
+    const char *v = getenv(name);
+    return v && strcmp(v, value) == 0;
+}
+
+static void di_release(void)
+{
+    if (!g_di.ready) return;
+    cudaSetDevice(g_di.device);
+    for (int q = 0; q < DI_NVV; ++q) cudaFree(g_di.vv[q]);
+    for (int q = 0; q < DO_NOV; ++q) cudaFree(g_di.ov[q]);
+    for (int q = 0; q < 4; ++q) cudaFree(g_di.nov[q]);
+    for (int q = 0; q < 6; ++q) cudaFree(g_di.vec[q]);
+    cudaFree(g_di.eorb);
+    cudaFree(g_di.f);
+    cudaFree(g_di.bpart);
+    cudaFree(g_di.out4);
+    cudaFree(g_di.tcount);
+    cudaFreeHost(g_di.h_out4);
+    cudaStreamDestroy(g_di.stream);
+    memset(&g_di, 0, sizeof g_di);
+}
+
+void trpdrv_finalize(void)
+{
+    pthread_mutex_lock(&g_di_mu);
+    di_release();
+    pthread_mutex_unlock(&g_di_mu);
+}
+
+#define DI_GROW(ptr, count)                                                                         \
+    do {                                                                                            \
+        if (ptr) cudaFree(ptr);                                                                     \
+        ptr = NULL;                                                                                 \
+        CUDA_TRY(cudaMalloc((void **)&(ptr), sizeof(double) * (count)));                            \
+    } while (0)
+
+/* Makes the drop-in device buffers at least as large as one triple of (nocc, nvir, nbf) needs. */
+static int di_reserve(int nocc, int nvir, int nbf)
+{
+    if (!g_di.ready) {
+        int dev = 0;
+        TRY(ensure_device(-1, &dev, NULL));
+        g_di.device = dev;
+        CUDA_TRY(cudaStreamCreateWithFlags(&g_di.stream, cudaStreamNonBlocking));
+        CUDA_TRY(cudaMalloc((void **)&g_di.tcount, sizeof(unsigned)));
+        CUDA_TRY(cudaMemset(g_di.tcount, 0, sizeof(unsigned)));
+        CUDA_TRY(cudaMalloc((void **)&g_di.out4, sizeof(double) * 4));
+        CUDA_TRY(cudaMallocHost((void **)&g_di.h_out4, sizeof(double) * 4));
+        g_di.ready = 1;
+    } else {
+        CUDA_TRY(cudaSetDevice(g_di.device));
+    }
+    const size_t vv = (size_t)nvir * nvir, ov = (size_t)nocc * nvir, v = (size_t)nvir, bf = (size_t)nbf;
+    const int nb = (nvir + TRPDRV_TILE - 1) / TRPDRV_TILE;
+    const size_t pairs = (size_t)nb * (nb + 1) / 2;
+    if (vv > g_di.cap_vv) {
+        for (int q = 0; q < DI_NVV; ++q) DI_GROW(g_di.vv[q], vv);
+        DI_GROW(g_di.f, 8 * vv);
+        g_di.cap_vv = vv;
+    }
+    if (ov > g_di.cap_ov) {
+        for (int q = 0; q < DO_NOV; ++q) DI_GROW(g_di.ov[q], ov);
+        for (int q = 0; q < 4; ++q) DI_GROW(g_di.nov[q], ov);
+        g_di.cap_ov = ov;
+    }
+    if (v > g_di.cap_v) {
+        for (int q = 0; q < 6; ++q) DI_GROW(g_di.vec[q], v);
+        g_di.cap_v = v;
+    }
+    if (bf > g_di.cap_bf) {
+        DI_GROW(g_di.eorb, bf);
+        g_di.cap_bf = bf;
+    }
+    if (pairs > g_di.cap_pairs) {
+        DI_GROW(g_di.bpart, 4 * pairs);
+        g_di.cap_pairs = pairs;
+    }
+    return TRPDRV_OK;
+}
+
+static int h2d(double *dst, const double *src, size_t n)
+{
+    CUDA_TRY(cudaMemcpyAsync(dst, src, sizeof(double) * n, cudaMemcpyHostToDevice, g_di.stream));
+    return TRPDRV_OK;
+}
+
+static int di_tengy_launch(int ncor, int nocc, int nvir, double eaijk)
+{
+    trpdrv_tengy_args ta;
+    memset(&ta, 0, sizeof ta);
+    ta.ncor = ncor;
+    ta.nocc = nocc;
+    ta.nvir = nvir;
+    ta.use_eaijk = 1;
+    ta.eaijk = eaijk;
+    ta.f = g_di.f;
+    ta.eorb = g_di.eorb;
+    ta.dintc1 = g_di.vec[0];
+    ta.dintx1 = g_di.vec[1];
+    ta.t1v1 = g_di.vec[2];
+    ta.dintc2 = g_di.vec[3];
+    ta.dintx2 = g_di.vec[4];
+    ta.t1v2 = g_di.vec[5];
+    ta.block_partial = g_di.bpart;
+    ta.counter = g_di.tcount;
+    ta.out4 = g_di.out4;
+    LAUNCH_TRY(trpdrv_launch_tengy(&ta, g_di.stream));
+    CUDA_TRY(cudaMemcpyAsync(g_di.h_out4, g_di.out4, sizeof(double) * 4, cudaMemcpyDeviceToHost, g_di.stream));
+    CUDA_TRY(cudaStreamSynchronize(g_di.stream));
+    return TRPDRV_OK;
+}
+
+/* omp/ccsd_trpdrv_omp_cbody.c:31-145 on the device, for one triple from host buffers. */
+static int body_impl(double *f1n, double *f1t, double *f2n, double *f2t, double *f3n, double *f3t, double *f4n,
+                     double *f4t, double *eorb, int *ncor_, int *nocc_, int *nvir_, double *emp4_, double *emp5_,
+                     int *a_, int *i_, int *j_, int *k_, int *klo_, double *tij, double *tkj, double *tia,
+                     double *tka, double *xia, double *xka, double *jia, double *jka, double *kia, double *kka,
+                     double *jij, double *jkj, double *kij, double *kkj, double *dintc1, double *dintx1,
+                     double *t1v1, double *dintc2, double *dintx2, double *t1v2)
+{
+    if (!ncor_ || !nocc_ || !nvir_ || !a_ || !i_ || !j_ || !k_ || !klo_ || !emp4_ || !emp5_)
+        return fail(TRPDRV_ERR_ARG, "NULL scalar argument");
+    const int ncor = *ncor_, nocc = *nocc_, nvir = *nvir_;
+    const int a = *a_, i = *i_, j = *j_, k = *k_, klo = *klo_;
+    const double *arrays[] = {eorb, tij, tkj, tia, tka, xia, xka, jia, jka, kia, kka,
+                              jij, jkj, kij, kkj, dintc1, dintx1, t1v1, dintc2, dintx2, t1v2};
+    for (size_t q = 0; q < sizeof arrays / sizeof arrays[0]; ++q)
+        if (!arrays[q]) return fail(TRPDRV_ERR_ARG, "NULL array argument #%zu", q);
+    if (nocc < 1 || nvir < 1 || ncor < 0 || nocc > TRPDRV_MAX_NOCC || nvir > TRPDRV_MAX_NVIR)
+        return fail(TRPDRV_ERR_ARG, "ncor=%d nocc=%d nvir=%d", ncor, nocc, nvir);
+    const int nbf = ncor + nocc + nvir;
+    if (a < 1 || a > nbf) return fail(TRPDRV_ERR_ARG, "a=%d outside [1,%d]", a, nbf);
+    if (i < 1 || i > nocc || j < 1 || j > nocc || k < 1 || k > nocc)
+        return fail(TRPDRV_ERR_ARG, "i=%d j=%d k=%d outside [1,%d]", i, j, k, nocc);
+    if (klo < 1 || klo > k) return fail(TRPDRV_ERR_ARG, "klo=%d must satisfy 1 <= klo <= k=%d", klo, k);
+    const int write_f = env_flag("TRPDRV_WRITE_F", "1");
+    if (write_f && (!f1n || !f1t || !f2n || !f2t || !f3n || !f3t || !f4n || !f4t))
+        return fail(TRPDRV_ERR_ARG, "TRPDRV_WRITE_F=1 with a NULL f array");
+
+    TRY(di_reserve(nocc, nvir, nbf));
+    const size_t lnvv = (size_t)nvir * nvir, lnov = (size_t)nocc * nvir;
+    const size_t vv = (size_t)(k - klo) * lnvv, ov = (size_t)(k - klo) * lnov;
+    TRY(h2d(g_di.vv[DI_JIA], jia, lnvv));
+    TRY(h2d(g_di.vv[DI_KIA], kia, lnvv));
+    TRY(h2d(g_di.vv[DI_JKA], jka + vv, lnvv));
+    TRY(h2d(g_di.vv[DI_KKA], kka + vv, lnvv));
+    TRY(h2d(g_di.vv[DI_TIJ], tij, lnvv));
+    TRY(h2d(g_di.vv[DI_TKJ], tkj + vv, lnvv));
+    TRY(h2d(g_di.ov[DO_TIA], tia, lnov));
+    TRY(h2d(g_di.ov[DO_XIA], xia, lnov));
+    TRY(h2d(g_di.ov[DO_TKA], tka + ov, lnov));
+    TRY(h2d(g_di.ov[DO_XKA], xka + ov, lnov));
+    TRY(h2d(g_di.ov[DO_JIJ], jij, lnov));
+    TRY(h2d(g_di.ov[DO_JKJ], jkj + ov, lnov));
+    TRY(h2d(g_di.ov[DO_KIJ], kij, lnov));
+    TRY(h2d(g_di.ov[DO_KKJ], kkj + ov, lnov));
+    const double *vecs[6] = {dintc1, dintx1, t1v1, dintc2, dintx2, t1v2};
+    for (int q = 0; q < 6; ++q) TRY(h2d(g_di.vec[q], vecs[q], (size_t)nvir));
+    TRY(h2d(g_di.eorb, eorb, (size_t)nbf));
+    for (int q = 0; q < 4; ++q) LAUNCH_TRY(trpdrv_launch_negate(g_di.ov[q], g_di.nov[q], lnov, g_di.stream));
+
+    trpdrv_plain_args ga;
+    memset(&ga, 0, sizeof ga);
+    ga.nocc = nocc;
+    ga.nvir = nvir;
+    ga.f = g_di.f;
+    double *const *V = g_di.vv;
+    double *const *N = g_di.nov;
+    double *const *Ob = g_di.ov;
+    const double *a1[8] = {V[DI_JIA], V[DI_KIA], V[DI_JIA], V[DI_KIA], V[DI_JKA], V[DI_KKA], V[DI_JKA], V[DI_KKA]};
+    const double *b1[8] = {V[DI_TKJ], V[DI_TKJ], V[DI_TKJ], V[DI_TKJ], V[DI_TIJ], V[DI_TIJ], V[DI_TIJ], V[DI_TIJ]};
+    const int nt[8] = {1, 1, 0, 0, 1, 1, 0, 0};
+    const double *a2[8] = {N[0], N[1], N[0], N[1], N[2], N[3], N[2], N[3]};
+    const double *b2[8] = {Ob[DO_KKJ], Ob[DO_KKJ], Ob[DO_JKJ], Ob[DO_JKJ], Ob[DO_KIJ], Ob[DO_KIJ], Ob[DO_JIJ], Ob[DO_JIJ]};
+    for (int x = 0; x < 8; ++x) {
+        ga.a1[x] = a1[x];
+        ga.b1[x] = b1[x];
+        ga.b1_nt[x] = nt[x];
+        ga.a2[x] = a2[x];
+        ga.b2[x] = b2[x];
+    }
+    const int vec2 = !(nvir & 1) && !(nocc & 1);
+    LAUNCH_TRY(trpdrv_launch_plain_gemm(&ga, vec2, g_di.stream));
+
+    /* omp/ccsd_trpdrv_omp_cbody.c:122-126 */
+    const double eaijk = eorb[a - 1] - (eorb[ncor + i - 1] + eorb[ncor + j - 1] + eorb[ncor + k - 1]);
+    TRY(di_tengy_launch(ncor, nocc, nvir, eaijk));
+
+    if (write_f) {
+        double *outs[8] = {f1n, f2n, f3n, f4n, f1t, f2t, f3t, f4t};
+        for (int x = 0; x < 8; ++x)
+            CUDA_TRY(cudaMemcpy(outs[x], g_di.f + (size_t)x * lnvv, sizeof(double) * lnvv, cudaMemcpyDeviceToHost));
+    }
+    /* omp/ccsd_trpdrv_omp_cbody.c:133-142 */
+    const double e4i = g_di.h_out4[0], e5i = g_di.h_out4[1], e4k = g_di.h_out4[2], e5k = g_di.h_out4[3];
+    double emp4 = *emp4_, emp5 = *emp5_;
+    emp4 += e4i;
+    emp5 += e5i;
+    if (i != k) {
+        emp4 += e4k;
+        emp5 += e5k;
+    }
+    *emp4_ = emp4;
+    *emp5_ = emp5;
+    return TRPDRV_OK;
+}
+
+static void report(int rc, const char *who)
+{
+    if (rc == TRPDRV_OK) return;
+    if (env_flag("TRPDRV_ON_ERROR", "return")) return;
+    fprintf(stderr, "%s: %s: %s\n", who, trpdrv_status_string(rc), t_message);
+    abort();
+}
+
+#define BODY_ARGS                                                                                   \
+    double *f1n, double *f1t, double *f2n, double *f2t, double *f3n, double *f3t, double *f4n, double *f4t, \
+        double *eorb, int *ncor, int *nocc, int *nvir, double *emp4, double *emp5, int *a, int *i, int *j,  \
+        int *k, int *klo, double *tij, double *tkj, double *tia, double *tka, double *xia, double *xka,     \
+        double *jia, double *jka, double *kia, double *kka, double *jij, double *jkj, double *kij,          \
+        double *kkj, double *dintc1, double *dintx1, double *t1v1, double *dintc2, double *dintx2,          \
+        double *t1v2
+#define BODY_PASS                                                                                   \
+    f1n, f1t, f2n, f2t, f3n, f3t, f4n, f4t, eorb, ncor, nocc, nvir, emp4, emp5, a, i, j, k, klo, tij, tkj, \
+        tia, tka, xia, xka, jia, jka, kia, kka, jij, jkj, kij, kkj, dintc1, dintx1, t1v1, dintc2, dintx2, t1v2
+
+static void body_entry(const char *who, BODY_ARGS)
+{
+    pthread_mutex_lock(&g_di_mu);
+    t_status = TRPDRV_OK;
+    const int rc = body_impl(BODY_PASS);
+    pthread_mutex_unlock(&g_di_mu);
+    report(rc, who);
+}
+
+void ccsd_trpdrv_omp_cbody_(BODY_ARGS) { body_entry("ccsd_trpdrv_omp_cbody_", BODY_PASS); }
+void ccsd_trpdrv_omp_fbody_(BODY_ARGS) { body_entry("ccsd_trpdrv_omp_fbody_", BODY_PASS); }
+void ccsd_trpdrv_cbody_(BODY_ARGS) { body_entry("ccsd_trpdrv_cbody_", BODY_PASS); }
+void ccsd_trpdrv_opencl_(BODY_ARGS) { body_entry("ccsd_trpdrv_opencl_", BODY_PASS); }
+
+/* omp/ccsd_tengy_c99.c:5-119 on the device, from host f arrays. */
+static int tengy_impl(const double *f1n, const double *f1t, const double *f2n, const double *f2t,
+                      const double *f3n, const double *f3t, const double *f4n, const double *f4t,
+                      const double *dintc1, const double *dintx1, const double *t1v1, const double *dintc2,
+                      const double *dintx2, const double *t1v2, const double *eorb, double eaijk, double *emp4i,
+                      double *emp5i, double *emp4k, double *emp5k, int ncor, int nocc, int nvir)
+{
+    const double *arrays[] = {f1n, f1t, f2n, f2t, f3n, f3t, f4n, f4t, dintc1, dintx1, t1v1, dintc2, dintx2, t1v2, eorb};
+    for (size_t q = 0; q < sizeof arrays / sizeof arrays[0]; ++q)
+        if (!arrays[q]) return fail(TRPDRV_ERR_ARG, "NULL array argument #%zu", q);
+    if (!emp4i || !emp5i || !emp4k || !emp5k) return fail(TRPDRV_ERR_ARG, "NULL output");
+    if (nocc < 0 || nvir < 1 || ncor < 0 || nvir > TRPDRV_MAX_NVIR)
+        return fail(TRPDRV_ERR_ARG, "ncor=%d nocc=%d nvir=%d", ncor, nocc, nvir);
+    const int nbf = ncor + nocc + nvir;
+    TRY(di_reserve(nocc > 0 ? nocc : 1, nvir, nbf));
+    const size_t lnvv = (size_t)nvir * nvir;
+    const double *fs[8] = {f1n, f2n, f3n, f4n, f1t, f2t, f3t, f4t};
+    for (int x = 0; x < 8; ++x) TRY(h2d(g_di.f + (size_t)x * lnvv, fs[x], lnvv));
+    const double *vecs[6] = {dintc1, dintx1, t1v1, dintc2, dintx2, t1v2};
+    for (int q = 0; q < 6; ++q) TRY(h2d(g_di.vec[q], vecs[q], (size_t)nvir));
+    TRY(h2d(g_di.eorb, eorb, (size_t)nbf));
+    TRY(di_tengy_launch(ncor, nocc, nvir, eaijk));
+    *emp4i = g_di.h_out4[0];
+    *emp5i = g_di.h_out4[1];
+    *emp4k = g_di.h_out4[2];
+    *emp5k = g_di.h_out4[3];
+    return TRPDRV_OK;
+}
+
+#define TENGY_ARGS                                                                                  \
+    const double *f1n, const double *f1t, const double *f2n, const double *f2t, const double *f3n,       \
+        const double *f3t, const double *f4n, const double *f4t, const double *dintc1, const double *dintx1, \
+        const double *t1v1, const double *dintc2, const double *dintx2, const double *t1v2,             \
+        const double *eorb, const double eaijk, double *emp4i, double *emp5i, double *emp4k, double *emp5k, \
+        const int ncor, const int nocc, const int nvir
+
+static void tengy_entry(const char *who, TENGY_ARGS)
+{
+    pthread_mutex_lock(&g_di_mu);
+    t_status = TRPDRV_OK;
+    const int rc = tengy_impl(f1n, f1t, f2n, f2t, f3n, f3t, f4n, f4t, dintc1, dintx1, t1v1, dintc2, dintx2, t1v2,
+                              eorb, eaijk, emp4i, emp5i, emp4k, emp5k, ncor, nocc, nvir);
+    pthread_mutex_unlock(&g_di_mu);
+    report(rc, who);
+}
+
+void ccsd_tengy_omp(TENGY_ARGS)
+{
+    tengy_entry("ccsd_tengy_omp", f1n, f1t, f2n, f2t, f3n, f3t, f4n, f4t, dintc1, dintx1, t1v1, dintc2, dintx2,
+                t1v2, eorb, eaijk, emp4i, emp5i, emp4k, emp5k, ncor, nocc, nvir);
+}
+
+void ccsd_tengy(TENGY_ARGS)
+{
+    tengy_entry("ccsd_tengy", f1n, f1t, f2n, f2t, f3n, f3t, f4n, f4t, dintc1, dintx1, t1v1, dintc2, dintx2, t1v2,
+                eorb, eaijk, emp4i, emp5i, emp4k, emp5k, ncor, nocc, nvir);
+}
+
+/* Fortran order (omp/ccsd_tengy_f77.f:1-5): dintc1, dintc2, dintx1, dintx2, t1v1, t1v2, all by reference. */
+void ccsd_tengy_omp_(const double *f1n, const double *f1t, const double *f2n, const double *f2t, const double *f3n,
+                     const double *f3t, const double *f4n, const double *f4t, const double *dintc1,
+                     const double *dintc2, const double *dintx1, const double *dintx2, const double *t1v1,
+                     const double *t1v2, const double *eorb, const double *eaijk, double *emp4i, double *emp5i,
+                     double *emp4k, double *emp5k, const int *ncor, const int *nocc, const int *nvir)
+{
+    if (!eaijk || !ncor || !nocc || !nvir) {
+        pthread_mutex_lock(&g_di_mu);
+        const int rc = fail(TRPDRV_ERR_ARG, "NULL scalar argument");
+        pthread_mutex_unlock(&g_di_mu);
+        report(rc, "ccsd_tengy_omp_");
+        return;
+    }
+    tengy_entry("ccsd_tengy_omp_", f1n, f1t, f2n, f2t, f3n, f3t, f4n, f4t, dintc1, dintx1, t1v1, dintc2, dintx2,
+                t1v2, eorb, *eaijk, emp4i, emp5i, emp4k, emp5k, *ncor, *nocc, *nvir);
+}

@@ -1,0 +1,93 @@
+/*
+ * Internal interface between the C host layer (host.c) and the CUDA translation units.
+ * Plain C structs and extern "C" launchers only; every launcher enqueues on the given stream and
+ * returns a cudaError_t value (0 = success).
+ */
+#ifndef TRPDRV_LAUNCH_H
+#define TRPDRV_LAUNCH_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Width of the (b,c) tiles of the fused kernel and of the standalone tengy kernel. */
+#define TRPDRV_TILE 32
+/* Triples are packed as (i-1) | (j-1) << 10 | (k-1) << 20 (0-based), so nocc must be < 1024. */
+#define TRPDRV_MAX_NOCC 1023
+/* Largest nvir the kernels accept (index arithmetic is 32-bit within one nvir x nvir block). */
+#define TRPDRV_MAX_NVIR 16384
+
+/* Device view of one system in a plan.  ntov/nxov hold -tov/-xov, so that every f is the sum of
+ * two products accumulated with +1 (the reference's alpha = -1 GEMMs, omp/ccsd_trpdrv_omp_cbody.c:73-116). */
+typedef struct trpdrv_dev_system {
+    int ncor, nocc, nvir, a;
+    int nb;              /* ceil(nvir / TRPDRV_TILE) */
+    int npairs;          /* nb*(nb+1)/2 tile pairs (B <= C) */
+    int64_t ntriples;    /* triples of this system in the plan (this rank's share) */
+    int64_t item_begin;  /* first fused work item of this system */
+    const double *eorb, *t2, *jvv, *kvv, *ntov, *nxov, *jov, *kov, *dintc, *dintx, *t1v;
+    const int32_t *triples; /* packed triples, processing order */
+    double *partial;        /* [ntriples*npairs][4] per work item: e4i, e5i, e4k, e5k */
+    double *rec;            /* [ntriples][4] per triple */
+} trpdrv_dev_system;
+
+/* Fused persistent kernel: grid CTAs pull (triple, tile pair) items from *counter (must be 0 at
+ * launch) and write per-item energies.  vec2 = 1 requires even nvir and nocc for every system. */
+int trpdrv_launch_fused(const trpdrv_dev_system *d_sys, int nsys, int64_t total_items,
+                        unsigned long long *counter, int *status, int grid, int vec2, void *stream);
+size_t trpdrv_fused_smem_bytes(void);
+int trpdrv_fused_threads(void);
+int trpdrv_fused_max_ctas_per_sm(int *n);
+
+/* Per-triple sum of the per-item energies of one system (partial -> rec). */
+int trpdrv_launch_item_reduce(const trpdrv_dev_system *h_sys, void *stream);
+
+/* Compensated per-system total over rec: out[0..3] = emp4 hi, emp4 lo, emp5 hi, emp5 lo, where the
+ * total is emp4i + [i != k] emp4k summed over the triples. */
+int trpdrv_launch_system_reduce(const double *rec, const int32_t *triples, int64_t ntriples,
+                                double *out, void *stream);
+
+/* dst[i] = -src[i]. */
+int trpdrv_launch_negate(const double *src, double *dst, size_t n, void *stream);
+
+/* Plain per-triple path: one grouped launch computes the eight f = A1*op(B1) + A2*B2 into
+ * f[8][nvir][nvir] (order f1n f2n f3n f4n f1t f2t f3t f4t); b1_nt[x] = 1 if B1 is used transposed. */
+typedef struct trpdrv_plain_args {
+    int nocc, nvir;
+    const double *a1[8], *b1[8], *a2[8], *b2[8];
+    int b1_nt[8];
+    double *f;
+} trpdrv_plain_args;
+int trpdrv_launch_plain_gemm(const trpdrv_plain_args *args, int vec2, void *stream);
+
+/* Standalone tengy over f[8][nvir][nvir] on the device.  eaijk is taken from `eaijk` when
+ * use_eaijk != 0, else computed on the device from eorb and the 1-based a, i, j, k.  Writes
+ * out4[0..3] = emp4i, emp5i, emp4k, emp5k.  block_partial needs 4*npairs doubles, counter one
+ * zeroed unsigned int (it is left at zero again). */
+typedef struct trpdrv_tengy_args {
+    int ncor, nocc, nvir;
+    int use_eaijk;
+    double eaijk;
+    int a, i, j, k;
+    const double *f;
+    const double *eorb, *dintc1, *dintx1, *t1v1, *dintc2, *dintx2, *t1v2;
+    double *block_partial;
+    unsigned int *counter;
+    double *out4;
+} trpdrv_tengy_args;
+int trpdrv_launch_tengy(const trpdrv_tengy_args *args, void *stream);
+size_t trpdrv_tengy_smem_bytes(void);
+
+/* FP64 issue-rate probe: kind as trpdrv_probe_fp64_peak; returns FLOPs executed. */
+int trpdrv_launch_probe(int kind, int grid, int iters, double *sink, double *flops, void *stream);
+
+/* Sets the dynamic shared memory limits of every kernel (call once per device). */
+int trpdrv_kernels_init(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,96 @@
+// FP64 issue-rate probe: the roofline denominator for the FP64 contraction kernels.
+//
+// Every warp keeps NACC independent accumulator chains in registers and issues NACC MMAs (or DFMAs)
+// per iteration with register operands only, so the measured rate is the FP64 tensor (or FMA) pipe
+// throughput of the device, not a memory rate.  The accumulators are written out at the end so the
+// work cannot be eliminated.
+
+#include "device_common.cuh"
+#include "launch.h"
+
+namespace trpdrv {
+namespace probe {
+
+constexpr int NACC = 8;
+constexpr int NTHREAD = 256;
+
+template <int KIND>
+__global__ void __launch_bounds__(NTHREAD)
+probe_kernel(int iters, double *sink)
+{
+    const int lane = threadIdx.x & 31;
+    const double a0 = 1.0 + 1e-9 * lane, a1 = 1.0 - 1e-9 * lane, b0 = 0.5 + 1e-9 * threadIdx.x;
+    double acc[NACC][4];
+#pragma unroll
+    for (int q = 0; q < NACC; ++q)
+#pragma unroll
+        for (int e = 0; e < 4; ++e) acc[q][e] = 0.0;
+    double a4[4] = {a0, a1, a0, a1}, b2[2] = {b0, b0};
+    double a8[8] = {a0, a1, a0, a1, a0, a1, a0, a1}, b4[4] = {b0, b0, b0, b0};
+
+    for (int it = 0; it < iters; ++it) {
+#pragma unroll
+        for (int q = 0; q < NACC; ++q) {
+            if (KIND == 0) {
+                double d[2] = {acc[q][0], acc[q][1]};
+                dmma_8x8x4(d, a0, b0);
+                acc[q][0] = d[0];
+                acc[q][1] = d[1];
+            } else if (KIND == 1) {
+                dmma_16x8x4(acc[q], a0, a1, b0);
+            } else if (KIND == 2) {
+                dmma_16x8x8(acc[q], a4, b2);
+            } else if (KIND == 3) {
+                dmma_16x8x16(acc[q], a8, b4);
+            } else {
+#pragma unroll
+                for (int e = 0; e < 4; ++e) asm volatile("fma.rn.f64 %0, %1, %2, %0;" : "+d"(acc[q][e]) : "d"(a0), "d"(b0));
+            }
+        }
+    }
+    double s = 0.0;
+#pragma unroll
+    for (int q = 0; q < NACC; ++q)
+#pragma unroll
+        for (int e = 0; e < 4; ++e) s += acc[q][e];
+    sink[blockIdx.x * NTHREAD + threadIdx.x] = s;
+}
+
+}  // namespace probe
+}  // namespace trpdrv
+
+using namespace trpdrv;
+
+extern "C" int trpdrv_launch_probe(int kind, int grid, int iters, double *sink, double *flops, void *stream)
+{
+    cudaStream_t st = (cudaStream_t)stream;
+    const double warps = (double)grid * (probe::NTHREAD / 32);
+    const double per_iter = probe::NACC;
+    double mma_flops = 0.0;
+    switch (kind) {
+    case 0:
+        probe::probe_kernel<0><<<grid, probe::NTHREAD, 0, st>>>(iters, sink);
+        mma_flops = 2.0 * 8 * 8 * 4;
+        break;
+    case 1:
+        probe::probe_kernel<1><<<grid, probe::NTHREAD, 0, st>>>(iters, sink);
+        mma_flops = 2.0 * 16 * 8 * 4;
+        break;
+    case 2:
+        probe::probe_kernel<2><<<grid, probe::NTHREAD, 0, st>>>(iters, sink);
+        mma_flops = 2.0 * 16 * 8 * 8;
+        break;
+    case 3:
+        probe::probe_kernel<3><<<grid, probe::NTHREAD, 0, st>>>(iters, sink);
+        mma_flops = 2.0 * 16 * 8 * 16;
+        break;
+    case 4:
+        probe::probe_kernel<4><<<grid, probe::NTHREAD, 0, st>>>(iters, sink);
+        mma_flops = 2.0 * 4 * 32;  // 4 DFMA per accumulator per lane
+        break;
+    default:
+        return (int)cudaErrorInvalidValue;
+    }
+    if (flops) *flops = warps * iters * per_iter * mma_flops;
+    return (int)cudaGetLastError();
+}

@@ -1,0 +1,130 @@
+// Deterministic energy reductions and small device utilities.
+//
+//  item_reduce_kernel:   per triple, the sum of its tile-pair items (fixed order) -> rec[t][4]
+//  system_reduce_kernel: per system, the compensated total of emp4i + [i != k] emp4k and of
+//                        emp5i + [i != k] emp5k over the triples (the accumulation of
+//                        omp/ccsd_trpdrv_omp_cbody.c:133-142), as a double-double (hi, lo) pair,
+//                        built with error-free TwoSum in a fixed order.
+//  negate_kernel:        dst = -src (the occupied A operands are stored negated).
+
+#include "device_common.cuh"
+#include "launch.h"
+
+namespace trpdrv {
+
+__global__ void item_reduce_kernel(const double *__restrict__ partial, int npairs, long long ntriples,
+                                   double *__restrict__ rec)
+{
+    const long long t = (long long)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    const int lane = threadIdx.x & 31;
+    if (t >= ntriples) return;
+    const double *p = partial + 4 * t * (long long)npairs;
+    double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
+    for (int q = lane; q < npairs; q += 32) {
+        s0 += p[4 * q + 0];
+        s1 += p[4 * q + 1];
+        s2 += p[4 * q + 2];
+        s3 += p[4 * q + 3];
+    }
+    s0 = warp_sum(s0);
+    s1 = warp_sum(s1);
+    s2 = warp_sum(s2);
+    s3 = warp_sum(s3);
+    if (lane == 0) {
+        rec[4 * t + 0] = s0;
+        rec[4 * t + 1] = s1;
+        rec[4 * t + 2] = s2;
+        rec[4 * t + 3] = s3;
+    }
+}
+
+__device__ __forceinline__ void dd_add(double &hi, double &lo, double x)
+{
+    double s, e;
+    two_sum(hi, x, s, e);
+    hi = s;
+    lo += e;
+}
+
+constexpr int RED_THREADS = 1024;
+
+__global__ void __launch_bounds__(RED_THREADS)
+system_reduce_kernel(const double *__restrict__ rec, const int32_t *__restrict__ triples, long long n,
+                     double *__restrict__ out)
+{
+    __shared__ double sh[4][RED_THREADS];
+    double h4 = 0.0, l4 = 0.0, h5 = 0.0, l5 = 0.0;
+    for (long long t = threadIdx.x; t < n; t += RED_THREADS) {
+        const int packed = triples[t];
+        const int i = packed & 1023, k = (packed >> 20) & 1023;
+        dd_add(h4, l4, rec[4 * t + 0]);
+        dd_add(h5, l5, rec[4 * t + 1]);
+        if (i != k) {
+            dd_add(h4, l4, rec[4 * t + 2]);
+            dd_add(h5, l5, rec[4 * t + 3]);
+        }
+    }
+    sh[0][threadIdx.x] = h4;
+    sh[1][threadIdx.x] = l4;
+    sh[2][threadIdx.x] = h5;
+    sh[3][threadIdx.x] = l5;
+    __syncthreads();
+    for (int w = RED_THREADS / 2; w > 0; w >>= 1) {
+        if ((int)threadIdx.x < w) {
+            const int o = threadIdx.x + w;
+            double s, e;
+            two_sum(sh[0][threadIdx.x], sh[0][o], s, e);
+            sh[0][threadIdx.x] = s;
+            sh[1][threadIdx.x] += sh[1][o] + e;
+            two_sum(sh[2][threadIdx.x], sh[2][o], s, e);
+            sh[2][threadIdx.x] = s;
+            sh[3][threadIdx.x] += sh[3][o] + e;
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        double s, e;
+        two_sum(sh[0][0], sh[1][0], s, e);  // renormalise
+        out[0] = s;
+        out[1] = e;
+        two_sum(sh[2][0], sh[3][0], s, e);
+        out[2] = s;
+        out[3] = e;
+    }
+}
+
+__global__ void negate_kernel(const double *__restrict__ src, double *__restrict__ dst, size_t n)
+{
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+        dst[i] = -src[i];
+}
+
+}  // namespace trpdrv
+
+using namespace trpdrv;
+
+extern "C" int trpdrv_launch_item_reduce(const trpdrv_dev_system *h_sys, void *stream)
+{
+    if (h_sys->ntriples <= 0) return 0;
+    const int warps = 8;
+    const long long blocks = (h_sys->ntriples + warps - 1) / warps;
+    item_reduce_kernel<<<(unsigned)blocks, warps * 32, 0, (cudaStream_t)stream>>>(h_sys->partial, h_sys->npairs,
+                                                                                 h_sys->ntriples, h_sys->rec);
+    return (int)cudaGetLastError();
+}
+
+extern "C" int trpdrv_launch_system_reduce(const double *rec, const int32_t *triples, int64_t ntriples,
+                                           double *out, void *stream)
+{
+    system_reduce_kernel<<<1, RED_THREADS, 0, (cudaStream_t)stream>>>(rec, triples, (long long)ntriples, out);
+    return (int)cudaGetLastError();
+}
+
+extern "C" int trpdrv_launch_negate(const double *src, double *dst, size_t n, void *stream)
+{
+    if (n == 0) return 0;
+    size_t blocks = (n + 255) / 256;
+    if (blocks > 4096) blocks = 4096;
+    negate_kernel<<<(unsigned)blocks, 256, 0, (cudaStream_t)stream>>>(src, dst, n);
+    return (int)cudaGetLastError();
+}

@@ -1,0 +1,46 @@
+// The tengy reduction over one tile pair {B,C} whose f tiles are parked in shared memory.
+// Layout of `park`: 16 tiles of 32 x 33 doubles; tile (o*8 + x) holds f_x(B+r, C+q) for o = 0 and
+// f_x(C+r, B+q) for o = 1 at [r*33 + q] (x = f1n f2n f3n f4n f1t f2t f3t f4t).  For a diagonal pair
+// (B == C) only the o = 0 tiles are used.  Follows omp/ccsd_tengy_c99.c:58-111: every (b,c) of
+// BxC and CxB contributes one term with denom = -1/(e_b + e_c + eaijk).
+#pragma once
+
+#include "device_common.cuh"
+
+namespace trpdrv {
+
+constexpr int TT = 32;           // tile width
+constexpr int TPP = TT + 1;      // parked tile pitch
+constexpr int TPTILE = TT * TPP;
+
+struct TengyVecs {
+    const double *eorb, *dintc1, *dintx1, *t1v1, *dintc2, *dintx2, *t1v2;
+    double eaijk;
+    int voff;  // ncor + nocc: index of the first virtual orbital energy
+    int nvir;
+};
+
+__device__ __forceinline__ void tengy_tile_pair(const double *park, int b0, int c0, bool diag,
+                                                const TengyVecs &v, int tid, int nthreads, TengySums &su)
+{
+    const int nterm = diag ? TT * TT : 2 * TT * TT;
+    for (int idx = tid; idx < nterm; idx += nthreads) {
+        const int s = idx >> 10, r = (idx >> 5) & 31, q = idx & 31;
+        const int b = (s ? c0 : b0) + r, c = (s ? b0 : c0) + q;
+        if (b < v.nvir && c < v.nvir) {
+            const double *bcT = park + (s * 8) * TPTILE + r * TPP + q;
+            const double *cbT = park + ((diag ? 0 : 1 - s) * 8) * TPTILE + q * TPP + r;
+            double fbc[8], fcb[8];
+#pragma unroll
+            for (int f = 0; f < 8; ++f) {
+                fbc[f] = bcT[f * TPTILE];
+                fcb[f] = cbT[f * TPTILE];
+            }
+            const double denom = -1.0 / (__ldg(v.eorb + v.voff + b) + __ldg(v.eorb + v.voff + c) + v.eaijk);
+            tengy_term(fbc, fcb, denom, __ldg(v.t1v1 + b), __ldg(v.t1v2 + b), __ldg(v.dintx1 + c),
+                       __ldg(v.dintx2 + c), __ldg(v.dintc1 + c), __ldg(v.dintc2 + c), su);
+        }
+    }
+}
+
+}  // namespace trpdrv

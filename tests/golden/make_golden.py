@@ -43,6 +43,10 @@ def checksums(s):
 
 
 def main():
+    if os.environ.get("OMP_NUM_THREADS") != "1":
+        # one OpenMP thread inside the reference tengy: a fixed reduction order, reproducible fixtures
+        os.execvpe(sys.executable, [sys.executable, os.path.abspath(__file__)],
+                   dict(os.environ, OMP_NUM_THREADS="1", OPENBLAS_NUM_THREADS="1"))
     out_dir = os.path.dirname(os.path.abspath(__file__))
     for name, (ncor, nocc, nvir, seed, dist, nkpass) in CASES.items():
         s = T.synth_system(nocc, nvir, seed=seed, ncor=ncor, dist=dist)
@@ -62,14 +66,17 @@ def main():
             json.dump(doc, f, separators=(",", ":"))
         print(name, len(rec), tot)
 
-    kat = subprocess.run([O.REF_TEST, "10", "60", "100000"], capture_output=True, text=True, check=True,
-                         env=dict(os.environ, OMP_NUM_THREADS="1", OPENBLAS_NUM_THREADS="1"))
-    line = [ln for ln in kat.stdout.splitlines() if ln.startswith("emp4=")][0]
+    runs = []
+    for argv in (["10", "60", "100000"], ["10", "60", "100000", "3"], ["12", "50", "100000", "2"]):
+        kat = subprocess.run([O.REF_TEST, *argv], capture_output=True, text=True, check=True,
+                             env=dict(os.environ, OMP_NUM_THREADS="1", OPENBLAS_NUM_THREADS="1"))
+        line = [ln for ln in kat.stdout.splitlines() if ln.startswith("emp4=")][0]
+        runs.append({"argv": argv, "line": line})
+        print(argv, line)
     with open(os.path.join(out_dir, "kat_test_c99_10_60.json"), "w") as f:
-        json.dump({"command": "test_c99 10 60 100000", "line": line,
+        json.dump({"command": "test_c99 10 60 100000", "line": runs[0]["line"], "runs": runs,
                    "source": "reference omp/test.c + omp/ccsd_trpdrv_omp_cbody.c + omp/ccsd_tengy_c99.c, unmodified"},
                   f, indent=1)
-    print(line)
 
 
 if __name__ == "__main__":

@@ -4,6 +4,7 @@ Every call goes through the C ABI (libtrpdrv_b200.so).  Bars: emp4/emp5 totals w
 relative (TOTAL_RTOL); per-triple records within 1e-11 normwise per column (RECORD_RTOL); f arrays
 within 1e-12 normwise; shards, batches and repeated runs bit-identical where the arithmetic is.
 """
+import json
 import os
 import subprocess
 
@@ -183,11 +184,13 @@ def test_unmodified_reference_driver_links_and_passes_kat(O, binary):
     path = os.path.join(os.path.dirname(O.ORACLE_LIB), "_ref", binary)
     if not os.path.exists(path):
         pytest.skip(f"{binary} not built")
-    out = subprocess.run([path, "10", "60", "100000"], capture_output=True, text=True, timeout=300)
-    assert out.returncode == 0, out.stderr
-    assert "emp4=2.647247 emp5=-1.560018" in out.stdout
-    out = subprocess.run([path, "10", "60", "100000", "3"], capture_output=True, text=True, timeout=300)
-    assert out.returncode == 0 and "emp4=2.647247 emp5=-1.560018" in out.stdout
+    with open(os.path.join(GOLDEN, "kat_test_c99_10_60.json")) as f:
+        runs = json.load(f)["runs"]
+    assert runs[0]["line"] == "emp4=2.647247 emp5=-1.560018"
+    for run in runs:  # (10, 60), (10, 60, nkpass 3), (12, 50, nkpass 2): the reference driver's own prints
+        out = subprocess.run([path, *run["argv"]], capture_output=True, text=True, timeout=300)
+        assert out.returncode == 0, out.stderr
+        assert run["line"] in out.stdout, (run, out.stdout[-300:])
 
 
 def test_dropin_errors_are_reported_not_computed(T, monkeypatch):

@@ -46,7 +46,12 @@ def parse():
     ap.add_argument("--nvir", type=int, default=NVIR)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-plain", action="store_true")
-    return ap.parse_args()
+    ap.add_argument("--profile", action="store_true",
+                    help="fused steps only (no probes, e2e, plain or CPU legs): the command profiled with ncu")
+    args = ap.parse_args()
+    if args.profile:
+        args.no_cpu_baseline = args.no_plain = True
+    return args
 
 
 def workload(nocc, nvir):
@@ -208,19 +213,22 @@ def run_b200_arm(args):
     in_bytes = s.nbytes()
 
     # FP64 peak of this device (library probe; best of the DMMA shapes) and cuBLAS DGEMM for context
-    probe = {k: T.probe_fp64_peak(k, local) for k in (1, 2, 3, 4)}
-    peak = max(probe[1], probe[2], probe[3])
-    a = torch.randn(8192, 8192, dtype=torch.float64, device=dev)
-    torch.matmul(a, a)
-    torch.cuda.synchronize()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record()
-    for _ in range(3):
+    probe, cublas_dgemm = {1: 0.0, 2: 0.0, 3: 0.0, 4: 0.0}, 0.0
+    if not args.profile:
+        probe = {k: T.probe_fp64_peak(k, local) for k in (1, 2, 3, 4)}
+        a = torch.randn(8192, 8192, dtype=torch.float64, device=dev)
         torch.matmul(a, a)
-    e1.record()
-    torch.cuda.synchronize()
-    cublas_dgemm = 3 * 2 * 8192 ** 3 / (e0.elapsed_time(e1) * 1e-3) / 1e12
-    del a
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(3):
+            torch.matmul(a, a)
+        e1.record()
+        torch.cuda.synchronize()
+        cublas_dgemm = 3 * 2 * 8192 ** 3 / (e0.elapsed_time(e1) * 1e-3) / 1e12
+        del a
+    # roofline denominator: the best FP64 rate measured on this device (DMMA shapes, DFMA, cuBLAS DGEMM)
+    peak = max(max(probe.values()), cublas_dgemm) or 1.0
 
     plan = T.Plan([s], mode=T.MODE_FUSED, rank=rank, world=world, device=local)
     plan.upload(stream=sp)
@@ -269,7 +277,7 @@ def run_b200_arm(args):
 
     # e2e through the C ABI with host buffers: H2D of every input + execute + D2H of the energies
     e2e_times = []
-    for it in range(args.warmup + args.steps):
+    for it in range(0 if args.profile else args.warmup + args.steps):
         torch.cuda.synchronize()
         barrier()
         t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -285,7 +293,7 @@ def run_b200_arm(args):
             el = float(tt.item())
         if it >= args.warmup:
             e2e_times.append(el)
-    e2e_value = n_all / statistics.mean(e2e_times)
+    e2e_value = n_all / statistics.mean(e2e_times) if e2e_times else None
     plan.close()
 
     # plain per-triple GPU path on a bounded sample of the same workload (1/16 of the triples)
@@ -335,8 +343,9 @@ def run_b200_arm(args):
         "emp4": e4[0], "emp5": e5[0],
         "roofline": {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
                      "frac": achieved / peak, "traffic": traffic,
-                     "peak_source": "measured live: library FP64 DMMA probe (best of m16n8k4/k8/k16, register "
-                                    "operands, 50 ms burst); MEASURED_PEAKS.json has no FP64 entry",
+                     "peak_source": "measured live on this device: max of the library's FP64 probes (DMMA "
+                                    "m16n8k4/k8/k16 and DFMA, register operands, 50 ms bursts) and cuBLAS DGEMM "
+                                    "8192^3; MEASURED_PEAKS.json has no FP64 entry",
                      "kernel_ms": kms},
         "fp64_probe_tflops": {"dmma_m16n8k4": probe[1], "dmma_m16n8k8": probe[2], "dmma_m16n8k16": probe[3],
                               "dfma": probe[4], "cublas_dgemm_8192": cublas_dgemm},

@@ -46,6 +46,7 @@ def parse():
     ap.add_argument("--nvir", type=int, default=NVIR)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-plain", action="store_true")
+    ap.add_argument("--mma-k", type=int, default=8, choices=[4, 8], help="FP64 MMA shape of the fused kernel")
     ap.add_argument("--profile", action="store_true",
                     help="fused steps only (no probes, e2e, plain or CPU legs): the command profiled with ncu")
     args = ap.parse_args()
@@ -230,7 +231,7 @@ def run_b200_arm(args):
     # roofline denominator: the best FP64 rate measured on this device (DMMA shapes, DFMA, cuBLAS DGEMM)
     peak = max(max(probe.values()), cublas_dgemm) or 1.0
 
-    plan = T.Plan([s], mode=T.MODE_FUSED, rank=rank, world=world, device=local)
+    plan = T.Plan([s], mode=T.MODE_FUSED, rank=rank, world=world, device=local, mma_k=args.mma_k)
     plan.upload(stream=sp)
     my_triples = plan.num_triples(0)
 
@@ -338,7 +339,8 @@ def run_b200_arm(args):
         "warmup": args.warmup, "ms_per_step": 1e3 * elapsed / args.steps, "higher_is_better": True,
         "scaling": "strong", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic (seeded counter-based generator, reference config distributions)",
-        "config": dict(wl, parallelism=f"triples sharded over {world} rank(s), one 2-double all-reduce per step"),
+        "config": dict(wl, parallelism=f"triples sharded over {world} rank(s), one 2-double all-reduce per step",
+                       mma=f"m16n8k{args.mma_k} f64"),
         "tflops_fp64_equiv": value * flop_triple / 1e12,
         "emp4": e4[0], "emp5": e5[0],
         "roofline": {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",

@@ -170,7 +170,8 @@ typedef struct trpdrv_options {
     int tile;         /* fused tile width (32 is the only compiled width); 0 = default */
     int ctas_per_sm;  /* fused persistent grid = ctas_per_sm * SM count; 0 = default */
     int use_graph;    /* capture trpdrv_plan_execute's launch sequence in a CUDA graph; default 1 */
-    int reserved[8];
+    int mma_k;        /* FP64 MMA shape of the fused kernel: 8 = m16n8k8 (default), 4 = m16n8k4 */
+    int reserved[7];
 } trpdrv_options;
 
 void trpdrv_options_default(trpdrv_options *opt);

@@ -200,6 +200,7 @@ void trpdrv_options_default(trpdrv_options *opt)
     opt->tile = 0;
     opt->ctas_per_sm = 0;
     opt->use_graph = 1;
+    opt->mma_k = 8;
 }
 
 static void plan_free(trpdrv_plan *p)
@@ -279,7 +280,8 @@ static int plan_build(trpdrv_plan *p, const trpdrv_system *shape)
             CUDA_TRY(cudaMalloc((void **)&b->rec, sizeof(double) * 4 * (size_t)b->ntriples));
             CUDA_TRY(cudaMemset(b->rec, 0, sizeof(double) * 4 * (size_t)b->ntriples));
             if (o->mode == TRPDRV_MODE_FUSED)
-                CUDA_TRY(cudaMalloc((void **)&b->partial, sizeof(double) * 4 * (size_t)b->ntriples * b->npairs));
+                CUDA_TRY(cudaMalloc((void **)&b->partial, sizeof(double) * 4 * TRPDRV_FUSED_SLOTS *
+                                                       (size_t)b->ntriples * b->npairs));
         }
         const size_t ov = (size_t)nocc * nocc * nvir;
         CUDA_TRY(cudaMalloc((void **)&b->ntov, sizeof(double) * ov));
@@ -345,6 +347,8 @@ int trpdrv_plan_create(trpdrv_plan **plan, const trpdrv_system *shape, int nsys,
     if (o.tile != 0 && o.tile != TRPDRV_TILE)
         return fail(TRPDRV_ERR_UNSUPPORTED, "tile %d: only %d is compiled", o.tile, TRPDRV_TILE);
     if (o.nkpass < 1) o.nkpass = 1;
+    if (o.mma_k == 0) o.mma_k = 8;
+    if (o.mma_k != 4 && o.mma_k != 8) return fail(TRPDRV_ERR_ARG, "mma_k %d: must be 4 or 8", o.mma_k);
     for (int q = 0; q < nsys; ++q) TRY(check_shape(&shape[q], q));
 
     int dev = 0, nsm = 0;
@@ -454,7 +458,7 @@ static int enqueue_fused(trpdrv_plan *p, cudaStream_t st, int capturing)
     CUDA_TRY(cudaEventRecordWithFlags(p->ev0, st, capturing ? cudaEventRecordExternal : cudaEventRecordDefault));
     if (p->total_items > 0) {
         LAUNCH_TRY(trpdrv_launch_fused(p->d_dev, p->nsys, p->total_items, p->d_counter, p->d_status, p->grid,
-                                       p->vec2, st));
+                                       p->vec2, p->opt.mma_k, st));
         ++launches;
     }
     CUDA_TRY(cudaEventRecordWithFlags(p->ev1, st, capturing ? cudaEventRecordExternal : cudaEventRecordDefault));

@@ -15,6 +15,8 @@ extern "C" {
 
 /* Width of the (b,c) tiles of the fused kernel and of the standalone tengy kernel. */
 #define TRPDRV_TILE 32
+/* Energy slots per fused work item (one per warp of the fused CTA). */
+#define TRPDRV_FUSED_SLOTS 8
 /* Triples are packed as (i-1) | (j-1) << 10 | (k-1) << 20 (0-based), so nocc must be < 1024. */
 #define TRPDRV_MAX_NOCC 1023
 /* Largest nvir the kernels accept (index arithmetic is 32-bit within one nvir x nvir block). */
@@ -30,14 +32,16 @@ typedef struct trpdrv_dev_system {
     int64_t item_begin;  /* first fused work item of this system */
     const double *eorb, *t2, *jvv, *kvv, *ntov, *nxov, *jov, *kov, *dintc, *dintx, *t1v;
     const int32_t *triples; /* packed triples, processing order */
-    double *partial;        /* [ntriples*npairs][4] per work item: e4i, e5i, e4k, e5k */
+    double *partial;        /* [ntriples*npairs][TRPDRV_FUSED_SLOTS][4]: e4i, e5i, e4k, e5k */
     double *rec;            /* [ntriples][4] per triple */
 } trpdrv_dev_system;
 
 /* Fused persistent kernel: grid CTAs pull (triple, tile pair) items from *counter (must be 0 at
- * launch) and write per-item energies.  vec2 = 1 requires even nvir and nocc for every system. */
+ * launch) and write per-item energies.  vec2 = 1 requires even nvir and nocc for every system;
+ * mma_k selects the FP64 MMA shape m16n8k4 (4) or m16n8k8 (8). */
 int trpdrv_launch_fused(const trpdrv_dev_system *d_sys, int nsys, int64_t total_items,
-                        unsigned long long *counter, int *status, int grid, int vec2, void *stream);
+                        unsigned long long *counter, int *status, int grid, int vec2, int mma_k,
+                        void *stream);
 size_t trpdrv_fused_smem_bytes(void);
 int trpdrv_fused_threads(void);
 int trpdrv_fused_max_ctas_per_sm(int *n);

@@ -18,33 +18,37 @@ template <int KIND>
 __global__ void __launch_bounds__(NTHREAD)
 probe_kernel(int iters, double *sink)
 {
-    const int lane = threadIdx.x & 31;
-    const double a0 = 1.0 + 1e-9 * lane, a1 = 1.0 - 1e-9 * lane, b0 = 0.5 + 1e-9 * threadIdx.x;
+    // every operand register distinct: repeated registers inside one MMA understate the rate
+    double a[8], b[4];
+#pragma unroll
+    for (int q = 0; q < 8; ++q) a[q] = 1.0 + 1e-9 * (threadIdx.x + q);
+#pragma unroll
+    for (int q = 0; q < 4; ++q) b[q] = 0.5 + 1e-9 * (threadIdx.x + 3 * q);
     double acc[NACC][4];
 #pragma unroll
     for (int q = 0; q < NACC; ++q)
 #pragma unroll
         for (int e = 0; e < 4; ++e) acc[q][e] = 0.0;
-    double a4[4] = {a0, a1, a0, a1}, b2[2] = {b0, b0};
-    double a8[8] = {a0, a1, a0, a1, a0, a1, a0, a1}, b4[4] = {b0, b0, b0, b0};
+    const double (&a4)[4] = *reinterpret_cast<const double(*)[4]>(a);
+    const double (&b2)[2] = *reinterpret_cast<const double(*)[2]>(b);
 
     for (int it = 0; it < iters; ++it) {
 #pragma unroll
         for (int q = 0; q < NACC; ++q) {
             if (KIND == 0) {
                 double d[2] = {acc[q][0], acc[q][1]};
-                dmma_8x8x4(d, a0, b0);
+                dmma_8x8x4(d, a[0], b[0]);
                 acc[q][0] = d[0];
                 acc[q][1] = d[1];
             } else if (KIND == 1) {
-                dmma_16x8x4(acc[q], a0, a1, b0);
+                dmma_16x8x4(acc[q], a[0], a[1], b[0]);
             } else if (KIND == 2) {
                 dmma_16x8x8(acc[q], a4, b2);
             } else if (KIND == 3) {
-                dmma_16x8x16(acc[q], a8, b4);
+                dmma_16x8x16(acc[q], a, b);
             } else {
 #pragma unroll
-                for (int e = 0; e < 4; ++e) asm volatile("fma.rn.f64 %0, %1, %2, %0;" : "+d"(acc[q][e]) : "d"(a0), "d"(b0));
+                for (int e = 0; e < 4; ++e) asm volatile("fma.rn.f64 %0, %1, %2, %0;" : "+d"(acc[q][e]) : "d"(a[e]), "d"(b[e]));
             }
         }
     }

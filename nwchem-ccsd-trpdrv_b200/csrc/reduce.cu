@@ -18,9 +18,10 @@ __global__ void item_reduce_kernel(const double *__restrict__ partial, int npair
     const long long t = (long long)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
     const int lane = threadIdx.x & 31;
     if (t >= ntriples) return;
-    const double *p = partial + 4 * t * (long long)npairs;
+    const int nslot = npairs * TRPDRV_FUSED_SLOTS;
+    const double *p = partial + 4 * t * (long long)nslot;
     double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
-    for (int q = lane; q < npairs; q += 32) {
+    for (int q = lane; q < nslot; q += 32) {
         s0 += p[4 * q + 0];
         s1 += p[4 * q + 1];
         s2 += p[4 * q + 2];

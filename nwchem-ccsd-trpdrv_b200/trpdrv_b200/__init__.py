@@ -55,7 +55,7 @@ class SystemStruct(C.Structure):
 class OptionsStruct(C.Structure):
     _fields_ = [("mode", C.c_int), ("nkpass", C.c_int), ("rank", C.c_int), ("world", C.c_int),
                 ("device", C.c_int), ("tile", C.c_int), ("ctas_per_sm", C.c_int),
-                ("use_graph", C.c_int), ("reserved", C.c_int * 8)]
+                ("use_graph", C.c_int), ("mma_k", C.c_int), ("reserved", C.c_int * 7)]
 
 
 def _proto(name, res, args):
@@ -279,11 +279,14 @@ def tengy(f8: np.ndarray, vecs: Sequence[np.ndarray], eorb: np.ndarray, eaijk: f
 # --------------------------------------------------------------------------------------------
 # plans
 # --------------------------------------------------------------------------------------------
-def options(mode=MODE_FUSED, nkpass=1, rank=0, world=1, device=-1, ctas_per_sm=0, use_graph=1) -> OptionsStruct:
+def options(mode=MODE_FUSED, nkpass=1, rank=0, world=1, device=-1, ctas_per_sm=0, use_graph=1,
+            mma_k=0) -> OptionsStruct:
     o = OptionsStruct()
     lib.trpdrv_options_default(C.byref(o))
     o.mode, o.nkpass, o.rank, o.world, o.device = mode, nkpass, rank, world, device
     o.ctas_per_sm, o.use_graph = ctas_per_sm, use_graph
+    if mma_k:
+        o.mma_k = mma_k
     return o
 
 

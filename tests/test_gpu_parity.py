@@ -17,7 +17,7 @@ from kat import run_make_array_loop
 
 pytestmark = pytest.mark.gpu
 
-MODES = {"fused": 1, "plain": 0}
+MODES = {"fused": dict(mode=1, mma_k=8), "fused_k4": dict(mode=1, mma_k=4), "plain": dict(mode=0)}
 
 
 def _plan_run(T, systems, **opt):
@@ -35,7 +35,7 @@ def _plan_run(T, systems, **opt):
 def test_plan_matches_reference_golden(T, name, mode):
     g = load_golden(name)
     s = system_from_golden(g)
-    e4, e5, recs, launches = _plan_run(T, [s], mode=MODES[mode], nkpass=g["nkpass"])
+    e4, e5, recs, launches = _plan_run(T, [s], nkpass=g["nkpass"], **MODES[mode])
     assert launches > 0
     assert_records_close(recs[0], g["records"])
     assert_total_close(e4[0], g["emp4"], what="emp4")
@@ -120,8 +120,8 @@ def test_fused_and_plain_match_reference_odd_shapes(T, O, nocc, nvir, seed, ncor
     s = T.synth_system(nocc, nvir, seed=seed, ncor=ncor)
     rec_ref, tot_ref, mism = O.run_system(s, "reference", nthreads=8)
     assert mism == 0
-    for mode in (1, 0):
-        e4, e5, recs, _ = _plan_run(T, [s], mode=mode)
+    for opt in MODES.values():
+        e4, e5, recs, _ = _plan_run(T, [s], **opt)
         assert_records_close(recs[0], rec_ref)
         assert_total_close(e4[0], tot_ref[0], what="emp4")
         assert_total_close(e5[0], tot_ref[1], what="emp5")

@@ -170,8 +170,11 @@ typedef struct trpdrv_options {
     int tile;         /* fused tile width (32 is the only compiled width); 0 = default */
     int ctas_per_sm;  /* fused persistent grid = ctas_per_sm * SM count; 0 = default */
     int use_graph;    /* capture trpdrv_plan_execute's launch sequence in a CUDA graph; default 1 */
-    int mma_k;        /* FP64 MMA shape of the fused kernel: 8 = m16n8k8 (default), 4 = m16n8k4 */
-    int reserved[7];
+    int mma_k;        /* FP64 MMA shape of the cp.async fused kernel: 8 = m16n8k8 (default), 4 = m16n8k4 */
+    int staging;      /* fused-kernel operand staging: 0 = TMA where supported (even nvir and nocc,
+                         16-byte aligned tensors, <= 8 systems), else cp.async; 1 = cp.async; 2 = TMA
+                         or fail with TRPDRV_ERR_UNSUPPORTED */
+    int reserved[6];
 } trpdrv_options;
 
 void trpdrv_options_default(trpdrv_options *opt);
@@ -198,6 +201,9 @@ int64_t trpdrv_plan_num_triples(const trpdrv_plan *plan, int sys);
 int trpdrv_plan_triples(const trpdrv_plan *plan, int sys, int32_t *ijk);
 /* Per-triple records of system `sys` after a job: rec[4*t..] = emp4i, emp5i, emp4k, emp5k. */
 int trpdrv_plan_triple_energies(trpdrv_plan *plan, int sys, double *rec);
+/* Operand staging the plan's fused kernel uses: 1 = cp.async, 2 = TMA (0 for plain plans or
+ * before data is bound). */
+int trpdrv_plan_staging(const trpdrv_plan *plan);
 /* Kernel launches the last execute enqueued (for launch accounting). */
 int64_t trpdrv_plan_last_launches(const trpdrv_plan *plan);
 /* Device-time (ms) of the last execute's main kernel(s), measured with events on the plan stream. */

@@ -1,0 +1,528 @@
+// Fused persistent triples kernel, TMA + mbarrier pipeline (sm_100a, FP64 DMMA).
+//
+// Same work decomposition and register-resident energy epilogue as fused.cu (a work item is
+// (triple, tile pair {B,C}); each consumer warp owns a 16(b) x 8(c) sub-block and computes all eight
+// f of omp/ccsd_trpdrv_omp_cbody.c:70-117 at (b,c) and, through the operand-swapped MMA, at (c,b)),
+// but the operand panels are staged by the Tensor Memory Accelerator:
+//
+//  * one producer thread takes work tickets, writes each item's context to a ring in shared memory
+//    and issues, per chunk of DK contraction indices, one or two cp.async.bulk.tensor loads per
+//    panel (no cluster multicast) that complete on the stage's "full" mbarrier;
+//  * eight consumer warps wait on "full", run the m16n8k8 DMMAs straight from the staged panels and
+//    release the stage through its "empty" mbarrier; no CTA-wide barrier in the main loop.
+//
+// Panel layouts in shared memory (2 KB per panel, 16 panels per stage):
+//  * K-major panels (rows contiguous in HBM: Jia/Kia/Jka/Kka, -Tia/-Xia/-Tka/-Xka, T2 as T(c,d)):
+//    two 16-row boxes of [DK][16] doubles written with the 128-byte swizzle, which makes the
+//    k-permuted fragment reads bank-conflict free;
+//  * X-major panels (contraction contiguous: T2 as T(d,c), Jkj/Kkj/Jij/Kij): one [32][DK] box,
+//    read with 128-bit loads, conflict free without swizzle.
+// The 3-D tensor maps ([system block][contraction][row]) give every dimension its own bound, so the
+// ragged tails in nvir and nocc are zero-filled by the TMA unit.
+//
+// Every wait is bounded (globaltimer); a wait that runs out sets bit 1 of *status and the CTA stops
+// issuing work.  Requires even nvir and nocc and 16-byte aligned tensors (host checks).
+
+#include <cuda.h>
+#include <cudaTypedefs.h>
+
+#include "device_common.cuh"
+#include "launch.h"
+
+namespace trpdrv {
+namespace tma {
+
+constexpr int T = TRPDRV_TILE;  // 32
+constexpr int DK = 8;           // contraction indices per stage
+constexpr int STAGES = 6;
+constexpr int NCW = TRPDRV_FUSED_SLOTS;  // consumer warps (8) = two warpgroups
+constexpr int NTHREAD = (NCW + 4) * 32;  // + one producer warpgroup (one thread issues)
+// Register split by setmaxnreg: launched at 65536 / 384 = 168 per thread; the producer warpgroup
+// drops to 40 and the two consumer warpgroups rise to 232:  2*128*232 + 128*40 = 64512 = 384*168.
+constexpr int REG_LAUNCH = 168, REG_CONSUMER = 232, REG_PRODUCER = 40;
+static_assert(2 * 128 * REG_CONSUMER + 128 * REG_PRODUCER <= NTHREAD * REG_LAUNCH, "register split exceeds the launch");
+constexpr int PANEL_BYTES = 2048;
+constexpr int NPANEL = 16;
+constexpr int STAGE_BYTES = NPANEL * PANEL_BYTES;
+constexpr int RING = 16;
+constexpr size_t SMEM_BYTES = (size_t)STAGES * STAGE_BYTES + 1024;  // + alignment slack
+constexpr unsigned long long WAIT_LIMIT_NS = 4000000000ull;       // 4 s: far above any legitimate wait
+
+static_assert(RING >= STAGES + 2, "context ring too small");
+
+enum { M_J = 0, M_K, M_NT, M_NX, M_T2K, M_T2X, M_JOV, M_KOV, NMAP };
+
+struct __align__(64) Maps {
+    CUtensorMap m[TRPDRV_TMA_MAX_SYSTEMS][NMAP];
+};
+
+struct ItemCtx {
+    const double *eorb, *dintc1, *dintx1, *t1v1, *dintc2, *dintx2, *t1v2;
+    double *out;
+    double eaijk;
+    int ncor, nocc, nvir, b0, c0, diag, nV, nch, state;  // state: 1 work, 0 malformed, -1 end
+};
+
+// ------------------------------------------------------------------------------------------------
+// PTX helpers
+// ------------------------------------------------------------------------------------------------
+__device__ __forceinline__ unsigned saddr(const void *p) { return (unsigned)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ unsigned long long globaltimer()
+{
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+__device__ __forceinline__ void mbar_init(unsigned long long *b, unsigned count)
+{
+    asm volatile("mbarrier.init.shared.b64 [%0], %1;" ::"r"(saddr(b)), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive_expect_tx(unsigned long long *b, unsigned bytes)
+{
+    asm volatile("mbarrier.arrive.expect_tx.shared.b64 _, [%0], %1;" ::"r"(saddr(b)), "r"(bytes) : "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive(unsigned long long *b)
+{
+    asm volatile("mbarrier.arrive.shared.b64 _, [%0];" ::"r"(saddr(b)) : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(unsigned long long *b, unsigned parity)
+{
+    unsigned ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(ok)
+        : "r"(saddr(b)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+
+// Bounded wait for the phase with the given parity; false (and status bit 1) when it runs out.
+__device__ __forceinline__ bool mbar_wait(unsigned long long *b, unsigned parity, int *status)
+{
+    if (mbar_try_wait(b, parity)) return true;
+    const unsigned long long t0 = globaltimer();
+    for (;;) {
+        if (mbar_try_wait(b, parity)) return true;
+        if (globaltimer() - t0 > WAIT_LIMIT_NS) {
+            atomicOr(status, 2);
+            return false;
+        }
+    }
+}
+
+__device__ __forceinline__ void tma_load_3d(void *dst, const CUtensorMap *map, unsigned long long *bar, int x, int y,
+                                            int z)
+{
+    asm volatile(
+        "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4, %5}], [%2];"
+        ::"r"(saddr(dst)), "l"(map), "r"(saddr(bar)), "r"(x), "r"(y), "r"(z)
+        : "memory");
+}
+
+// ------------------------------------------------------------------------------------------------
+// fragments (m16n8k8, lane t holds logical k = t and t+4 at physical kk = 2t, 2t+1)
+// ------------------------------------------------------------------------------------------------
+// K-major swizzled panel: element (kk, x) of a panel at byte base P
+__device__ __forceinline__ double kel(const char *P, int kk, int x)
+{
+    const int h = x >> 4, xi = x & 15;
+    return *reinterpret_cast<const double *>(P + h * 1024 + kk * 128 + ((((xi >> 1) ^ kk)) << 4) + ((xi & 1) << 3));
+}
+
+__device__ __forceinline__ void ldA(double (&a)[4], const char *P, bool km, int x0, int g, int t)
+{
+    const int kk = 2 * t;
+    if (km) {
+        a[0] = kel(P, kk, x0 + g);
+        a[1] = kel(P, kk, x0 + g + 8);
+        a[2] = kel(P, kk + 1, x0 + g);
+        a[3] = kel(P, kk + 1, x0 + g + 8);
+    } else {
+        const double2 lo = *reinterpret_cast<const double2 *>(P + (x0 + g) * (DK * 8) + kk * 8);
+        const double2 hi = *reinterpret_cast<const double2 *>(P + (x0 + g + 8) * (DK * 8) + kk * 8);
+        a[0] = lo.x;
+        a[2] = lo.y;
+        a[1] = hi.x;
+        a[3] = hi.y;
+    }
+}
+
+__device__ __forceinline__ void ldB(double (&b)[2], const char *P, bool km, int x0, int g, int t)
+{
+    const int kk = 2 * t;
+    if (km) {
+        b[0] = kel(P, kk, x0 + g);
+        b[1] = kel(P, kk + 1, x0 + g);
+    } else {
+        const double2 v = *reinterpret_cast<const double2 *>(P + (x0 + g) * (DK * 8) + kk * 8);
+        b[0] = v.x;
+        b[1] = v.y;
+    }
+}
+
+// ------------------------------------------------------------------------------------------------
+// energies of one warp's sub-block, in registers (as fused.cu)
+// ------------------------------------------------------------------------------------------------
+__device__ __forceinline__ void warp_epilogue(const ItemCtx &cx, const double (&f)[8][4], const double (&gT)[8][4],
+                                              int rb0, int cb0, int g, int t, int lane, double *out)
+{
+    TengySums su = {0.0, 0.0, 0.0, 0.0};
+    const int V = cx.nvir, voff = cx.ncor + cx.nocc;
+    const double eaijk = cx.eaijk;
+#pragma unroll
+    for (int e = 0; e < 4; ++e) {
+        const int b = rb0 + g + ((e & 2) ? 8 : 0);
+        const int c = cb0 + 2 * t + (e & 1);
+        if (b < V && c < V) {
+            double fbc[8], fcb[8];
+#pragma unroll
+            for (int x = 0; x < 8; ++x) {
+                fbc[x] = f[x][e];
+                fcb[x] = gT[x][e];
+            }
+            const double eb = __ldg(cx.eorb + voff + b), ec = __ldg(cx.eorb + voff + c);
+            // term at (b,c): omp/ccsd_tengy_c99.c:65 denominator, :91-111 forms
+            tengy_term(fbc, fcb, -1.0 / (eb + ec + eaijk), __ldg(cx.t1v1 + b), __ldg(cx.t1v2 + b),
+                       __ldg(cx.dintx1 + c), __ldg(cx.dintx2 + c), __ldg(cx.dintc1 + c), __ldg(cx.dintc2 + c), su);
+            if (!cx.diag)  // term at (c,b) of the mirrored tile
+                tengy_term(fcb, fbc, -1.0 / (ec + eb + eaijk), __ldg(cx.t1v1 + c), __ldg(cx.t1v2 + c),
+                           __ldg(cx.dintx1 + b), __ldg(cx.dintx2 + b), __ldg(cx.dintc1 + b), __ldg(cx.dintc2 + b),
+                           su);
+        }
+    }
+    su.e4i = warp_sum(su.e4i);
+    su.e5i = warp_sum(su.e5i);
+    su.e4k = warp_sum(su.e4k);
+    su.e5k = warp_sum(su.e5k);
+    if (lane == 0 && out) {
+        out[0] = su.e4i;
+        out[1] = su.e5i;
+        out[2] = su.e4k;
+        out[3] = su.e5k;
+    }
+}
+
+// ------------------------------------------------------------------------------------------------
+// producer: tickets, item contexts, TMA loads
+// ------------------------------------------------------------------------------------------------
+__device__ __forceinline__ void producer(const trpdrv_dev_system *__restrict__ sys, int nsys, long long total,
+                                         unsigned long long *counter, int *status, const Maps &maps, char *stages,
+                                         unsigned long long *full, unsigned long long *empty, ItemCtx *ring)
+{
+    int stage = 0;
+    unsigned phase = 0;  // parity of the current pass over the stages
+    long long n = 0;     // items produced
+    long long next = (long long)atomicAdd(counter, 1ULL);
+    for (;; ++n) {
+        const long long item = next;
+        if (item < total) next = (long long)atomicAdd(counter, 1ULL);  // ticket for the following item
+        ItemCtx &cx = ring[n % RING];
+        if (item >= total) {
+            if (!mbar_wait(&empty[stage], phase ^ 1, status)) return;
+            cx.state = -1;
+            mbar_arrive(&full[stage]);
+            return;
+        }
+        int s = 0;
+        while (s + 1 < nsys && item >= sys[s + 1].item_begin) ++s;
+        const trpdrv_dev_system &S = sys[s];
+        const long long local = item - S.item_begin;
+        const long long tt = local / S.npairs;
+        const int p = (int)(local - tt * S.npairs);
+        int B = 0, rem = p;
+        while (B < S.nb && rem >= S.nb - B) {
+            rem -= S.nb - B;
+            ++B;
+        }
+        const int C = B + rem;
+        const int O = S.nocc, V = S.nvir;
+        const bool in_range = local >= 0 && tt < S.ntriples;
+        const int packed = in_range ? S.triples[tt] : 0;
+        const int i = packed & 1023, j = (packed >> 10) & 1023, k = (packed >> 20) & 1023;
+        const bool ok = in_range && B < S.nb && C < S.nb && i < O && j < O && k < O && k <= i && s < TRPDRV_TMA_MAX_SYSTEMS;
+        const int B0 = B * T, C0 = C * T;
+        if (!ok) {
+            atomicOr(status, 1);
+            if (!mbar_wait(&empty[stage], phase ^ 1, status)) return;
+            cx.state = 0;
+            cx.out = in_range ? S.partial + (size_t)local * NCW * 4 : nullptr;
+            cx.nch = 0;
+            mbar_arrive(&full[stage]);
+            if (++stage == STAGES) {
+                stage = 0;
+                phase ^= 1;
+            }
+            continue;
+        }
+        cx.eorb = S.eorb;
+        cx.dintc1 = S.dintc + (size_t)i * V;
+        cx.dintx1 = S.dintx + (size_t)i * V;
+        cx.t1v1 = S.t1v + (size_t)i * V;
+        cx.dintc2 = S.dintc + (size_t)k * V;
+        cx.dintx2 = S.dintx + (size_t)k * V;
+        cx.t1v2 = S.t1v + (size_t)k * V;
+        cx.out = S.partial + (size_t)local * NCW * 4;
+        // omp/ccsd_trpdrv_omp_cbody.c:126 (a is 1-based, i/j/k here 0-based)
+        cx.eaijk = S.eorb[S.a - 1] - (S.eorb[S.ncor + i] + S.eorb[S.ncor + j] + S.eorb[S.ncor + k]);
+        cx.ncor = S.ncor;
+        cx.nocc = O;
+        cx.nvir = V;
+        cx.b0 = B0;
+        cx.c0 = C0;
+        cx.diag = (B == C);
+        const int nV = (V + DK - 1) / DK, nO = (O + DK - 1) / DK;
+        cx.nV = nV;
+        cx.nch = nV + nO;
+        cx.state = 1;
+
+        const CUtensorMap *mp = maps.m[s];
+        const int zjk = j * O + k, zji = j * O + i;
+        const bool diag = (B == C);
+        const unsigned bytes = (diag ? NPANEL / 2 : NPANEL) * PANEL_BYTES;
+        for (int ch = 0; ch < nV + nO; ++ch) {
+            if (!mbar_wait(&empty[stage], phase ^ 1, status)) return;
+            mbar_arrive_expect_tx(&full[stage], bytes);
+            char *st = stages + (size_t)stage * STAGE_BYTES;
+            const bool ph1 = ch >= nV;
+            const int kk0 = (ph1 ? ch - nV : ch) * DK;
+#pragma unroll 1
+            for (int fam = 0; fam < 2; ++fam) {
+                const int za = fam ? k : i;      // A operands: Jia/Kia (n), Jka/Kka (t)
+                const int zb = fam ? zji : zjk;  // B operands: Tkj/Kkj/Jkj (n), Tij/Kij/Jij (t)
+                char *P = st + fam * 8 * PANEL_BYTES;
+                const CUtensorMap *mA_J = &mp[ph1 ? M_NT : M_J];
+                const CUtensorMap *mA_K = &mp[ph1 ? M_NX : M_K];
+#pragma unroll 1
+                for (int o = 0; o < (diag ? 1 : 2); ++o) {
+                    const int ra = o ? C0 : B0;  // A rows: B for (B,C), C for (C,B)
+                    const int cb = o ? B0 : C0;  // B columns: C for (B,C), B for (C,B)
+                    // A_J / A_K rows: K-major, two 16-row boxes
+                    tma_load_3d(P + (0 + o) * PANEL_BYTES, mA_J, &full[stage], ra, kk0, za);
+                    tma_load_3d(P + (0 + o) * PANEL_BYTES + 1024, mA_J, &full[stage], ra + 16, kk0, za);
+                    tma_load_3d(P + (2 + o) * PANEL_BYTES, mA_K, &full[stage], ra, kk0, za);
+                    tma_load_3d(P + (2 + o) * PANEL_BYTES + 1024, mA_K, &full[stage], ra + 16, kk0, za);
+                    // B_1 columns: T(c,d) K-major in the virtual phase, K(m,c) X-major in the occupied one
+                    if (!ph1) {
+                        tma_load_3d(P + (4 + o) * PANEL_BYTES, &mp[M_T2K], &full[stage], cb, kk0, zb);
+                        tma_load_3d(P + (4 + o) * PANEL_BYTES + 1024, &mp[M_T2K], &full[stage], cb + 16, kk0, zb);
+                    } else {
+                        tma_load_3d(P + (4 + o) * PANEL_BYTES, &mp[M_KOV], &full[stage], kk0, cb, zb);
+                    }
+                    // B_3 columns: T(d,c) / J(m,c), X-major in both phases
+                    tma_load_3d(P + (6 + o) * PANEL_BYTES, &mp[ph1 ? M_JOV : M_T2X], &full[stage], kk0, cb, zb);
+                }
+            }
+            if (++stage == STAGES) {
+                stage = 0;
+                phase ^= 1;
+            }
+        }
+    }
+}
+
+// ------------------------------------------------------------------------------------------------
+__global__ void __launch_bounds__(NTHREAD, 1)
+fused_tma_kernel(const trpdrv_dev_system *__restrict__ sys, int nsys, long long total, unsigned long long *counter,
+                 int *status, const __grid_constant__ Maps maps)
+{
+    extern __shared__ char smem_raw[];
+    __shared__ __align__(8) unsigned long long full[STAGES], empty[STAGES];
+    __shared__ ItemCtx ring[RING];
+    char *stages = reinterpret_cast<char *>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~(uintptr_t)1023);
+
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    if (tid == 0) {
+        for (int s = 0; s < STAGES; ++s) {
+            mbar_init(&full[s], 1);
+            mbar_init(&empty[s], NCW);
+        }
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+
+    if (warp >= NCW) {  // producer warpgroup: one thread issues everything
+        asm volatile("setmaxnreg.dec.sync.aligned.u32 %0;" ::"n"(REG_PRODUCER));
+        if (warp == NCW && lane == 0) producer(sys, nsys, total, counter, status, maps, stages, full, empty, ring);
+        return;
+    }
+    asm volatile("setmaxnreg.inc.sync.aligned.u32 %0;" ::"n"(REG_CONSUMER));
+
+    const int g = lane >> 2, t = lane & 3;
+    // sub-block: rows (b) rs*16.., columns (c) cs*8..; warps w and w+4 share a scheduler and differ in both
+    const int rs = warp >> 2, cs = (warp & 3) ^ (rs << 1);
+    const int rx0 = rs * 16, cx0 = cs * 8;
+
+    double f[8][4], gT[8][4];
+    int stage = 0;
+    unsigned phase = 0;
+    for (long long n = 0;; ++n) {
+        if (!mbar_wait(&full[stage], phase, status)) return;
+        const ItemCtx &cx = ring[n % RING];
+        const int state = cx.state;
+        if (state < 0) return;
+        if (state == 0) {
+            if (lane == 0 && cx.out) {
+                double *o = cx.out + warp * 4;
+                o[0] = o[1] = o[2] = o[3] = 0.0;
+            }
+            __syncwarp();
+            if (lane == 0) mbar_arrive(&empty[stage]);
+            if (++stage == STAGES) {
+                stage = 0;
+                phase ^= 1;
+            }
+            continue;
+        }
+#pragma unroll
+        for (int x = 0; x < 8; ++x)
+#pragma unroll
+            for (int e = 0; e < 4; ++e) f[x][e] = gT[x][e] = 0.0;
+        const int nch = cx.nch, nV = cx.nV;
+        const bool active = (cx.b0 + rx0 < cx.nvir) && (cx.c0 + cx0 < cx.nvir);
+        const int o1 = cx.diag ? 0 : 1;  // diagonal pair: the C panels are the B panels
+        for (int ch = 0; ch < nch; ++ch) {
+            if (ch > 0 && !mbar_wait(&full[stage], phase, status)) return;
+            const char *st = stages + (size_t)stage * STAGE_BYTES;
+            const bool ph1 = ch >= nV;
+            if (active) {
+#pragma unroll
+                for (int fam = 0; fam < 2; ++fam) {
+                    const char *P = st + fam * 8 * PANEL_BYTES;
+                    double aJ[4], aK[4], a1[4], a3[4], bJ[2], bK[2], b1[2], b3[2];
+                    ldA(aJ, P + 0 * PANEL_BYTES, true, rx0, g, t);
+                    ldA(aK, P + 2 * PANEL_BYTES, true, rx0, g, t);
+                    ldB(bJ, P + (0 + o1) * PANEL_BYTES, true, cx0, g, t);
+                    ldB(bK, P + (2 + o1) * PANEL_BYTES, true, cx0, g, t);
+                    ldB(b1, P + 4 * PANEL_BYTES, !ph1, cx0, g, t);
+                    ldB(b3, P + 6 * PANEL_BYTES, false, cx0, g, t);
+                    ldA(a1, P + (4 + o1) * PANEL_BYTES, !ph1, rx0, g, t);
+                    ldA(a3, P + (6 + o1) * PANEL_BYTES, false, rx0, g, t);
+                    const int x0 = fam * 4;
+                    // f1 = A_J B_1, f2 = A_K B_1, f3 = A_J B_3, f4 = A_K B_3
+                    dmma_16x8x8(f[x0 + 0], aJ, b1);
+                    dmma_16x8x8(f[x0 + 1], aK, b1);
+                    dmma_16x8x8(f[x0 + 2], aJ, b3);
+                    dmma_16x8x8(f[x0 + 3], aK, b3);
+                    // transposes: f_x(c,b) = sum_d B_x(d,b) A_x(c,d)
+                    dmma_16x8x8(gT[x0 + 0], a1, bJ);
+                    dmma_16x8x8(gT[x0 + 1], a1, bK);
+                    dmma_16x8x8(gT[x0 + 2], a3, bJ);
+                    dmma_16x8x8(gT[x0 + 3], a3, bK);
+                }
+            }
+            __syncwarp();
+            if (lane == 0) mbar_arrive(&empty[stage]);
+            if (++stage == STAGES) {
+                stage = 0;
+                phase ^= 1;
+            }
+        }
+        warp_epilogue(cx, f, gT, cx.b0 + rx0, cx.c0 + cx0, g, t, lane, cx.out + warp * 4);
+    }
+}
+
+// ------------------------------------------------------------------------------------------------
+// host side: tensor maps
+// ------------------------------------------------------------------------------------------------
+static PFN_cuTensorMapEncodeTiled_v12000 encode_fn()
+{
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    if (!fn) {
+        void *p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+    }
+    return fn;
+}
+
+// 3-D map over doubles: dims {d0 (contiguous), d1, d2}, box {b0, b1, 1}
+static int make_map(CUtensorMap *m, const double *base, unsigned long long d0, unsigned long long d1,
+                    unsigned long long d2, unsigned b0, unsigned b1, bool swizzle)
+{
+    PFN_cuTensorMapEncodeTiled_v12000 fn = encode_fn();
+    if (!fn) return 1;
+    const cuuint64_t dims[3] = {d0, d1, d2};
+    const cuuint64_t strides[2] = {d0 * 8ull, d0 * d1 * 8ull};
+    const cuuint32_t box[3] = {b0, b1, 1};
+    const cuuint32_t estr[3] = {1, 1, 1};
+    const CUresult r = fn(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3, const_cast<double *>(base), dims, strides, box, estr,
+                          CU_TENSOR_MAP_INTERLEAVE_NONE,
+                          swizzle ? CU_TENSOR_MAP_SWIZZLE_128B : CU_TENSOR_MAP_SWIZZLE_NONE,
+                          CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    return r == CUDA_SUCCESS ? 0 : 2;
+}
+
+}  // namespace tma
+}  // namespace trpdrv
+
+using namespace trpdrv;
+
+extern "C" size_t trpdrv_tma_maps_bytes(void) { return sizeof(tma::Maps); }
+
+// Registers per thread the kernel is launched with (read back at init).  The setmaxnreg split is
+// only valid when this equals REG_LAUNCH: with fewer, the consumers' increase could never be met.
+static int g_launch_regs = -1;
+
+extern "C" int trpdrv_tma_supported(const trpdrv_dev_system *h_sys, int nsys)
+{
+    if (g_launch_regs != tma::REG_LAUNCH) return 0;
+    if (nsys > TRPDRV_TMA_MAX_SYSTEMS || !tma::encode_fn()) return 0;
+    for (int s = 0; s < nsys; ++s) {
+        const trpdrv_dev_system &S = h_sys[s];
+        if ((S.nvir & 1) || (S.nocc & 1)) return 0;  // row strides must be multiples of 16 bytes
+        const void *p[] = {S.t2, S.jvv, S.kvv, S.ntov, S.nxov, S.jov, S.kov};
+        for (const void *q : p)
+            if (((uintptr_t)q) & 15u) return 0;
+    }
+    return 1;
+}
+
+extern "C" int trpdrv_tma_prepare(const trpdrv_dev_system *h_sys, int nsys, void *maps_out)
+{
+    tma::Maps *M = static_cast<tma::Maps *>(maps_out);
+    memset(M, 0, sizeof(*M));
+    for (int s = 0; s < nsys && s < TRPDRV_TMA_MAX_SYSTEMS; ++s) {
+        const trpdrv_dev_system &S = h_sys[s];
+        const unsigned long long V = S.nvir, O = S.nocc, O2 = O * O;
+        CUtensorMap *m = M->m[s];
+        int e = 0;
+        e |= tma::make_map(&m[tma::M_J], S.jvv, V, V, O, 16, tma::DK, true);    // [i][d][b]
+        e |= tma::make_map(&m[tma::M_K], S.kvv, V, V, O, 16, tma::DK, true);
+        e |= tma::make_map(&m[tma::M_NT], S.ntov, V, O, O, 16, tma::DK, true);  // [i][m][b]
+        e |= tma::make_map(&m[tma::M_NX], S.nxov, V, O, O, 16, tma::DK, true);
+        e |= tma::make_map(&m[tma::M_T2K], S.t2, V, V, O2, 16, tma::DK, true);  // [jx][d][c]: T(c,d)
+        e |= tma::make_map(&m[tma::M_T2X], S.t2, V, V, O2, tma::DK, 32, false); // [jx][c][d]: T(d,c)
+        e |= tma::make_map(&m[tma::M_JOV], S.jov, O, V, O2, tma::DK, 32, false);  // [jx][c][m]
+        e |= tma::make_map(&m[tma::M_KOV], S.kov, O, V, O2, tma::DK, 32, false);
+        if (e) return e;
+    }
+    return 0;
+}
+
+extern "C" int trpdrv_launch_fused_tma(const trpdrv_dev_system *d_sys, int nsys, int64_t total_items,
+                                       unsigned long long *counter, int *status, int grid, const void *maps,
+                                       void *stream)
+{
+    if (grid <= 0 || total_items <= 0) return 0;
+    if (g_launch_regs != tma::REG_LAUNCH) return (int)cudaErrorInvalidConfiguration;
+    tma::fused_tma_kernel<<<grid, tma::NTHREAD, tma::SMEM_BYTES, (cudaStream_t)stream>>>(
+        d_sys, nsys, total_items, counter, status, *static_cast<const tma::Maps *>(maps));
+    return (int)cudaGetLastError();
+}
+
+extern "C" int trpdrv_fused_tma_init(void)
+{
+    cudaFuncAttributes fa;
+    cudaError_t e = cudaFuncGetAttributes(&fa, tma::fused_tma_kernel);
+    if (e != cudaSuccess) return (int)e;
+    g_launch_regs = fa.numRegs;
+    return (int)cudaFuncSetAttribute(tma::fused_tma_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)tma::SMEM_BYTES);
+}

@@ -109,6 +109,7 @@ static int ensure_device(int device, int *out_dev, int *out_nsm)
     int rc = 0;
     if (!g_init_done[dev]) {
         rc = trpdrv_fused_init();
+        if (!rc) rc = trpdrv_fused_tma_init();
         if (!rc) rc = trpdrv_plain_init();
         if (!rc) g_init_done[dev] = 1;
     }
@@ -168,7 +169,7 @@ typedef struct sysbuf {
 } sysbuf;
 
 struct trpdrv_plan {
-    int nsys, device, nsm, grid, vec2, bound;
+    int nsys, device, nsm, grid, grid_tma, vec2, bound;
     trpdrv_options opt;
     cudaStream_t stream;
     sysbuf *s;
@@ -186,6 +187,8 @@ struct trpdrv_plan {
     int events_valid;
     int64_t last_launches;
     cudaStream_t last_stream;
+    int use_tma;        /* the fused launch stages panels with TMA (fused_tma.cu) */
+    void *tma_maps;     /* tensor maps of every system, passed by value to each launch */
 };
 
 void trpdrv_options_default(trpdrv_options *opt)
@@ -223,6 +226,7 @@ static void plan_free(trpdrv_plan *p)
         free(p->s);
     }
     free(p->h_dev);
+    free(p->tma_maps);
     if (p->d_dev) cudaFree(p->d_dev);
     if (p->d_counter) cudaFree(p->d_counter);
     if (p->d_status) cudaFree(p->d_status);
@@ -327,6 +331,9 @@ static int plan_build(trpdrv_plan *p, const trpdrv_system *shape)
     int64_t grid = (int64_t)per_sm * p->nsm;
     if (grid > p->total_items) grid = p->total_items;
     p->grid = (int)(grid > 0 ? grid : 0);
+    int64_t grid_tma = p->nsm; /* fused_tma.cu: one CTA per SM */
+    if (grid_tma > p->total_items) grid_tma = p->total_items;
+    p->grid_tma = (int)(grid_tma > 0 ? grid_tma : 0);
     return TRPDRV_OK;
 }
 
@@ -349,6 +356,7 @@ int trpdrv_plan_create(trpdrv_plan **plan, const trpdrv_system *shape, int nsys,
     if (o.nkpass < 1) o.nkpass = 1;
     if (o.mma_k == 0) o.mma_k = 8;
     if (o.mma_k != 4 && o.mma_k != 8) return fail(TRPDRV_ERR_ARG, "mma_k %d: must be 4 or 8", o.mma_k);
+    if (o.staging < 0 || o.staging > 2) return fail(TRPDRV_ERR_ARG, "staging %d: must be 0, 1 or 2", o.staging);
     for (int q = 0; q < nsys; ++q) TRY(check_shape(&shape[q], q));
 
     int dev = 0, nsm = 0;
@@ -390,6 +398,30 @@ static int plan_publish(trpdrv_plan *p)
         const size_t ov = (size_t)b->shape.nocc * b->shape.nocc * b->shape.nvir;
         LAUNCH_TRY(trpdrv_launch_negate(b->t[TRPDRV_T_TOV], b->ntov, ov, p->stream));
         LAUNCH_TRY(trpdrv_launch_negate(b->t[TRPDRV_T_XOV], b->nxov, ov, p->stream));
+    }
+    if (p->opt.mode == TRPDRV_MODE_FUSED) {
+        const int want = p->opt.staging;
+        const int ok = want != 1 && trpdrv_tma_supported(p->h_dev, p->nsys);
+        if (want == 2 && !ok)
+            return fail(TRPDRV_ERR_UNSUPPORTED, "TMA staging needs even nvir and nocc, 16-byte aligned tensors "
+                                                "and at most %d systems", TRPDRV_TMA_MAX_SYSTEMS);
+        if (ok) {
+            if (!p->tma_maps) {
+                p->tma_maps = aligned_alloc(64, (trpdrv_tma_maps_bytes() + 63) & ~(size_t)63);
+                if (!p->tma_maps) return fail(TRPDRV_ERR_NOMEM, "host allocation failed");
+            }
+            const int e = trpdrv_tma_prepare(p->h_dev, p->nsys, p->tma_maps);
+            if (e) return fail(TRPDRV_ERR_CUDA, "tensor-map encoding failed (%d)", e);
+        }
+        p->use_tma = ok;
+        /* a captured graph holds the previous launch parameters */
+        if (p->graph_ready) {
+            cudaGraphExecDestroy(p->gexec);
+            cudaGraphDestroy(p->graph);
+            p->gexec = NULL;
+            p->graph = NULL;
+            p->graph_ready = 0;
+        }
     }
     CUDA_TRY(cudaMemcpyAsync(p->d_dev, p->h_dev, sizeof(trpdrv_dev_system) * (size_t)p->nsys,
                              cudaMemcpyHostToDevice, p->stream));
@@ -457,8 +489,12 @@ static int enqueue_fused(trpdrv_plan *p, cudaStream_t st, int capturing)
     CUDA_TRY(cudaMemsetAsync(p->d_tot, 0, sizeof(double) * 4 * (size_t)p->nsys, st));
     CUDA_TRY(cudaEventRecordWithFlags(p->ev0, st, capturing ? cudaEventRecordExternal : cudaEventRecordDefault));
     if (p->total_items > 0) {
-        LAUNCH_TRY(trpdrv_launch_fused(p->d_dev, p->nsys, p->total_items, p->d_counter, p->d_status, p->grid,
-                                       p->vec2, p->opt.mma_k, st));
+        if (p->use_tma)
+            LAUNCH_TRY(trpdrv_launch_fused_tma(p->d_dev, p->nsys, p->total_items, p->d_counter, p->d_status,
+                                               p->grid_tma, p->tma_maps, st));
+        else
+            LAUNCH_TRY(trpdrv_launch_fused(p->d_dev, p->nsys, p->total_items, p->d_counter, p->d_status, p->grid,
+                                           p->vec2, p->opt.mma_k, st));
         ++launches;
     }
     CUDA_TRY(cudaEventRecordWithFlags(p->ev1, st, capturing ? cudaEventRecordExternal : cudaEventRecordDefault));
@@ -585,6 +621,7 @@ static int plan_wait(trpdrv_plan *p)
     CUDA_TRY(cudaStreamSynchronize(p->last_stream ? p->last_stream : p->stream));
     int status = 0;
     CUDA_TRY(cudaMemcpy(&status, p->d_status, sizeof(int), cudaMemcpyDeviceToHost));
+    if (status & 2) return fail(TRPDRV_ERR_DEVICE, "a fused-kernel pipeline wait ran out of time");
     if (status) return fail(TRPDRV_ERR_DEVICE, "the fused kernel rejected a malformed work-queue entry");
     return TRPDRV_OK;
 }
@@ -638,6 +675,12 @@ int trpdrv_plan_triple_energies(trpdrv_plan *p, int sys, double *rec)
 }
 
 int64_t trpdrv_plan_last_launches(const trpdrv_plan *p) { return p ? p->last_launches : -1; }
+
+int trpdrv_plan_staging(const trpdrv_plan *p)
+{
+    if (!p || !p->bound || p->opt.mode != TRPDRV_MODE_FUSED) return 0;
+    return p->use_tma ? 2 : 1;
+}
 
 int trpdrv_plan_last_kernel_ms(trpdrv_plan *p, double *ms)
 {

@@ -45,6 +45,21 @@ int trpdrv_launch_fused(const trpdrv_dev_system *d_sys, int nsys, int64_t total_
 size_t trpdrv_fused_smem_bytes(void);
 int trpdrv_fused_threads(void);
 int trpdrv_fused_max_ctas_per_sm(int *n);
+int trpdrv_fused_init(void);
+
+/* The same fused computation with TMA-staged panels and mbarrier pipelines (fused_tma.cu).  Needs
+ * even nvir and nocc, 16-byte aligned tensors and at most TRPDRV_TMA_MAX_SYSTEMS systems
+ * (trpdrv_tma_supported).  trpdrv_tma_prepare encodes the tensor maps of every system into a
+ * host blob of trpdrv_tma_maps_bytes() bytes (64-byte aligned) that each launch passes by value.
+ * One CTA per SM.  *status bit 0: malformed queue entry; bit 1: a pipeline wait ran out. */
+#define TRPDRV_TMA_MAX_SYSTEMS 8
+int trpdrv_tma_supported(const trpdrv_dev_system *h_sys, int nsys);
+size_t trpdrv_tma_maps_bytes(void);
+int trpdrv_tma_prepare(const trpdrv_dev_system *h_sys, int nsys, void *maps_out);
+int trpdrv_launch_fused_tma(const trpdrv_dev_system *d_sys, int nsys, int64_t total_items,
+                            unsigned long long *counter, int *status, int grid, const void *maps,
+                            void *stream);
+int trpdrv_fused_tma_init(void);
 
 /* Per-triple sum of the per-item energies of one system (partial -> rec). */
 int trpdrv_launch_item_reduce(const trpdrv_dev_system *h_sys, void *stream);

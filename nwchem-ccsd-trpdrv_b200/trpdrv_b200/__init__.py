@@ -15,7 +15,7 @@ from typing import Optional, Sequence
 import numpy as np
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(os.path.dirname(_HERE), "lib", "libtrpdrv_b200.so")
+LIB_PATH = os.environ.get("TRPDRV_LIB") or os.path.join(os.path.dirname(_HERE), "lib", "libtrpdrv_b200.so")
 INCLUDE_DIR = os.path.join(os.path.dirname(os.path.dirname(_HERE)), "include")
 
 MODE_PLAIN = 0
@@ -55,7 +55,9 @@ class SystemStruct(C.Structure):
 class OptionsStruct(C.Structure):
     _fields_ = [("mode", C.c_int), ("nkpass", C.c_int), ("rank", C.c_int), ("world", C.c_int),
                 ("device", C.c_int), ("tile", C.c_int), ("ctas_per_sm", C.c_int),
-                ("use_graph", C.c_int), ("mma_k", C.c_int), ("reserved", C.c_int * 7)]
+                ("use_graph", C.c_int), ("mma_k", C.c_int), ("staging", C.c_int), ("reserved", C.c_int * 6)]
+
+STAGING_AUTO, STAGING_CPASYNC, STAGING_TMA = 0, 1, 2
 
 
 def _proto(name, res, args):
@@ -81,6 +83,7 @@ _proto("trpdrv_plan_num_triples", C.c_int64, [C.c_void_p, C.c_int])
 _proto("trpdrv_plan_triples", C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_int32)])
 _proto("trpdrv_plan_triple_energies", C.c_int, [C.c_void_p, C.c_int, _dp])
 _proto("trpdrv_plan_last_launches", C.c_int64, [C.c_void_p])
+_proto("trpdrv_plan_staging", C.c_int, [C.c_void_p])
 _proto("trpdrv_plan_last_kernel_ms", C.c_int, [C.c_void_p, _dp])
 _proto("trpdrv_plan_destroy", C.c_int, [C.c_void_p])
 _proto("trpdrv_run", C.c_int, [C.POINTER(SystemStruct), C.c_int, C.POINTER(OptionsStruct), _dp, _dp])
@@ -280,11 +283,11 @@ def tengy(f8: np.ndarray, vecs: Sequence[np.ndarray], eorb: np.ndarray, eaijk: f
 # plans
 # --------------------------------------------------------------------------------------------
 def options(mode=MODE_FUSED, nkpass=1, rank=0, world=1, device=-1, ctas_per_sm=0, use_graph=1,
-            mma_k=0) -> OptionsStruct:
+            mma_k=0, staging=STAGING_AUTO) -> OptionsStruct:
     o = OptionsStruct()
     lib.trpdrv_options_default(C.byref(o))
     o.mode, o.nkpass, o.rank, o.world, o.device = mode, nkpass, rank, world, device
-    o.ctas_per_sm, o.use_graph = ctas_per_sm, use_graph
+    o.ctas_per_sm, o.use_graph, o.staging = ctas_per_sm, use_graph, staging
     if mma_k:
         o.mma_k = mma_k
     return o
@@ -336,6 +339,10 @@ class Plan:
         out = np.zeros((max(n, 1), 4))
         _check(lib.trpdrv_plan_triple_energies(self.h, sys, out.ctypes.data_as(_dp)))
         return out[:n]
+
+    def staging(self) -> int:
+        """1 = cp.async, 2 = TMA staging in the fused kernel (0 for plain plans)."""
+        return int(lib.trpdrv_plan_staging(self.h))
 
     def last_launches(self) -> int:
         return int(lib.trpdrv_plan_last_launches(self.h))

@@ -17,7 +17,8 @@ from kat import run_make_array_loop
 
 pytestmark = pytest.mark.gpu
 
-MODES = {"fused": dict(mode=1, mma_k=8), "fused_k4": dict(mode=1, mma_k=4), "plain": dict(mode=0)}
+MODES = {"fused": dict(mode=1), "fused_cpasync": dict(mode=1, staging=1, mma_k=8),
+         "fused_cpasync_k4": dict(mode=1, staging=1, mma_k=4), "plain": dict(mode=0)}
 
 
 def _plan_run(T, systems, **opt):
@@ -27,6 +28,11 @@ def _plan_run(T, systems, **opt):
         e4, e5 = p.energies()
         recs = [p.triple_energies(q) for q in range(len(systems))]
         launches = p.last_launches()
+        staging = p.staging()
+    if opt.get("mode", 1) == 1:  # TMA wherever the shapes allow it, cp.async otherwise
+        even = all(s.nvir % 2 == 0 and s.nocc % 2 == 0 for s in systems)
+        want = {0: 2 if even else 1, 1: 1, 2: 2}[opt.get("staging", 0)]
+        assert staging == want, (staging, want)
     return e4, e5, recs, launches
 
 
@@ -233,3 +239,19 @@ def test_full_size_fused_vs_plain_and_reference_sample(T, O):
             rec, _, mism = O.run_system(s, "reference", t_begin=lo, t_end=lo + 8, nthreads=8)
             assert mism == 0
             assert_records_close(recf[0][lo:lo + 8], rec)
+
+
+def test_tma_staging_is_refused_for_odd_sizes(T):
+    s = T.synth_system(5, 33, seed=3)
+    with T.Plan([s], mode=1, staging=2) as p:
+        with pytest.raises(T.TrpdrvError) as ei:
+            p.upload()
+        assert ei.value.status == 6
+
+
+def test_tma_and_cpasync_agree_bitwise_where_the_order_matches(T):
+    """Both stagings feed identical operands to identical MMA sequences: equal records."""
+    s = T.synth_system(6, 96, seed=44)
+    a = _plan_run(T, [s], mode=1, staging=2)
+    b = _plan_run(T, [s], mode=1, staging=1, mma_k=8)
+    assert np.array_equal(a[2][0], b[2][0])

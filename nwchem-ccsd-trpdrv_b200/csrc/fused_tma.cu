@@ -47,6 +47,7 @@ constexpr int PANEL_BYTES = 4096;
 constexpr int NPANEL = 16;
 constexpr int STAGE_BYTES = NPANEL * PANEL_BYTES;
 constexpr int RING = 16;
+constexpr int XBUF = T * (T + 1);  // one padded 32x32 f tile
 constexpr int KBOX = PANEL_BYTES / 2;  // one 16-row K-major box
 constexpr size_t SMEM_BYTES = (size_t)STAGES * STAGE_BYTES + 1024;  // + alignment slack
 constexpr unsigned long long WAIT_LIMIT_NS = 4000000000ull;       // 4 s: far above any legitimate wait
@@ -381,6 +382,8 @@ fused_tma_kernel(const trpdrv_dev_system *__restrict__ sys, int nsys, long long 
     extern __shared__ char smem_raw[];
     __shared__ __align__(8) unsigned long long full[STAGES], empty[STAGES];
     __shared__ ItemCtx ring[RING];
+    __shared__ double xbuf[2 * XBUF];                       // diagonal-pair transpose exchange
+    __shared__ __align__(8) unsigned long long xbar[1];
     char *stages = reinterpret_cast<char *>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~(uintptr_t)1023);
 
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -389,6 +392,7 @@ fused_tma_kernel(const trpdrv_dev_system *__restrict__ sys, int nsys, long long 
             mbar_init(&full[s], 1);
             mbar_init(&empty[s], NCW);
         }
+        mbar_init(xbar, NCW);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     __syncthreads();
@@ -408,7 +412,7 @@ fused_tma_kernel(const trpdrv_dev_system *__restrict__ sys, int nsys, long long 
 
     double f[8][4], gT[8][4];
     int stage = 0;
-    unsigned phase = 0;
+    unsigned phase = 0, xphase = 0;
     for (long long n = 0;; ++n) {
         if (!mbar_wait(&full[stage], phase, status)) return;
         const ItemCtx &cx = ring[n % RING];
@@ -433,48 +437,55 @@ fused_tma_kernel(const trpdrv_dev_system *__restrict__ sys, int nsys, long long 
             for (int e = 0; e < 4; ++e) f[x][e] = gT[x][e] = 0.0;
         const int nch = cx.nch, nV = cx.nV;
         const bool active = (cx.b0 + rx0 < cx.nvir) && (cx.c0 + cx0 < cx.nvir);
-        const int o1 = cx.diag ? 0 : 1;  // diagonal pair: the C panels are the B panels
+        const bool diag = cx.diag != 0;
         const int pf = nch > 3 ? nch - 3 : 0;
         for (int ch = 0; ch < nch; ++ch) {
             if (ch > 0 && !mbar_wait(&full[stage], phase, status)) return;
             const char *st = stages + (size_t)stage * STAGE_BYTES;
             const bool ph1 = ch >= nV;
+            // the second k-step of a chunk is skipped when it lies entirely in the zero padding
+            const int kval = ph1 ? cx.nocc - (ch - nV) * DK : cx.nvir - ch * DK;
             if (ch == pf) prefetch_epilogue(cx, lane);
             if (active) {
 #pragma unroll
                 for (int ks = 0; ks < 2; ++ks)
 #pragma unroll
                 for (int fam = 0; fam < 2; ++fam) {
+                    if (ks == 1 && kval <= 8) break;
                     const char *P = st + fam * 8 * PANEL_BYTES + ks * 1024;    // o = 0 panels (K-major k-step)
-                    const char *Q = P + o1 * PANEL_BYTES;          // o = 1 panels (C side)
+                    const char *Q = P + PANEL_BYTES;               // o = 1 panels (C side)
                     const char *PX = st + fam * 8 * PANEL_BYTES;   // X-major bases
-                    const char *QX = PX + o1 * PANEL_BYTES;
+                    const char *QX = PX + PANEL_BYTES;
                     const int kx = ks * 64;
-                    double aJ[4], aK[4], a1[4], a3[4], bJ[2], bK[2], b1[2], b3[2];
+                    const int x0 = fam * 4;
+                    double aJ[4], aK[4], b1[2], b3[2];
                     fo.ldA_K(aJ, P + 0 * PANEL_BYTES);
                     fo.ldA_K(aK, P + 2 * PANEL_BYTES);
-                    fo.ldB_K(bJ, Q + 0 * PANEL_BYTES);
-                    fo.ldB_K(bK, Q + 2 * PANEL_BYTES);
                     fo.ldB_X(b3, PX + 6 * PANEL_BYTES, kx);
-                    fo.ldA_X(a3, QX + 6 * PANEL_BYTES, kx);
-                    if (!ph1) {
+                    if (!ph1)
                         fo.ldB_K(b1, P + 4 * PANEL_BYTES);
-                        fo.ldA_K(a1, Q + 4 * PANEL_BYTES);
-                    } else {
+                    else
                         fo.ldB_X(b1, PX + 4 * PANEL_BYTES, kx);
-                        fo.ldA_X(a1, QX + 4 * PANEL_BYTES, kx);
-                    }
-                    const int x0 = fam * 4;
                     // f1 = A_J B_1, f2 = A_K B_1, f3 = A_J B_3, f4 = A_K B_3
                     dmma_16x8x8(f[x0 + 0], aJ, b1);
                     dmma_16x8x8(f[x0 + 1], aK, b1);
                     dmma_16x8x8(f[x0 + 2], aJ, b3);
                     dmma_16x8x8(f[x0 + 3], aK, b3);
-                    // transposes: f_x(c,b) = sum_d B_x(d,b) A_x(c,d)
-                    dmma_16x8x8(gT[x0 + 0], a1, bJ);
-                    dmma_16x8x8(gT[x0 + 1], a1, bK);
-                    dmma_16x8x8(gT[x0 + 2], a3, bJ);
-                    dmma_16x8x8(gT[x0 + 3], a3, bK);
+                    if (!diag) {  // a diagonal pair gets f(c,b) from the other warps instead (below)
+                        double a1[4], a3[4], bJ[2], bK[2];
+                        fo.ldB_K(bJ, Q + 0 * PANEL_BYTES);
+                        fo.ldB_K(bK, Q + 2 * PANEL_BYTES);
+                        fo.ldA_X(a3, QX + 6 * PANEL_BYTES, kx);
+                        if (!ph1)
+                            fo.ldA_K(a1, Q + 4 * PANEL_BYTES);
+                        else
+                            fo.ldA_X(a1, QX + 4 * PANEL_BYTES, kx);
+                        // transposes: f_x(c,b) = sum_d B_x(d,b) A_x(c,d)
+                        dmma_16x8x8(gT[x0 + 0], a1, bJ);
+                        dmma_16x8x8(gT[x0 + 1], a1, bK);
+                        dmma_16x8x8(gT[x0 + 2], a3, bJ);
+                        dmma_16x8x8(gT[x0 + 3], a3, bK);
+                    }
                 }
             }
             __syncwarp();
@@ -482,6 +493,25 @@ fused_tma_kernel(const trpdrv_dev_system *__restrict__ sys, int nsys, long long 
             if (++stage == STAGES) {
                 stage = 0;
                 phase ^= 1;
+            }
+        }
+        if (diag) {
+            // f(c,b) of a diagonal pair is f at the mirrored position of the same 32x32 block, held
+            // by another warp: exchange one f at a time through two alternating shared buffers,
+            // separated by a consumer-only mbarrier (bounded wait; no CTA-wide barrier).
+#pragma unroll
+            for (int x = 0; x < 8; ++x) {
+                double *xb = xbuf + (x & 1) * XBUF;
+#pragma unroll
+                for (int e = 0; e < 4; ++e)
+                    xb[(rx0 + g + ((e & 2) ? 8 : 0)) * (T + 1) + cx0 + 2 * t + (e & 1)] = f[x][e];
+                __syncwarp();
+                if (lane == 0) mbar_arrive(xbar);
+                if (!mbar_wait(xbar, xphase, status)) return;
+                xphase ^= 1;
+#pragma unroll
+                for (int e = 0; e < 4; ++e)
+                    gT[x][e] = xb[(cx0 + 2 * t + (e & 1)) * (T + 1) + rx0 + g + ((e & 2) ? 8 : 0)];
             }
         }
         warp_epilogue(cx, f, gT, cx.b0 + rx0, cx.c0 + cx0, g, t, lane, cx.out + warp * 4);

@@ -126,6 +126,34 @@ __device__ __forceinline__ void tengy_term(const double (&bc)[8], const double (
            + denom * t1v2b * dc2c * (t1bc + t4bc + n1cb - (t2bc + t3bc + n2cb) * 2);
 }
 
+// The same four forms with the denominator factored out of each, for callers that already hold
+// denom = -1/(e_b + e_c + eaijk) (shared by the mirrored positions (b,c) and (c,b)).  Equal to
+// tengy_term up to floating-point reassociation.
+__device__ __forceinline__ void tengy_term_factored(const double (&bc)[8], const double (&cb)[8], double denom,
+                                                    double t1v1b, double t1v2b, double dx1c, double dx2c,
+                                                    double dc1c, double dc2c, TengySums &s)
+{
+    const double n1bc = bc[0], n2bc = bc[1], n3bc = bc[2], n4bc = bc[3];
+    const double t1bc = bc[4], t2bc = bc[5], t3bc = bc[6], t4bc = bc[7];
+    const double n1cb = cb[0], n2cb = cb[1], n3cb = cb[2], n4cb = cb[3];
+    const double t1cb = cb[4], t2cb = cb[5], t3cb = cb[6], t4cb = cb[7];
+
+    const double a4i = (t1bc + n1cb + t2cb + n3bc + n4cb) * (t1bc - t2bc * 2 - t3bc * 2 + t4bc)
+                     - (n1bc + t1cb + n2cb + n3cb) * (t1bc * 2 - t2bc - t3bc + t4bc * 2)
+                     + 3 * (n1bc * (n1bc + n3cb + t4cb * 2) + n2bc * t2cb + n3bc * t4bc);
+    const double a4k = (n1bc + t1cb + n2cb + t3bc + t4cb) * (n1bc - n2bc * 2 - n3bc * 2 + n4bc)
+                     - (t1bc + n1cb + t2cb + t3cb) * (n1bc * 2 - n2bc - n3bc + n4bc * 2)
+                     + 3 * (t1bc * (t1bc + t3cb + n4cb * 2) + t2bc * n2cb + t3bc * n4bc);
+    const double f5i = t1bc + n2bc + n4cb - (t3bc + n4bc + n2cb + n1bc + t2bc + n3cb) * 2 + (n3bc + t4bc + n1cb) * 4;
+    const double g5i = n1bc + n4bc + t1cb - (n2bc + n3bc + t2cb) * 2;
+    const double f5k = n1bc + t2bc + t4cb - (n3bc + t4bc + t2cb + t1bc + n2bc + t3cb) * 2 + (t3bc + n4bc + t1cb) * 4;
+    const double g5k = t1bc + t4bc + n1cb - (t2bc + t3bc + n2cb) * 2;
+    s.e4i += denom * a4i;
+    s.e4k += denom * a4k;
+    s.e5i += denom * (t1v1b * (dx1c * f5i + dc1c * g5i));
+    s.e5k += denom * (t1v2b * (dx2c * f5k + dc2c * g5k));
+}
+
 // Block-wide sum of the four partial energies; returns the totals in thread 0.  `scratch` must
 // hold 4 * (blockDim.x / 32) doubles.  The summation order is fixed (deterministic).
 __device__ __forceinline__ TengySums block_sum4(TengySums s, double *scratch)

@@ -106,12 +106,16 @@ __device__ __forceinline__ bool mbar_try_wait(unsigned long long *b, unsigned pa
 }
 
 // Bounded wait for the phase with the given parity; false (and status bit 1) when it runs out.
+// try_wait itself suspends the warp for a while in hardware; the clock is read only every 256
+// failed polls so that waiting warps take few issue slots from the MMA warps of their scheduler.
 __device__ __forceinline__ bool mbar_wait(unsigned long long *b, unsigned parity, int *status)
 {
     if (mbar_try_wait(b, parity)) return true;
     const unsigned long long t0 = globaltimer();
     for (;;) {
-        if (mbar_try_wait(b, parity)) return true;
+#pragma unroll 1
+        for (int spin = 0; spin < 256; ++spin)
+            if (mbar_try_wait(b, parity)) return true;
         if (globaltimer() - t0 > WAIT_LIMIT_NS) {
             atomicOr(status, 2);
             return false;
@@ -228,13 +232,14 @@ __device__ __forceinline__ void warp_epilogue(const ItemCtx &cx, const double (&
                 fcb[x] = gT[x][e];
             }
             const double eb = __ldg(cx.eorb + voff + b), ec = __ldg(cx.eorb + voff + c);
-            // term at (b,c): omp/ccsd_tengy_c99.c:65 denominator, :91-111 forms
-            tengy_term(fbc, fcb, -1.0 / (eb + ec + eaijk), __ldg(cx.t1v1 + b), __ldg(cx.t1v2 + b),
-                       __ldg(cx.dintx1 + c), __ldg(cx.dintx2 + c), __ldg(cx.dintc1 + c), __ldg(cx.dintc2 + c), su);
+            // omp/ccsd_tengy_c99.c:65 denominator; e_b + e_c == e_c + e_b, so (b,c) and (c,b) share it
+            const double denom = -1.0 / (eb + ec + eaijk);
+            // term at (b,c): :91-111 forms
+            tengy_term_factored(fbc, fcb, denom, __ldg(cx.t1v1 + b), __ldg(cx.t1v2 + b), __ldg(cx.dintx1 + c),
+                                __ldg(cx.dintx2 + c), __ldg(cx.dintc1 + c), __ldg(cx.dintc2 + c), su);
             if (!cx.diag)  // term at (c,b) of the mirrored tile
-                tengy_term(fcb, fbc, -1.0 / (ec + eb + eaijk), __ldg(cx.t1v1 + c), __ldg(cx.t1v2 + c),
-                           __ldg(cx.dintx1 + b), __ldg(cx.dintx2 + b), __ldg(cx.dintc1 + b), __ldg(cx.dintc2 + b),
-                           su);
+                tengy_term_factored(fcb, fbc, denom, __ldg(cx.t1v1 + c), __ldg(cx.t1v2 + c), __ldg(cx.dintx1 + b),
+                                    __ldg(cx.dintx2 + b), __ldg(cx.dintc1 + b), __ldg(cx.dintc2 + b), su);
         }
     }
     su.e4i = warp_sum(su.e4i);

@@ -1,0 +1,98 @@
+"""Host-side logic of the library (no GPU): triple enumeration, partitioning, shards, the synthetic
+generator, argument validation of the drop-in entry points and plan creation without a device."""
+import numpy as np
+import pytest
+
+from conftest import has_gpu
+
+
+@pytest.mark.parametrize("nocc", [1, 2, 5, 8, 13])
+@pytest.mark.parametrize("nkpass", [1, 2, 3, 7])
+def test_enumeration_matches_reference_driver_order(T, O, nocc, nkpass):
+    got = T.enumerate_triples(nocc, nkpass)
+    want = O.enumerate_triples(nocc, nkpass)
+    assert np.array_equal(got, want)
+    assert len(got) == T.count_triples(nocc) == nocc * nocc * (nocc + 1) // 2
+    # every (i, j, k <= i) exactly once, whatever the k-chunking
+    assert len({tuple(r[:3]) for r in got}) == len(got)
+    assert np.all(got[:, 2] <= got[:, 0]) and np.all(got[:, 3] <= got[:, 2])
+
+
+def test_partition_is_contiguous_and_balanced(T):
+    rng = np.random.default_rng(0)
+    cost = rng.uniform(0.5, 2.0, 1000)
+    for world in (1, 2, 3, 7, 16):
+        b = T.partition(cost, len(cost), world)
+        assert b[0] == 0 and b[-1] == len(cost) and np.all(np.diff(b) >= 0)
+        shares = np.array([cost[b[r]:b[r + 1]].sum() for r in range(world)])
+        assert shares.max() - shares.min() <= 2 * cost.max()
+    b = T.partition(None, 10, 3)
+    assert list(b) == [0, 3, 7, 10]
+    b = T.partition(None, 2, 4)  # more ranks than items
+    assert b[0] == 0 and b[-1] == 2 and np.all(np.diff(b) >= 0)
+
+
+@pytest.mark.parametrize("nocc,world", [(5, 2), (6, 3), (3, 8), (10, 7)])
+def test_shards_cover_the_driver_order(T, nocc, world):
+    parts = [T.shard_triples(nocc, 1, r, world) for r in range(world)]
+    assert np.array_equal(np.concatenate(parts), T.enumerate_triples(nocc, 1)[:, :3])
+    sizes = [len(p) for p in parts]
+    assert max(sizes) - min(sizes) <= 1
+    with pytest.raises(T.TrpdrvError):
+        T.shard_triples(nocc, 1, world, world)
+
+
+def test_synthetic_generator_is_deterministic_and_in_range(T):
+    a = T.synth_system(4, 20, seed=5, ncor=2)
+    b = T.synth_system(4, 20, seed=5, ncor=2)
+    c = T.synth_system(4, 20, seed=6, ncor=2)
+    for n in T.TENSOR_NAMES:
+        assert np.array_equal(a.arrays[n], b.arrays[n])
+        assert not np.array_equal(a.arrays[n], c.arrays[n])
+        assert a.arrays[n].size == T.tensor_elems(T.TENSOR_NAMES.index(n), 2, 4, 20)
+    e = a.arrays["eorb"]
+    core, occ, vir = e[:2], e[2:6], e[6:]
+    assert np.all(np.diff(core) >= 0) and np.all(np.diff(occ) >= 0) and np.all(np.diff(vir) >= 0)
+    assert core.min() >= -20 and core.max() <= -5 and occ.min() >= -2 and occ.max() <= -0.5
+    assert vir.min() >= 0.2 and vir.max() <= 3.0
+    assert np.abs(a.arrays["t2"]).max() <= 0.05 and np.abs(a.arrays["tov"]).max() <= 0.02
+    assert np.abs(a.arrays["jvv"]).max() <= 0.1 and np.abs(a.arrays["t1v"]).max() <= 0.02
+    assert a.a == 2 + 4 + 1  # first virtual: every denominator e_b + e_c + eaijk >= 2.1
+    lg = T.synth_system(3, 16, seed=1, dist=T.DIST_LOGUNIFORM)
+    mag = np.abs(lg.arrays["kvv"])
+    assert mag.min() >= 1e-6 * (1 - 1e-12) and mag.max() <= 1.0
+    assert (lg.arrays["kvv"] < 0).mean() > 0.3 and (lg.arrays["kvv"] > 0).mean() > 0.3
+    assert np.abs(lg.arrays["t2"]).max() <= 0.05  # amplitudes keep the uniform distribution
+
+
+def test_dropin_rejects_bad_arguments_before_touching_a_device(T, monkeypatch):
+    monkeypatch.setenv("TRPDRV_ON_ERROR", "return")
+    s = T.synth_system(3, 12, seed=2)
+    T.clear_error()
+    assert T.cbody(s, 4, 1, 1, 1, emp4=1.5, emp5=2.5) == (1.5, 2.5)  # i > nocc
+    code, msg = T.last_error()
+    assert code == 1 and "outside" in msg
+    T.clear_error()
+    assert T.cbody(s, 2, 1, 2, 3, emp4=1.5, emp5=2.5) == (1.5, 2.5)  # klo > k
+    assert T.last_error()[0] == 1
+
+
+@pytest.mark.skipif(has_gpu(), reason="checks the behaviour without a device")
+def test_plan_without_a_device_reports_nodev(T):
+    s = T.synth_system(2, 8, seed=1)
+    with pytest.raises(T.TrpdrvError) as ei:
+        T.Plan([s])
+    assert ei.value.status in (4, 2)
+
+
+def test_plan_argument_checks_precede_device_use(T):
+    s = T.synth_system(2, 8, seed=1)
+    with pytest.raises(T.TrpdrvError) as ei:
+        T.Plan([T.System(0, 2, 8, 0, s.arrays)])
+    assert ei.value.status == 1
+    with pytest.raises(T.TrpdrvError) as ei:
+        T.Plan([s], rank=3, world=2)
+    assert ei.value.status == 1
+    with pytest.raises(T.TrpdrvError) as ei:
+        T.Plan([s], staging=5)
+    assert ei.value.status == 1

@@ -243,6 +243,32 @@ size_t trpdrv_tensor_elems(int tensor, int ncor, int nocc, int nvir);
 int trpdrv_synth_fill(int tensor, int ncor, int nocc, int nvir, uint64_t seed, int dist,
                       double *out, size_t n);
 
+/* ---- one triple without device allocation ----
+ * No counterpart in the reference.  For callers that cannot allocate device memory when they need
+ * the work done: code inside a CUDA stream capture (cudaMalloc is not allowed there), code under a
+ * device-memory budget fixed by its host application, or callers that own every device buffer.
+ * Runs the body of one triple (a,i,j,k) on DEVICE pointers that are already sliced for the triple
+ * (tkj is the (k,j) block itself, not the k-chunk base; likewise jka, kka, tka, xka, jkj, kkj;
+ * dintc2/dintx2/t1v2 are the k vectors) and writes out4[0..3] = emp4i, emp5i, emp4k, emp5k on the
+ * device.  Enqueues on `stream` and returns without waiting; allocates nothing: its scratch is one
+ * static device array of about 4.7 MB per GPU, kept until the process exits, that limits the size
+ * to nvir <= TRPDRV_NOALLOC_MAX_NVIR and nocc <= TRPDRV_NOALLOC_MAX_NOCC (larger sizes are
+ * rejected with TRPDRV_ERR_ARG).  All calls on a device share that array: calls that overlap on
+ * the GPU race and must be serialised by the caller.  The first call on each device looks up the
+ * array and sets kernel attributes; make it before any stream capture. */
+#define TRPDRV_NOALLOC_MAX_NVIR 256
+#define TRPDRV_NOALLOC_MAX_NOCC 64
+typedef struct trpdrv_body_device_args {
+    int ncor, nocc, nvir;
+    int a, i, j, k;  /* 1-based, as in the reference body */
+    const double *eorb;
+    const double *tij, *tkj, *tia, *tka, *xia, *xka, *jia, *jka, *kia, *kka;
+    const double *jij, *jkj, *kij, *kkj;
+    const double *dintc1, *dintx1, *t1v1, *dintc2, *dintx2, *t1v2;
+    double *out4;
+} trpdrv_body_device_args;
+int trpdrv_body_device_noalloc(const trpdrv_body_device_args *args, void *stream);
+
 /* ---- device probes ---- */
 
 /* FP64 issue-rate microbenchmark on `device`: kind 0 = DMMA m8n8k4, 1 = m16n8k4, 2 = m16n8k8,

@@ -33,6 +33,12 @@ static int fail(int status, const char *fmt, ...)
     return status;
 }
 
+/* Records a failure from another translation unit (declared in launch.h). */
+int trpdrv_record_error(int status, const char *message)
+{
+    return fail(status, "%s", message ? message : "");
+}
+
 int trpdrv_last_error(void) { return t_status; }
 const char *trpdrv_last_error_message(void) { return t_message; }
 void trpdrv_clear_error(void)

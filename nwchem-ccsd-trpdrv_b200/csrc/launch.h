@@ -106,6 +106,9 @@ int trpdrv_launch_probe(int kind, int grid, int iters, double *sink, double *flo
 /* Sets the dynamic shared memory limits of every kernel (call once per device). */
 int trpdrv_kernels_init(void);
 
+/* Sets the calling thread's trpdrv_last_error() status and message; returns status. */
+int trpdrv_record_error(int status, const char *message);
+
 #ifdef __cplusplus
 }
 #endif

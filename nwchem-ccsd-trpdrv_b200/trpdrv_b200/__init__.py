@@ -59,6 +59,16 @@ class OptionsStruct(C.Structure):
 
 STAGING_AUTO, STAGING_CPASYNC, STAGING_TMA = 0, 1, 2
 
+BODY_DEVICE_FIELDS = ("eorb", "tij", "tkj", "tia", "tka", "xia", "xka", "jia", "jka", "kia", "kka", "jij", "jkj",
+                      "kij", "kkj", "dintc1", "dintx1", "t1v1", "dintc2", "dintx2", "t1v2", "out4")
+NOALLOC_MAX_NVIR, NOALLOC_MAX_NOCC = 256, 64
+
+
+class BodyDeviceArgs(C.Structure):
+    """trpdrv_body_device_args: one triple on caller-owned device pointers (already sliced)."""
+    _fields_ = [("ncor", C.c_int), ("nocc", C.c_int), ("nvir", C.c_int), ("a", C.c_int), ("i", C.c_int),
+                ("j", C.c_int), ("k", C.c_int)] + [(n, C.c_void_p) for n in BODY_DEVICE_FIELDS]
+
 
 def _proto(name, res, args):
     f = getattr(lib, name)
@@ -96,6 +106,7 @@ _proto("trpdrv_tensor_elems", C.c_size_t, [C.c_int, C.c_int, C.c_int, C.c_int])
 _proto("trpdrv_synth_fill", C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int, C.c_uint64, C.c_int, _dp,
                                       C.c_size_t])
 _proto("trpdrv_probe_fp64_peak", C.c_int, [C.c_int, C.c_int, _dp])
+_proto("trpdrv_body_device_noalloc", C.c_int, [C.POINTER(BodyDeviceArgs), C.c_void_p])
 _proto("trpdrv_finalize", None, [])
 _body_args = [_dp] * 9 + [_ip] * 3 + [_dp] * 2 + [_ip] * 5 + [_dp] * 20
 for _n in ("ccsd_trpdrv_omp_cbody_", "ccsd_trpdrv_omp_fbody_", "ccsd_trpdrv_cbody_", "ccsd_trpdrv_opencl_"):
@@ -378,6 +389,17 @@ def run(systems: Sequence[System], **opt):
     e5 = np.zeros(len(systems))
     _check(lib.trpdrv_run(arr, len(systems), C.byref(o), e4.ctypes.data_as(_dp), e5.ctypes.data_as(_dp)))
     return e4, e5
+
+
+def body_device_noalloc(ncor: int, nocc: int, nvir: int, a: int, i: int, j: int, k: int, ptrs: dict,
+                        stream: int = 0):
+    """trpdrv_body_device_noalloc: `ptrs` maps BODY_DEVICE_FIELDS to device addresses (ints).
+    Asynchronous on `stream`; raises TrpdrvError on a rejected call."""
+    args = BodyDeviceArgs()
+    args.ncor, args.nocc, args.nvir, args.a, args.i, args.j, args.k = ncor, nocc, nvir, a, i, j, k
+    for n in BODY_DEVICE_FIELDS:
+        setattr(args, n, C.c_void_p(int(ptrs[n])) if ptrs.get(n) else None)
+    _check(lib.trpdrv_body_device_noalloc(C.byref(args), C.c_void_p(stream) if stream else None))
 
 
 def probe_fp64_peak(kind: int, device: int = -1) -> float:

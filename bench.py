@@ -170,7 +170,7 @@ class ClockSampler:
 
 def read_profile_traffic():
     """DRAM bytes per fused launch from the committed ncu summary (profiles/), or None."""
-    path = os.path.join(ROOT, "profiles", "fused_nocc40_nvir300.md")
+    path = os.path.join(ROOT, "profiles", "fused_tma_nocc40_nvir300.md")
     if not os.path.exists(path):
         return None
     for ln in open(path):

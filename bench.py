@@ -174,6 +174,7 @@ def read_profile_traffic():
     if not os.path.exists(path):
         return None
     for ln in open(path):
+        ln = ln.lstrip("*- \t")
         if ln.startswith("traffic_bytes_per_launch:"):
             try:
                 return float(ln.split(":", 1)[1].split()[0])

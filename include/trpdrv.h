@@ -227,6 +227,13 @@ int trpdrv_partition(const double *cost, int64_t n, int world, int64_t *bounds);
  * split by trpdrv_partition into `world` contiguous ranges of equal count.  Writes ijk[3*t..] =
  * i, j, k (1-based) when ijk is not NULL and returns the share's size (negative on bad arguments). */
 int64_t trpdrv_shard_triples(int nocc, int nkpass, int rank, int world, int32_t *ijk);
+/* The order in which fused plans process a list of triples (ijk[3*t..] = i, j, k, 1-based, e.g. from
+ * trpdrv_shard_triples); energies are still stored and summed in list order, so the order changes
+ * no result.  Within each run of equal j the (i, k) triangle is walked in blocks of `block` i values
+ * (k outer, direction alternating from block to block, i inner), so that the operand slices one
+ * stretch of work touches fit in L2.  Writes the permutation order[position] = list index; returns
+ * 0, or -1 on bad arguments.  block <= 0 selects the default (8). */
+int trpdrv_processing_order(const int32_t *ijk, int64_t n, int block, int32_t *order);
 /* Cost (FLOPs) of one triple of a system: 16*nvir*nvir*(nvir+nocc). */
 double trpdrv_triple_flops(int nocc, int nvir);
 

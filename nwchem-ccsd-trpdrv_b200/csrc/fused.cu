@@ -186,8 +186,10 @@ __device__ __forceinline__ void prepare_item(const trpdrv_dev_system *__restrict
     while (s + 1 < nsys && item >= sys[s + 1].item_begin) ++s;
     const trpdrv_dev_system &S = sys[s];
     const long long local = item - S.item_begin;
-    const long long tt = local / S.npairs;
-    const int p = (int)(local - tt * S.npairs);
+    const long long qpos = local / S.npairs;  // processing order; energies go to the triple's own items
+    const int p = (int)(local - qpos * S.npairs);
+    const long long tt = (S.order && local >= 0 && qpos < S.ntriples) ? (long long)S.order[qpos] : qpos;
+    const long long own = tt * S.npairs + p;
     int B = 0, rem = p;
     while (B < S.nb && rem >= S.nb - B) {
         rem -= S.nb - B;
@@ -195,7 +197,7 @@ __device__ __forceinline__ void prepare_item(const trpdrv_dev_system *__restrict
     }
     const int C = B + rem;
     const int O = S.nocc, V = S.nvir;
-    const bool in_range = local >= 0 && tt < S.ntriples;
+    const bool in_range = local >= 0 && qpos < S.ntriples && tt >= 0 && tt < S.ntriples;
     const int packed = in_range ? S.triples[tt] : 0;
     const int i = packed & 1023, j = (packed >> 10) & 1023, k = (packed >> 20) & 1023;
     const bool ok = in_range && B < S.nb && C < S.nb && i < O && j < O && k < O && k <= i;
@@ -203,7 +205,7 @@ __device__ __forceinline__ void prepare_item(const trpdrv_dev_system *__restrict
         if (lane == 0) {
             atomicExch(status, 1);
             cx.state = 0;
-            cx.out = in_range ? S.partial + (size_t)local * NWARP * 4 : nullptr;
+            cx.out = in_range ? S.partial + (size_t)own * NWARP * 4 : nullptr;
             cx.nch = 0;
         }
         return;
@@ -262,7 +264,7 @@ __device__ __forceinline__ void prepare_item(const trpdrv_dev_system *__restrict
         cx.dintc2 = S.dintc + (size_t)k * V;
         cx.dintx2 = S.dintx + (size_t)k * V;
         cx.t1v2 = S.t1v + (size_t)k * V;
-        cx.out = S.partial + (size_t)local * NWARP * 4;
+        cx.out = S.partial + (size_t)own * NWARP * 4;
         // omp/ccsd_trpdrv_omp_cbody.c:126 (a is 1-based, i/j/k here 0-based)
         cx.eaijk = S.eorb[S.a - 1] - (S.eorb[S.ncor + i] + S.eorb[S.ncor + j] + S.eorb[S.ncor + k]);
         cx.ncor = S.ncor;

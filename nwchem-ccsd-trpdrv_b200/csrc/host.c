@@ -169,6 +169,7 @@ typedef struct sysbuf {
     double *own[TRPDRV_T_COUNT];     /* owned device copies made by upload */
     double *ntov, *nxov;             /* -tov, -xov */
     int32_t *d_triples, *h_triples;
+    int32_t *d_order;                /* fused processing order (trpdrv_processing_order) */
     int64_t ntriples;
     double *partial, *rec;
     int nb, npairs;
@@ -225,6 +226,7 @@ static void plan_free(trpdrv_plan *p)
             if (b->ntov) cudaFree(b->ntov);
             if (b->nxov) cudaFree(b->nxov);
             if (b->d_triples) cudaFree(b->d_triples);
+            if (b->d_order) cudaFree(b->d_order);
             if (b->partial) cudaFree(b->partial);
             if (b->rec) cudaFree(b->rec);
             free(b->h_triples);
@@ -281,7 +283,24 @@ static int plan_build(trpdrv_plan *p, const trpdrv_system *shape)
         }
         trpdrv_shard_triples(nocc, o->nkpass, o->rank, o->world, ijk);
         for (int64_t t = 0; t < n; ++t) b->h_triples[t] = pack_triple(ijk[3 * t], ijk[3 * t + 1], ijk[3 * t + 2]);
+        int32_t *order = NULL;
+        if (o->mode == TRPDRV_MODE_FUSED && n > 0) {
+            order = (int32_t *)malloc(sizeof(int32_t) * (size_t)n);
+            if (!order || trpdrv_processing_order(ijk, n, 0, order) != 0) {
+                free(order);
+                free(ijk);
+                return fail(TRPDRV_ERR_NOMEM, "host allocation failed");
+            }
+        }
         free(ijk);
+        if (order) {
+            const cudaError_t e1 = cudaMalloc((void **)&b->d_order, sizeof(int32_t) * (size_t)n);
+            const cudaError_t e2 = e1 == cudaSuccess ? cudaMemcpy(b->d_order, order, sizeof(int32_t) * (size_t)n,
+                                                                  cudaMemcpyHostToDevice)
+                                                     : e1;
+            free(order);
+            CUDA_TRY(e2);
+        }
 
         if (b->ntriples > 0) {
             CUDA_TRY(cudaMalloc((void **)&b->d_triples, sizeof(int32_t) * (size_t)b->ntriples));
@@ -307,6 +326,7 @@ static int plan_build(trpdrv_plan *p, const trpdrv_system *shape)
         d->ntriples = b->ntriples;
         d->item_begin = item;
         d->triples = b->d_triples;
+        d->order = b->d_order;
         d->partial = b->partial;
         d->rec = b->rec;
         d->ntov = b->ntov;

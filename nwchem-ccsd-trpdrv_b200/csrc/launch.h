@@ -31,7 +31,8 @@ typedef struct trpdrv_dev_system {
     int64_t ntriples;    /* triples of this system in the plan (this rank's share) */
     int64_t item_begin;  /* first fused work item of this system */
     const double *eorb, *t2, *jvv, *kvv, *ntov, *nxov, *jov, *kov, *dintc, *dintx, *t1v;
-    const int32_t *triples; /* packed triples, processing order */
+    const int32_t *triples; /* packed triples, driver order (energies are stored in this order) */
+    const int32_t *order;   /* fused kernels: processing position -> triple index, or NULL (identity) */
     double *partial;        /* [ntriples*npairs][TRPDRV_FUSED_SLOTS][4]: e4i, e5i, e4k, e5k */
     double *rec;            /* [ntriples][4] per triple */
 } trpdrv_dev_system;

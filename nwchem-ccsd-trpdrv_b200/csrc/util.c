@@ -5,6 +5,7 @@
 #include "trpdrv.h"
 
 #include <math.h>
+#include <stdint.h>
 #include <stdlib.h>
 #include <string.h>
 
@@ -93,6 +94,53 @@ int64_t trpdrv_shard_triples(int nocc, int nkpass, int rank, int world, int32_t 
     free(all);
     free(bounds);
     return hi - lo;
+}
+
+typedef struct order_key {
+    int64_t key;
+    int32_t idx;
+} order_key;
+
+static int order_key_cmp(const void *x, const void *y)
+{
+    const int64_t a = ((const order_key *)x)->key, b = ((const order_key *)y)->key;
+    return (a > b) - (a < b);
+}
+
+/* A triple (i, j, k) reads the slices of index i and of index k of T2[j], J, K, JOV[j], KOV[j], TOV
+ * and XOV (about 2.5 MB at nvir = 300, nocc = 40).  In the driver order (omp/test.c:160-165) every i
+ * sweeps k over 1..i, a cyclic walk over up to nocc slices that an LRU-like L2 cannot hold; here each
+ * block of i values stays resident while k streams past it, and consecutive blocks meet at the k
+ * slices the previous block touched last. */
+int trpdrv_processing_order(const int32_t *ijk, int64_t n, int block, int32_t *order)
+{
+    if (n < 0 || (n > 0 && (!ijk || !order)) || n > INT32_MAX) return -1;
+    if (block <= 0) block = 8;
+    order_key *ks = (order_key *)malloc(sizeof(order_key) * (size_t)(n > 0 ? n : 1));
+    if (!ks) return -1;
+    int64_t run = 0, nblocks = 0;
+    while (run < n) {
+        int64_t end = run + 1;
+        while (end < n && ijk[3 * end + 1] == ijk[3 * run + 1]) ++end;
+        int prev_blk = -1;
+        for (int64_t t = run; t < end; ++t) {
+            const int i = ijk[3 * t] - 1, k = ijk[3 * t + 2] - 1;
+            const int blk = i / block;
+            if (blk != prev_blk) {
+                ++nblocks;
+                prev_blk = blk;
+            }
+            /* the key sorts by block first, so any list (not only the driver's) gives a permutation */
+            const int64_t kk = (nblocks & 1) ? (int64_t)(k & 1023) : (int64_t)(1023 - (k & 1023));
+            ks[t].key = ((int64_t)(blk & 0xfffff) << 40) | (kk << 20) | (int64_t)(i & 0xfffff);
+            ks[t].idx = (int32_t)t;
+        }
+        qsort(ks + run, (size_t)(end - run), sizeof(order_key), order_key_cmp);
+        run = end;
+    }
+    for (int64_t t = 0; t < n; ++t) order[t] = ks[t].idx;
+    free(ks);
+    return 0;
 }
 
 double trpdrv_triple_flops(int nocc, int nvir)

@@ -101,6 +101,7 @@ _proto("trpdrv_count_triples", C.c_int64, [C.c_int])
 _proto("trpdrv_enumerate_triples", C.c_int64, [C.c_int, C.c_int, C.POINTER(C.c_int32)])
 _proto("trpdrv_partition", C.c_int, [_dp, C.c_int64, C.c_int, C.POINTER(C.c_int64)])
 _proto("trpdrv_shard_triples", C.c_int64, [C.c_int, C.c_int, C.c_int, C.c_int, C.POINTER(C.c_int32)])
+_proto("trpdrv_processing_order", C.c_int, [C.POINTER(C.c_int32), C.c_int64, C.c_int, C.POINTER(C.c_int32)])
 _proto("trpdrv_triple_flops", C.c_double, [C.c_int, C.c_int])
 _proto("trpdrv_tensor_elems", C.c_size_t, [C.c_int, C.c_int, C.c_int, C.c_int])
 _proto("trpdrv_synth_fill", C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int, C.c_uint64, C.c_int, _dp,
@@ -170,6 +171,17 @@ def shard_triples(nocc: int, nkpass: int, rank: int, world: int) -> np.ndarray:
     out = np.zeros((max(n, 1), 3), dtype=np.int32)
     lib.trpdrv_shard_triples(nocc, nkpass, rank, world, out.ctypes.data_as(C.POINTER(C.c_int32)))
     return out[:n]
+
+
+def processing_order(ijk: np.ndarray, block: int = 0) -> np.ndarray:
+    """Permutation position -> list index in which fused plans process the triples ijk ((n, 3), 1-based)."""
+    a = np.ascontiguousarray(ijk, dtype=np.int32).reshape(-1, 3)
+    out = np.zeros(max(len(a), 1), dtype=np.int32)
+    rc = lib.trpdrv_processing_order(a.ctypes.data_as(C.POINTER(C.c_int32)), len(a), block,
+                                     out.ctypes.data_as(C.POINTER(C.c_int32)))
+    if rc != 0:
+        raise TrpdrvError(1, "processing_order: bad arguments")
+    return out[:len(a)]
 
 
 def triple_flops(nocc: int, nvir: int) -> float:

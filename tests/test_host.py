@@ -96,3 +96,41 @@ def test_plan_argument_checks_precede_device_use(T):
     with pytest.raises(T.TrpdrvError) as ei:
         T.Plan([s], staging=5)
     assert ei.value.status == 1
+
+
+def _lru_misses(ijk, order, cap_slices):
+    """Slices (T2[j][x] per (j, x); J[x] and K[x] per x) that an LRU cache of cap_slices slices misses."""
+    from collections import OrderedDict
+    lru, miss = OrderedDict(), 0
+    for t in order:
+        i, j, k = (int(v) for v in ijk[t])
+        for key in (("t2", j, i), ("t2", j, k), ("jk", i), ("jk", k)):
+            if key in lru:
+                lru.move_to_end(key)
+            else:
+                miss += 1
+                lru[key] = 1
+                if len(lru) > cap_slices:
+                    lru.popitem(last=False)
+    return miss
+
+
+@pytest.mark.parametrize("nocc,nkpass,world", [(1, 1, 1), (7, 1, 1), (12, 3, 1), (20, 1, 3), (40, 1, 1)])
+def test_processing_order_is_a_permutation_that_keeps_slices_resident(T, nocc, nkpass, world):
+    for rank in range(world):
+        ijk = T.shard_triples(nocc, nkpass, rank, world)
+        order = T.processing_order(ijk)
+        assert np.array_equal(np.sort(order), np.arange(len(ijk)))
+        # the runs of equal j stay whole: one j's T2 slices at a time
+        js = ijk[order, 1]
+        assert np.count_nonzero(np.diff(js)) == np.count_nonzero(np.diff(ijk[:, 1]))
+    if nocc == 40:
+        # with room for 24 slices the driver order re-reads most of them; the blocked order does not
+        ident = np.arange(len(ijk))
+        assert _lru_misses(ijk, order, 24) * 4 < _lru_misses(ijk, ident, 24)
+
+
+def test_processing_order_rejects_bad_arguments(T):
+    assert T.lib.trpdrv_processing_order(None, 3, 0, None) == -1
+    assert T.lib.trpdrv_processing_order(None, -1, 0, None) == -1
+    assert len(T.processing_order(np.zeros((0, 3), np.int32))) == 0

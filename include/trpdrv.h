@@ -140,7 +140,9 @@ int trpdrv_version(void);                  /* major*10000 + minor*100 + patch */
 /* Execution modes. */
 enum {
     TRPDRV_MODE_PLAIN = 0,  /* per triple: one grouped launch of the 16 FP64 GEMMs (f to HBM) + tengy */
-    TRPDRV_MODE_FUSED = 1   /* persistent kernel over (triple, tile-pair) work items; f stays on chip */
+    TRPDRV_MODE_FUSED = 1,  /* persistent kernel over (triple, tile-pair) work items; f stays on chip */
+    TRPDRV_MODE_EMULATED = 2 /* emulated FP64: Ozaki int8 digit slices on the tensor cores (tcgen05),
+                                exact int32 sums, FP64 recombination; FP64 energies (see `slices`) */
 };
 
 /* One system: all (i,j,k) triples of one fixed virtual `a`, every reference pointer a slice:
@@ -174,7 +176,9 @@ typedef struct trpdrv_options {
     int staging;      /* fused-kernel operand staging: 0 = TMA where supported (even nvir and nocc,
                          16-byte aligned tensors, <= 8 systems), else cp.async; 1 = cp.async; 2 = TMA
                          or fail with TRPDRV_ERR_UNSUPPORTED */
-    int reserved[6];
+    int slices;       /* EMULATED: base-128 digits per operand element, 4..8; 0 = default (7) */
+    int batch;        /* EMULATED: triples whose f share one device buffer per launch pair; 0 = default (8) */
+    int reserved[4];
 } trpdrv_options;
 
 void trpdrv_options_default(trpdrv_options *opt);

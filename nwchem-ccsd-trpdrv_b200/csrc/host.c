@@ -117,6 +117,7 @@ static int ensure_device(int device, int *out_dev, int *out_nsm)
         rc = trpdrv_fused_init();
         if (!rc) rc = trpdrv_fused_tma_init();
         if (!rc) rc = trpdrv_plain_init();
+        if (!rc) rc = trpdrv_oz_init();
         if (!rc) g_init_done[dev] = 1;
     }
     pthread_mutex_unlock(&g_init_mu);
@@ -169,7 +170,9 @@ typedef struct sysbuf {
     double *own[TRPDRV_T_COUNT];     /* owned device copies made by upload */
     double *ntov, *nxov;             /* -tov, -xov */
     int32_t *d_triples, *h_triples;
-    int32_t *d_order;                /* fused processing order (trpdrv_processing_order) */
+    int32_t *d_order;                /* fused/emulated processing order (trpdrv_processing_order) */
+    trpdrv_oz_system oz;             /* emulated form: digit slices and scales (device) */
+    void *oz_maps;                   /* emulated form: tensor maps of oz.sa / oz.sb (host blob) */
     int64_t ntriples;
     double *partial, *rec;
     int nb, npairs;
@@ -195,6 +198,7 @@ struct trpdrv_plan {
     int64_t last_launches;
     cudaStream_t last_stream;
     int use_tma;        /* the fused launch stages panels with TMA (fused_tma.cu) */
+    double *d_fbuf;     /* emulated form: f of one batch of triples [batch][8][nvir][nvir] */
     void *tma_maps;     /* tensor maps of every system, passed by value to each launch */
 };
 
@@ -211,6 +215,8 @@ void trpdrv_options_default(trpdrv_options *opt)
     opt->ctas_per_sm = 0;
     opt->use_graph = 1;
     opt->mma_k = 8;
+    opt->slices = 7;
+    opt->batch = 8;
 }
 
 static void plan_free(trpdrv_plan *p)
@@ -227,6 +233,11 @@ static void plan_free(trpdrv_plan *p)
             if (b->nxov) cudaFree(b->nxov);
             if (b->d_triples) cudaFree(b->d_triples);
             if (b->d_order) cudaFree(b->d_order);
+            if (b->oz.sa) cudaFree(b->oz.sa);
+            if (b->oz.sb) cudaFree(b->oz.sb);
+            if (b->oz.ea) cudaFree(b->oz.ea);
+            if (b->oz.eb) cudaFree(b->oz.eb);
+            free(b->oz_maps);
             if (b->partial) cudaFree(b->partial);
             if (b->rec) cudaFree(b->rec);
             free(b->h_triples);
@@ -240,6 +251,7 @@ static void plan_free(trpdrv_plan *p)
     if (p->d_status) cudaFree(p->d_status);
     if (p->d_tot) cudaFree(p->d_tot);
     if (p->d_f) cudaFree(p->d_f);
+    if (p->d_fbuf) cudaFree(p->d_fbuf);
     if (p->d_bpart) cudaFree(p->d_bpart);
     if (p->d_tcount) cudaFree(p->d_tcount);
     if (p->ev0) cudaEventDestroy(p->ev0);
@@ -284,7 +296,7 @@ static int plan_build(trpdrv_plan *p, const trpdrv_system *shape)
         trpdrv_shard_triples(nocc, o->nkpass, o->rank, o->world, ijk);
         for (int64_t t = 0; t < n; ++t) b->h_triples[t] = pack_triple(ijk[3 * t], ijk[3 * t + 1], ijk[3 * t + 2]);
         int32_t *order = NULL;
-        if (o->mode == TRPDRV_MODE_FUSED && n > 0) {
+        if (o->mode != TRPDRV_MODE_PLAIN && n > 0) {
             order = (int32_t *)malloc(sizeof(int32_t) * (size_t)n);
             if (!order || trpdrv_processing_order(ijk, n, 0, order) != 0) {
                 free(order);
@@ -308,11 +320,25 @@ static int plan_build(trpdrv_plan *p, const trpdrv_system *shape)
                                 cudaMemcpyHostToDevice));
             CUDA_TRY(cudaMalloc((void **)&b->rec, sizeof(double) * 4 * (size_t)b->ntriples));
             CUDA_TRY(cudaMemset(b->rec, 0, sizeof(double) * 4 * (size_t)b->ntriples));
-            if (o->mode == TRPDRV_MODE_FUSED)
+            if (o->mode != TRPDRV_MODE_PLAIN)
                 CUDA_TRY(cudaMalloc((void **)&b->partial, sizeof(double) * 4 * TRPDRV_FUSED_SLOTS *
                                                        (size_t)b->ntriples * b->npairs));
         }
         const size_t ov = (size_t)nocc * nocc * nvir;
+        if (o->mode == TRPDRV_MODE_EMULATED) {
+            trpdrv_oz_system *z = &b->oz;
+            z->nocc = nocc;
+            z->nvir = nvir;
+            z->slices = o->slices;
+            z->dp = trpdrv_oz_dp(nocc, nvir);
+            const size_t rows = 2 * (size_t)nvir, per = (size_t)o->slices * rows * (size_t)z->dp;
+            CUDA_TRY(cudaMalloc((void **)&z->sa, per * (size_t)nocc));
+            CUDA_TRY(cudaMalloc((void **)&z->sb, per * (size_t)nocc * nocc));
+            CUDA_TRY(cudaMalloc((void **)&z->ea, sizeof(double) * rows * (size_t)nocc));
+            CUDA_TRY(cudaMalloc((void **)&z->eb, sizeof(double) * rows * (size_t)nocc * nocc));
+            b->oz_maps = aligned_alloc(64, (trpdrv_oz_maps_bytes() + 63) & ~(size_t)63);
+            if (!b->oz_maps) return fail(TRPDRV_ERR_NOMEM, "host allocation failed");
+        }
         CUDA_TRY(cudaMalloc((void **)&b->ntov, sizeof(double) * ov));
         CUDA_TRY(cudaMalloc((void **)&b->nxov, sizeof(double) * ov));
 
@@ -341,6 +367,8 @@ static int plan_build(trpdrv_plan *p, const trpdrv_system *shape)
     CUDA_TRY(cudaMemset(p->d_status, 0, sizeof(int)));
     CUDA_TRY(cudaMalloc((void **)&p->d_tot, sizeof(double) * 4 * (size_t)p->nsys));
     CUDA_TRY(cudaMemset(p->d_tot, 0, sizeof(double) * 4 * (size_t)p->nsys));
+    if (o->mode == TRPDRV_MODE_EMULATED)
+        CUDA_TRY(cudaMalloc((void **)&p->d_fbuf, sizeof(double) * 8 * (size_t)o->batch * maxv * maxv));
     if (o->mode == TRPDRV_MODE_PLAIN) {
         CUDA_TRY(cudaMalloc((void **)&p->d_f, sizeof(double) * 8 * (size_t)maxv * maxv));
         CUDA_TRY(cudaMalloc((void **)&p->d_bpart, sizeof(double) * 4 * (size_t)maxpairs));
@@ -373,8 +401,13 @@ int trpdrv_plan_create(trpdrv_plan **plan, const trpdrv_system *shape, int nsys,
         o = *opt;
     else
         trpdrv_options_default(&o);
-    if (o.mode != TRPDRV_MODE_PLAIN && o.mode != TRPDRV_MODE_FUSED)
+    if (o.mode != TRPDRV_MODE_PLAIN && o.mode != TRPDRV_MODE_FUSED && o.mode != TRPDRV_MODE_EMULATED)
         return fail(TRPDRV_ERR_ARG, "unknown mode %d", o.mode);
+    if (o.slices == 0) o.slices = 7;
+    if (o.batch == 0) o.batch = 8;
+    if (!trpdrv_oz_slices_supported(o.slices))
+        return fail(TRPDRV_ERR_ARG, "slices %d: must be %d..%d", o.slices, TRPDRV_OZ_MIN_SLICES, TRPDRV_OZ_MAX_SLICES);
+    if (o.batch < 1 || o.batch > 4096) return fail(TRPDRV_ERR_ARG, "batch %d: must be 1..4096", o.batch);
     if (o.world < 1 || o.rank < 0 || o.rank >= o.world)
         return fail(TRPDRV_ERR_ARG, "rank %d / world %d", o.rank, o.world);
     if (o.tile != 0 && o.tile != TRPDRV_TILE)
@@ -425,6 +458,19 @@ static int plan_publish(trpdrv_plan *p)
         LAUNCH_TRY(trpdrv_launch_negate(b->t[TRPDRV_T_TOV], b->ntov, ov, p->stream));
         LAUNCH_TRY(trpdrv_launch_negate(b->t[TRPDRV_T_XOV], b->nxov, ov, p->stream));
     }
+    if (p->opt.mode == TRPDRV_MODE_EMULATED) {
+        for (int q = 0; q < p->nsys; ++q) {
+            const int e = trpdrv_oz_prepare(&p->s[q].oz, p->s[q].oz_maps);
+            if (e) return fail(TRPDRV_ERR_CUDA, "tensor-map encoding failed (%d)", e);
+        }
+    }
+    if (p->opt.mode != TRPDRV_MODE_PLAIN && p->graph_ready) { /* the graph holds the old parameters */
+        cudaGraphExecDestroy(p->gexec);
+        cudaGraphDestroy(p->graph);
+        p->gexec = NULL;
+        p->graph = NULL;
+        p->graph_ready = 0;
+    }
     if (p->opt.mode == TRPDRV_MODE_FUSED) {
         const int want = p->opt.staging;
         const int ok = want != 1 && trpdrv_tma_supported(p->h_dev, p->nsys);
@@ -440,14 +486,6 @@ static int plan_publish(trpdrv_plan *p)
             if (e) return fail(TRPDRV_ERR_CUDA, "tensor-map encoding failed (%d)", e);
         }
         p->use_tma = ok;
-        /* a captured graph holds the previous launch parameters */
-        if (p->graph_ready) {
-            cudaGraphExecDestroy(p->gexec);
-            cudaGraphDestroy(p->graph);
-            p->gexec = NULL;
-            p->graph = NULL;
-            p->graph_ready = 0;
-        }
     }
     CUDA_TRY(cudaMemcpyAsync(p->d_dev, p->h_dev, sizeof(trpdrv_dev_system) * (size_t)p->nsys,
                              cudaMemcpyHostToDevice, p->stream));
@@ -532,6 +570,43 @@ static int enqueue_fused(trpdrv_plan *p, cudaStream_t st, int capturing)
     }
     p->last_launches = launches;
     return TRPDRV_OK;
+}
+
+/* Emulated form: slice every operand once per execution, then per batch of `batch` triples (in the
+ * processing order) one contraction launch writing their f and one tengy launch. */
+static int enqueue_emulated(trpdrv_plan *p, cudaStream_t st, int capturing)
+{
+    int64_t launches = 0;
+    CUDA_TRY(cudaMemsetAsync(p->d_status, 0, sizeof(int), st));
+    CUDA_TRY(cudaMemsetAsync(p->d_tot, 0, sizeof(double) * 4 * (size_t)p->nsys, st));
+    CUDA_TRY(cudaEventRecordWithFlags(p->ev0, st, capturing ? cudaEventRecordExternal : cudaEventRecordDefault));
+    for (int q = 0; q < p->nsys; ++q) {
+        const trpdrv_dev_system *d = &p->h_dev[q];
+        const sysbuf *b = &p->s[q];
+        if (d->ntriples <= 0) continue;
+        LAUNCH_TRY(trpdrv_launch_oz_slices(d, &b->oz, st));
+        ++launches;
+        for (int64_t pos = 0; pos < d->ntriples; pos += p->opt.batch) {
+            const int n = (int)(d->ntriples - pos < p->opt.batch ? d->ntriples - pos : p->opt.batch);
+            LAUNCH_TRY(trpdrv_launch_oz_gemm(d, &b->oz, b->oz_maps, pos, n, p->d_fbuf, p->d_status, st));
+            LAUNCH_TRY(trpdrv_launch_oz_tengy(d, pos, n, p->d_fbuf, st));
+            launches += 2;
+        }
+    }
+    CUDA_TRY(cudaEventRecordWithFlags(p->ev1, st, capturing ? cudaEventRecordExternal : cudaEventRecordDefault));
+    for (int q = 0; q < p->nsys; ++q) {
+        if (p->h_dev[q].ntriples <= 0) continue;
+        LAUNCH_TRY(trpdrv_launch_item_reduce(&p->h_dev[q], st));
+        LAUNCH_TRY(trpdrv_launch_system_reduce(p->s[q].rec, p->s[q].d_triples, p->s[q].ntriples, p->d_tot + 4 * q, st));
+        launches += 2;
+    }
+    p->last_launches = launches;
+    return TRPDRV_OK;
+}
+
+static int enqueue_device(trpdrv_plan *p, cudaStream_t st, int capturing)
+{
+    return p->opt.mode == TRPDRV_MODE_EMULATED ? enqueue_emulated(p, st, capturing) : enqueue_fused(p, st, capturing);
 }
 
 static int enqueue_plain(trpdrv_plan *p, cudaStream_t st)
@@ -621,7 +696,7 @@ int trpdrv_plan_execute(trpdrv_plan *p, void *stream)
     } else if (p->opt.use_graph) {
         if (!p->graph_ready) {
             CUDA_TRY(cudaStreamBeginCapture(p->stream, cudaStreamCaptureModeThreadLocal));
-            const int rc = enqueue_fused(p, p->stream, 1);
+            const int rc = enqueue_device(p, p->stream, 1);
             cudaGraph_t g = NULL;
             const cudaError_t ce = cudaStreamEndCapture(p->stream, &g);
             if (rc != TRPDRV_OK) {
@@ -635,7 +710,7 @@ int trpdrv_plan_execute(trpdrv_plan *p, void *stream)
         }
         CUDA_TRY(cudaGraphLaunch(p->gexec, st));
     } else {
-        TRY(enqueue_fused(p, st, 0));
+        TRY(enqueue_device(p, st, 0));
     }
     p->events_valid = 1;
     return TRPDRV_OK;
@@ -648,7 +723,7 @@ static int plan_wait(trpdrv_plan *p)
     int status = 0;
     CUDA_TRY(cudaMemcpy(&status, p->d_status, sizeof(int), cudaMemcpyDeviceToHost));
     if (status & 2) return fail(TRPDRV_ERR_DEVICE, "a fused-kernel pipeline wait ran out of time");
-    if (status) return fail(TRPDRV_ERR_DEVICE, "the fused kernel rejected a malformed work-queue entry");
+    if (status) return fail(TRPDRV_ERR_DEVICE, "a device kernel rejected a malformed work-queue entry");
     return TRPDRV_OK;
 }
 

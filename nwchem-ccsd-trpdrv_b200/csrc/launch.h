@@ -62,6 +62,33 @@ int trpdrv_launch_fused_tma(const trpdrv_dev_system *d_sys, int nsys, int64_t to
                             void *stream);
 int trpdrv_fused_tma_init(void);
 
+/* Emulated-FP64 (Ozaki int8) form, ozaki.cu.  Per system: digit slices of the A operands
+ * sa [nocc][slices][2 nvir][dp] and of the B operands sb [nocc*nocc][slices][2 nvir][dp] (int8,
+ * dp = trpdrv_oz_dp: nvir + nocc rounded up to 32), with power-of-two scales ea [nocc][2 nvir] and
+ * eb [nocc*nocc][2 nvir].  trpdrv_oz_prepare encodes the two tensor maps into a host blob of
+ * trpdrv_oz_maps_bytes() bytes (64-byte aligned).  A batch is npos consecutive positions of the
+ * system's processing order starting at pos0: the contraction kernel writes their f into
+ * fbuf [npos][8][nvir][nvir] and the tengy kernel writes each triple's energies into slot 0 of
+ * its items in `partial` (slots 1..7 zero), for trpdrv_launch_item_reduce.  *status as the fused
+ * kernels (bit 0 malformed entry, bit 1 a wait ran out). */
+#define TRPDRV_OZ_MIN_SLICES 4
+#define TRPDRV_OZ_MAX_SLICES 8
+typedef struct trpdrv_oz_system {
+    int nocc, nvir, slices, dp;
+    signed char *sa, *sb;
+    double *ea, *eb;
+} trpdrv_oz_system;
+int trpdrv_oz_slices_supported(int slices);
+int trpdrv_oz_dp(int nocc, int nvir);
+size_t trpdrv_oz_maps_bytes(void);
+int trpdrv_oz_prepare(const trpdrv_oz_system *oz, void *maps_out);
+int trpdrv_launch_oz_slices(const trpdrv_dev_system *h_sys, const trpdrv_oz_system *oz, void *stream);
+int trpdrv_launch_oz_gemm(const trpdrv_dev_system *h_sys, const trpdrv_oz_system *oz, const void *maps,
+                          int64_t pos0, int npos, double *fbuf, int *status, void *stream);
+int trpdrv_launch_oz_tengy(const trpdrv_dev_system *h_sys, int64_t pos0, int npos, const double *fbuf,
+                           void *stream);
+int trpdrv_oz_init(void);
+
 /* Per-triple sum of the per-item energies of one system (partial -> rec). */
 int trpdrv_launch_item_reduce(const trpdrv_dev_system *h_sys, void *stream);
 

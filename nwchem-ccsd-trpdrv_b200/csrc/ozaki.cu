@@ -1,0 +1,667 @@
+// Emulated-FP64 form of the triples body (sm_100a): Ozaki splitting of every contraction into int8
+// digit slices on the 5th-generation tensor cores, exact int32 accumulation in tensor memory, FP64
+// recombination; energy denominators and sums stay in native FP64.
+//
+// Each of the eight f of a triple is one contraction over d = [virtual | occupied]
+// (omp/ccsd_trpdrv_omp_cbody.c:70-117 with the occupied A operand negated, as in the fused kernels).
+// The emulation:
+//  * every row of an A operand and every column of a B operand is scaled by a power of two 2^e chosen
+//    so that its largest element has magnitude in [1/4, 1/2), then written as S signed base-128
+//    digits x = 2^e * sum_{p=1..S} d_p 2^(-7p) with |d_p| <= 64 (each digit rounded to nearest, so the
+//    remainder after S digits is at most 2^(e-7S-1));
+//  * products of digit slices with p + q <= S + 1 are accumulated on the tensor cores
+//    (tcgen05.mma kind::i8, int32 accumulators in TMEM).  Pairs with equal p + q carry the same
+//    weight and share one accumulator; |sum| <= S * dp * 64 * 64 < 2^31, so the integer sums are exact;
+//  * the S level sums are recombined in FP64: f = 2^(eA + eB) * sum_L 2^(-7L) C_L.
+// f of a batch of triples go to a device buffer (L2-sized) and the batched tengy kernel reduces
+// them in FP64 exactly like the plain path (omp/ccsd_tengy_c99.c:5-119).
+//
+// Operand slices (int8, contraction index d contiguous, zero-padded to dp, a multiple of 32):
+//   SA[x][p][r][d]:      r < V: [J(x) | -TOV(x)] row r;       r >= V: [K(x) | -XOV(x)] row r - V
+//   SB[j*O+y][p][c][d]:  c < V: [T2[j][y]^T ; KOV[j][y]] col c; c >= V: [T2[j][y] ; JOV[j][y]] col c - V
+// The n-group of triple (i, j, k) is SA[i] x SB[j,k] and its t-group SA[k] x SB[j,i]; the 2V x 2V
+// product [A1; A2] [B1 | B3] holds the four f of the group in its quadrants:
+//   f1n = A1 B1, f2n = A2 B1, f3n = A1 B3, f4n = A2 B3 (and f1t..f4t likewise).
+//
+// Contraction kernel: one CTA per 128 x 64 output tile of one (triple, group).  Warp 0 issues TMA
+// loads (64-byte swizzle) of all S digit slices of A and B for 64 contraction indices per stage;
+// warp 1 allocates tensor memory and one of its threads issues every MMA (M=128, N=64, K=32) into S
+// level accumulators (S*64 columns); warps 2-5 wait for the last MMA, read the accumulators with
+// tcgen05.ld and recombine them in FP64.  Every wait is bounded (globaltimer) and reports through
+// *status; tensor memory is released on every path.
+
+#include <cuda.h>
+#include <cudaTypedefs.h>
+
+#include "device_common.cuh"
+#include "launch.h"
+#include "tengy_tile.cuh"
+
+namespace trpdrv {
+namespace oz {
+
+constexpr int BM = 128;         // output rows per tile (TMEM lanes)
+constexpr int BN = 64;          // output columns per tile (TMEM columns per level)
+constexpr int KC = 64;          // contraction bytes (= int8 indices) per stage
+constexpr int KSTEP = 32;       // contraction indices per MMA
+constexpr int NTHREAD = 192;    // warp 0 TMA, warp 1 MMA + TMEM, warps 2-5 recombination
+constexpr unsigned SLICE_A = BM * KC;
+constexpr unsigned SLICE_B = BN * KC;
+constexpr int SMEM_AVAIL = 227 * 1024 - 2048;
+constexpr unsigned long long WAIT_LIMIT_NS = 4000000000ull;
+
+template <int S>
+struct Cfg {
+    static constexpr unsigned STAGE = S * (SLICE_A + SLICE_B);
+    static constexpr int FIT = SMEM_AVAIL / (int)STAGE;
+    static constexpr int STAGES = FIT > 4 ? 4 : FIT;
+    static constexpr size_t SMEM = (size_t)STAGES * STAGE + 1024;
+    static constexpr unsigned TMEM_COLS = S * BN <= 256 ? 256u : 512u;
+    static_assert(STAGES >= 2, "fewer than two stages fit");
+    static_assert(S * BN <= 512, "level accumulators exceed tensor memory");
+};
+
+// instruction descriptor, kind::i8: D s32 (bits 4-5 = 2), A and B signed (bits 7-9, 10-12 = 1),
+// both K-major (bits 15, 16 = 0), N >> 3 at bits 17-22, M >> 4 at bits 24-28
+constexpr unsigned IDESC = (2u << 4) | (1u << 7) | (1u << 10) | ((unsigned)(BN >> 3) << 17) |
+                           ((unsigned)(BM >> 4) << 24);
+
+struct GemmParams {
+    CUtensorMap mapA, mapB;  // 64-byte aligned members first
+    const double *ea, *eb;   // power-of-two scales per A row / B column
+    const int32_t *triples, *order;
+    long long pos0, ntriples;
+    double *fbuf;            // [batch][8][V][V]
+    int V, O, nks, mtiles;
+    int *status;
+};
+
+// ------------------------------------------------------------------------------------------------
+// PTX helpers
+// ------------------------------------------------------------------------------------------------
+__device__ __forceinline__ unsigned saddr(const void *p) { return (unsigned)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ unsigned long long globaltimer()
+{
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+__device__ __forceinline__ void mbar_init(unsigned long long *b, unsigned count)
+{
+    asm volatile("mbarrier.init.shared.b64 [%0], %1;" ::"r"(saddr(b)), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive_expect_tx(unsigned long long *b, unsigned bytes)
+{
+    asm volatile("mbarrier.arrive.expect_tx.shared.b64 _, [%0], %1;" ::"r"(saddr(b)), "r"(bytes) : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(unsigned long long *b, unsigned parity)
+{
+    unsigned ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(ok)
+        : "r"(saddr(b)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+
+// Bounded wait; false (and status bit 1) when it runs out.
+__device__ __forceinline__ bool mbar_wait(unsigned long long *b, unsigned parity, int *status)
+{
+    if (mbar_try_wait(b, parity)) return true;
+    const unsigned long long t0 = globaltimer();
+    for (;;) {
+#pragma unroll 1
+        for (int spin = 0; spin < 256; ++spin)
+            if (mbar_try_wait(b, parity)) return true;
+        if (globaltimer() - t0 > WAIT_LIMIT_NS) {
+            atomicOr(status, 2);
+            return false;
+        }
+    }
+}
+
+__device__ __forceinline__ void tma_load_3d(void *dst, const CUtensorMap *map, unsigned long long *bar, int x, int y,
+                                            int z)
+{
+    asm volatile(
+        "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4, %5}], [%2];"
+        ::"r"(saddr(dst)), "l"(map), "r"(saddr(bar)), "r"(x), "r"(y), "r"(z)
+        : "memory");
+}
+
+__device__ __forceinline__ void tmem_alloc(unsigned *dst, unsigned ncols)
+{
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(saddr(dst)), "r"(ncols)
+                 : "memory");
+}
+
+__device__ __forceinline__ void tmem_relinquish()
+{
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+}
+
+__device__ __forceinline__ void tmem_dealloc(unsigned taddr, unsigned ncols)
+{
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(taddr), "r"(ncols) : "memory");
+}
+
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+
+// K-major operand tile in shared memory with the 64-byte swizzle: rows of 64 bytes, 8-row atoms of
+// 512 bytes (stride byte offset 512), leading byte offset unused (1), descriptor version 1.
+__device__ __forceinline__ unsigned long long sdesc_sw64(const void *p)
+{
+    const unsigned a = saddr(p);
+    return (unsigned long long)((a >> 4) & 0x3FFFu) | (1ull << 16) | ((unsigned long long)(512 >> 4) << 32) |
+           (1ull << 46) | (4ull << 61);
+}
+
+__device__ __forceinline__ void mma_i8(unsigned d, unsigned long long a, unsigned long long b, int accumulate)
+{
+    asm volatile(
+        "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
+        " tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n}\n" ::"r"(d),
+        "l"(a), "l"(b), "r"(IDESC), "r"(accumulate), "r"(0), "r"(0), "r"(0), "r"(0)
+        : "memory");
+}
+
+__device__ __forceinline__ void mma_commit(unsigned long long *bar)
+{
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(saddr(bar))
+                 : "memory");
+}
+
+// 32 lanes x 16 columns of 32 bits; the wait names the registers so that no use moves above it
+__device__ __forceinline__ void tmem_ld16(unsigned taddr, unsigned (&v)[16])
+{
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
+        "%15}, [%16];"
+        : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
+          "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
+        : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;"
+                 : "+r"(v[0]), "+r"(v[1]), "+r"(v[2]), "+r"(v[3]), "+r"(v[4]), "+r"(v[5]), "+r"(v[6]), "+r"(v[7]),
+                   "+r"(v[8]), "+r"(v[9]), "+r"(v[10]), "+r"(v[11]), "+r"(v[12]), "+r"(v[13]), "+r"(v[14]),
+                   "+r"(v[15])
+                 :
+                 : "memory");
+}
+
+// ------------------------------------------------------------------------------------------------
+// contraction kernel
+// ------------------------------------------------------------------------------------------------
+template <int S>
+__global__ void __launch_bounds__(NTHREAD, 1) oz_gemm_kernel(const __grid_constant__ GemmParams P)
+{
+    using C = Cfg<S>;
+    extern __shared__ char smem_raw[];
+    __shared__ __align__(8) unsigned long long full[C::STAGES], empty[C::STAGES], accf[1];
+    __shared__ unsigned tmem_sh;
+    char *stages = reinterpret_cast<char *>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~(uintptr_t)1023);
+
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int y = blockIdx.y, grp = y & 1;
+    const long long pos = P.pos0 + (y >> 1);
+    const long long tt = (pos < P.ntriples) ? (P.order ? (long long)P.order[pos] : pos) : -1;
+    const int packed = (tt >= 0 && tt < P.ntriples) ? P.triples[tt] : -1;
+    const int i = packed & 1023, j = (packed >> 10) & 1023, k = (packed >> 20) & 1023;
+    if (packed < 0 || i >= P.O || j >= P.O || k >= P.O) {  // uniform over the CTA: nothing allocated yet
+        if (tid == 0) atomicOr(P.status, 1);
+        return;
+    }
+    const int planeA = grp ? k : i, planeB = j * P.O + (grp ? i : k);
+    const int mt = blockIdx.x % P.mtiles, nt = blockIdx.x / P.mtiles;
+    const int m0 = mt * BM, n0 = nt * BN;
+    const int nchunks = (P.nks * KSTEP + KC - 1) / KC;
+
+    if (tid == 0) {
+        for (int s = 0; s < C::STAGES; ++s) {
+            mbar_init(&full[s], 1);
+            mbar_init(&empty[s], 1);
+        }
+        mbar_init(accf, 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 1) {
+        tmem_alloc(&tmem_sh, C::TMEM_COLS);
+        tmem_relinquish();
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const unsigned tmem = tmem_sh;
+
+    if (warp == 0) {
+        if (lane == 0) {  // TMA producer
+            int stage = 0;
+            unsigned phase = 0;
+            for (int kc = 0; kc < nchunks; ++kc) {
+                if (!mbar_wait(&empty[stage], phase ^ 1, P.status)) break;
+                mbar_arrive_expect_tx(&full[stage], C::STAGE);
+                char *sA = stages + (size_t)stage * C::STAGE, *sB = sA + S * SLICE_A;
+#pragma unroll
+                for (int p = 0; p < S; ++p)
+                    tma_load_3d(sA + p * SLICE_A, &P.mapA, &full[stage], kc * KC, m0, planeA * S + p);
+#pragma unroll
+                for (int q = 0; q < S; ++q)
+                    tma_load_3d(sB + q * SLICE_B, &P.mapB, &full[stage], kc * KC, n0, planeB * S + q);
+                if (++stage == C::STAGES) {
+                    stage = 0;
+                    phase ^= 1;
+                }
+            }
+        }
+        __syncwarp();
+    } else if (warp == 1) {
+        if (lane == 0) {  // MMA issuer: level L = p + q (0-based) accumulates at columns L*BN..
+            int stage = 0;
+            unsigned phase = 0;
+            for (int kc = 0; kc < nchunks; ++kc) {
+                if (!mbar_wait(&full[stage], phase, P.status)) break;
+                tc_fence_after();
+                const char *sA = stages + (size_t)stage * C::STAGE, *sB = sA + S * SLICE_A;
+                const unsigned long long dA = sdesc_sw64(sA), dB = sdesc_sw64(sB);
+#pragma unroll
+                for (int ks = 0; ks < KC / KSTEP; ++ks) {
+                    const int kg = kc * (KC / KSTEP) + ks;
+                    if (kg < P.nks) {
+#pragma unroll
+                        for (int p = 0; p < S; ++p)
+#pragma unroll
+                            for (int q = 0; p + q < S; ++q)
+                                mma_i8(tmem + (unsigned)((p + q) * BN),
+                                       dA + (unsigned long long)(p * (SLICE_A >> 4) + ks * (KSTEP >> 4)),
+                                       dB + (unsigned long long)(q * (SLICE_B >> 4) + ks * (KSTEP >> 4)),
+                                       (kg > 0 || p > 0) ? 1 : 0);
+                    }
+                }
+                mma_commit(&empty[stage]);  // the stage is free once these MMAs have read it
+                if (++stage == C::STAGES) {
+                    stage = 0;
+                    phase ^= 1;
+                }
+            }
+            mma_commit(accf);  // tracks every MMA issued, also after an early stop
+        }
+        __syncwarp();
+    } else {  // recombination: this warp reads TMEM lanes 32*(warp%4)..
+        const int qd = warp & 3;
+        const bool ok = mbar_wait(accf, 0, P.status);
+        tc_fence_after();
+        if (ok) {
+            double acc[BN];
+#pragma unroll
+            for (int c = 0; c < BN; ++c) acc[c] = 0.0;
+            double w = 1.0 / 16384.0;  // level 0 (p = q = 1) carries 2^-14; each level after it 2^-7 less
+#pragma unroll
+            for (int L = 0; L < S; ++L) {
+#pragma unroll
+                for (int cb = 0; cb < BN / 16; ++cb) {
+                    unsigned v[16];
+                    tmem_ld16(tmem + ((unsigned)(qd * 32) << 16) + (unsigned)(L * BN + cb * 16), v);
+#pragma unroll
+                    for (int u = 0; u < 16; ++u) acc[cb * 16 + u] = fma((double)(int)v[u], w, acc[cb * 16 + u]);
+                }
+                w *= 1.0 / 128.0;
+            }
+            const int V = P.V, r = m0 + qd * 32 + lane;
+            if (r < 2 * V) {
+                const size_t vv = (size_t)V * V;
+                const double sa = P.ea[(size_t)planeA * 2 * V + r];
+                const int rh = r >= V ? 1 : 0, b = r - rh * V;
+                double *fj = P.fbuf + (size_t)(y >> 1) * 8 * vv + (size_t)grp * 4 * vv;
+                const double *eb = P.eb + (size_t)planeB * 2 * V;
+#pragma unroll
+                for (int c = 0; c < BN; ++c) {
+                    const int col = n0 + c;
+                    if (col < 2 * V) {
+                        const int ch = col >= V ? 1 : 0, cc = col - ch * V;
+                        fj[(size_t)(rh + 2 * ch) * vv + b + (size_t)cc * V] = acc[c] * sa * __ldg(eb + col);
+                    }
+                }
+            }
+        }
+    }
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 1) {
+        tc_fence_after();
+        tmem_dealloc(tmem, C::TMEM_COLS);
+    }
+}
+
+// ------------------------------------------------------------------------------------------------
+// slicing: power-of-two scale per row and S base-128 digits per element
+// ------------------------------------------------------------------------------------------------
+struct SliceParams {
+    const double *t2, *jvv, *kvv, *ntov, *nxov, *jov, *kov;
+    signed char *out;  // [planes][S][2V][dp]
+    double *scale;     // [planes][2V]
+    int V, O, S, dp;
+};
+
+// One element of row r of plane `plane`; A side (SIDE 0) or B side (SIDE 1).
+template <int SIDE>
+__device__ __forceinline__ double slice_src(const SliceParams &P, int plane, int r, int d)
+{
+    const int V = P.V, O = P.O;
+    const int h = r >= V ? 1 : 0, x = r - h * V;
+    const size_t vv = (size_t)V * V, ov = (size_t)O * V;
+    if (SIDE == 0) {
+        if (d < V) return (h ? P.kvv : P.jvv)[plane * vv + x + (size_t)d * V];
+        return (h ? P.nxov : P.ntov)[plane * ov + x + (size_t)(d - V) * V];
+    }
+    if (d < V) return h ? P.t2[plane * vv + d + (size_t)x * V] : P.t2[plane * vv + x + (size_t)d * V];
+    return (h ? P.jov : P.kov)[plane * ov + (d - V) + (size_t)x * O];
+}
+
+// whether row index is the contiguous one in memory for this tile (coalescing only)
+template <int SIDE>
+__device__ __forceinline__ bool slice_rows_contiguous(const SliceParams &P, int r0, int d0)
+{
+    if (SIDE == 0) return true;
+    return r0 < P.V && d0 < P.V;
+}
+
+template <int SIDE>
+__device__ __forceinline__ void slice_load(const SliceParams &P, int plane, int r0, int d0, double (*tile)[33],
+                                           int tid)
+{
+    const int D = P.V + P.O, R = 2 * P.V;
+    const bool rc = slice_rows_contiguous<SIDE>(P, r0, d0);
+#pragma unroll
+    for (int e = 0; e < 4; ++e) {
+        const int idx = tid + 256 * e;
+        const int rr = rc ? (idx & 31) : (idx >> 5), dd = rc ? (idx >> 5) : (idx & 31);
+        const int r = r0 + rr, d = d0 + dd;
+        tile[rr][dd] = (r < R && d < D) ? slice_src<SIDE>(P, plane, r, d) : 0.0;
+    }
+}
+
+template <int SIDE>
+__global__ void __launch_bounds__(256) oz_slice_kernel(const SliceParams P)
+{
+    __shared__ double tile[32][33];
+    const int tid = threadIdx.x, row = tid >> 3, part = tid & 7;
+    const int plane = blockIdx.y, r0 = blockIdx.x * 32;
+    const int D = P.V + P.O, R = 2 * P.V;
+
+    double mx = 0.0;
+    for (int d0 = 0; d0 < D; d0 += 32) {
+        slice_load<SIDE>(P, plane, r0, d0, tile, tid);
+        __syncthreads();
+#pragma unroll
+        for (int u = 0; u < 4; ++u) mx = fmax(mx, fabs(tile[row][part * 4 + u]));
+        __syncthreads();
+    }
+    mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, 1));
+    mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, 2));
+    mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, 4));
+    int e = 0;
+    if (mx > 0.0) {
+        frexp(mx, &e);  // mx = m 2^e, m in [1/2, 1)
+        e += 1;         // mx 2^-e in [1/4, 1/2)
+    }
+    const double inv = ldexp(1.0, -e);
+    const int r = r0 + row;
+    if (part == 0 && r < R) P.scale[(size_t)plane * R + r] = ldexp(1.0, e);
+
+    for (int d0 = 0; d0 < P.dp; d0 += 32) {
+        slice_load<SIDE>(P, plane, r0, d0, tile, tid);
+        __syncthreads();
+        unsigned w[8] = {0u, 0u, 0u, 0u, 0u, 0u, 0u, 0u};
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            double x = tile[row][part * 4 + u] * inv;  // exact: power-of-two scaling
+#pragma unroll
+            for (int p = 0; p < 8; ++p) {
+                if (p < P.S) {
+                    const double t = x * 128.0;
+                    const double dg = rint(t);  // |dg| <= 64 since |x| <= 1/2
+                    x = t - dg;                 // exact, |x| <= 1/2
+                    w[p] |= ((unsigned)(int)dg & 0xffu) << (8 * u);
+                }
+            }
+        }
+        if (r < R) {
+#pragma unroll
+            for (int p = 0; p < 8; ++p)
+                if (p < P.S)
+                    *reinterpret_cast<unsigned *>(P.out + (((size_t)plane * P.S + p) * R + r) * P.dp + d0 + part * 4) =
+                        w[p];
+        }
+        __syncthreads();
+    }
+}
+
+// ------------------------------------------------------------------------------------------------
+// batched tengy over the f of a batch: one CTA per (tile pair, triple); the CTA's four sums go to
+// slot 0 of the triple's item (the other slots are zero), so item_reduce sums them in fixed order
+// ------------------------------------------------------------------------------------------------
+constexpr int TNTHREAD = 512;
+constexpr size_t TSMEM_BYTES = (size_t)16 * TPTILE * sizeof(double);
+
+struct TengyParams {
+    trpdrv_dev_system sys;
+    long long pos0;
+    const double *fbuf;
+};
+
+__global__ void __launch_bounds__(TNTHREAD, 1) oz_tengy_kernel(const TengyParams P)
+{
+    extern __shared__ __align__(16) double park[];
+    __shared__ double red[4 * (TNTHREAD / 32)];
+    const trpdrv_dev_system &S = P.sys;
+    const int nvir = S.nvir, nb = S.nb, tid = threadIdx.x;
+    const long long pos = P.pos0 + blockIdx.y;
+    if (pos >= S.ntriples) return;
+    const long long tt = S.order ? (long long)S.order[pos] : pos;
+    if (tt < 0 || tt >= S.ntriples) return;
+    const int packed = S.triples[tt];
+    const int i = packed & 1023, j = (packed >> 10) & 1023, k = (packed >> 20) & 1023;
+
+    int B = 0, rem = blockIdx.x;
+    while (B < nb && rem >= nb - B) {
+        rem -= nb - B;
+        ++B;
+    }
+    const int Cb = B + rem;
+    const int b0 = B * TT, c0 = Cb * TT;
+    const bool diag = (B == Cb);
+    const size_t lnvv = (size_t)nvir * nvir;
+    const double *f = P.fbuf + (size_t)blockIdx.y * 8 * lnvv;
+
+    const int ntiles = diag ? 8 : 16;
+    for (int idx = tid; idx < ntiles * TT * TT; idx += TNTHREAD) {
+        const int tile = idx >> 10, q = (idx >> 5) & 31, r = idx & 31;
+        const int o = tile >> 3, xf = tile & 7;
+        const int row = (o ? c0 : b0) + r, col = (o ? b0 : c0) + q;
+        double v = 0.0;
+        if (row < nvir && col < nvir) v = f[(size_t)xf * lnvv + row + (size_t)col * nvir];
+        park[tile * TPTILE + r * TPP + q] = v;
+    }
+    __syncthreads();
+
+    TengyVecs v;
+    const int O = S.nocc;
+    v.eorb = S.eorb;
+    v.dintc1 = S.dintc + (size_t)i * nvir;
+    v.dintx1 = S.dintx + (size_t)i * nvir;
+    v.t1v1 = S.t1v + (size_t)i * nvir;
+    v.dintc2 = S.dintc + (size_t)k * nvir;
+    v.dintx2 = S.dintx + (size_t)k * nvir;
+    v.t1v2 = S.t1v + (size_t)k * nvir;
+    v.voff = S.ncor + O;
+    v.nvir = nvir;
+    // omp/ccsd_trpdrv_omp_cbody.c:126 (a is 1-based, i/j/k here 0-based)
+    v.eaijk = S.eorb[S.a - 1] - (S.eorb[S.ncor + i] + S.eorb[S.ncor + j] + S.eorb[S.ncor + k]);
+    TengySums su = {0.0, 0.0, 0.0, 0.0};
+    tengy_tile_pair(park, b0, c0, diag, v, tid, TNTHREAD, su);
+    const TengySums tot = block_sum4(su, red);
+    double *out = S.partial + ((size_t)tt * S.npairs + blockIdx.x) * TRPDRV_FUSED_SLOTS * 4;
+    if (tid == 0) {  // block_sum4's result is valid in thread 0
+        out[0] = tot.e4i;
+        out[1] = tot.e5i;
+        out[2] = tot.e4k;
+        out[3] = tot.e5k;
+    } else if (tid >= 4 && tid < TRPDRV_FUSED_SLOTS * 4) {
+        out[tid] = 0.0;
+    }
+}
+
+// ------------------------------------------------------------------------------------------------
+// host side
+// ------------------------------------------------------------------------------------------------
+static PFN_cuTensorMapEncodeTiled_v12000 encode_fn()
+{
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    if (!fn) {
+        void *p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+    }
+    return fn;
+}
+
+// 3-D map over int8 digits: dims {dp (contiguous), 2V, planes*S}, box {KC, rows, 1}, 64-byte swizzle
+static int make_map_i8(CUtensorMap *m, const signed char *base, unsigned long long dp, unsigned long long rows,
+                       unsigned long long planes, unsigned box_rows)
+{
+    PFN_cuTensorMapEncodeTiled_v12000 fn = encode_fn();
+    if (!fn) return 1;
+    const cuuint64_t dims[3] = {dp, rows, planes};
+    const cuuint64_t strides[2] = {dp, dp * rows};
+    const cuuint32_t box[3] = {(cuuint32_t)KC, box_rows, 1};
+    const cuuint32_t estr[3] = {1, 1, 1};
+    const CUresult r = fn(m, CU_TENSOR_MAP_DATA_TYPE_UINT8, 3, const_cast<signed char *>(base), dims, strides, box,
+                          estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_64B,
+                          CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    return r == CUDA_SUCCESS ? 0 : 2;
+}
+
+template <int S>
+static int set_attr()
+{
+    return (int)cudaFuncSetAttribute(oz_gemm_kernel<S>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)Cfg<S>::SMEM);
+}
+
+template <int S>
+static int launch_gemm(const GemmParams &P, dim3 grid, cudaStream_t st)
+{
+    oz_gemm_kernel<S><<<grid, NTHREAD, Cfg<S>::SMEM, st>>>(P);
+    return (int)cudaGetLastError();
+}
+
+}  // namespace oz
+}  // namespace trpdrv
+
+using namespace trpdrv;
+
+extern "C" int trpdrv_oz_slices_supported(int slices) { return slices >= TRPDRV_OZ_MIN_SLICES && slices <= TRPDRV_OZ_MAX_SLICES; }
+
+extern "C" int trpdrv_oz_dp(int nocc, int nvir) { return ((nvir + nocc) + 31) / 32 * 32; }
+
+extern "C" size_t trpdrv_oz_maps_bytes(void) { return 2 * sizeof(CUtensorMap); }
+
+extern "C" int trpdrv_oz_prepare(const trpdrv_oz_system *oz, void *maps_out)
+{
+    CUtensorMap *m = static_cast<CUtensorMap *>(maps_out);
+    const unsigned long long R = 2ull * oz->nvir, O = (unsigned long long)oz->nocc, S = (unsigned long long)oz->slices;
+    int e = oz::make_map_i8(&m[0], oz->sa, (unsigned long long)oz->dp, R, O * S, oz::BM);
+    if (e) return e;
+    return oz::make_map_i8(&m[1], oz->sb, (unsigned long long)oz->dp, R, O * O * S, oz::BN);
+}
+
+extern "C" int trpdrv_launch_oz_slices(const trpdrv_dev_system *h_sys, const trpdrv_oz_system *oz, void *stream)
+{
+    oz::SliceParams P;
+    P.t2 = h_sys->t2;
+    P.jvv = h_sys->jvv;
+    P.kvv = h_sys->kvv;
+    P.ntov = h_sys->ntov;
+    P.nxov = h_sys->nxov;
+    P.jov = h_sys->jov;
+    P.kov = h_sys->kov;
+    P.V = oz->nvir;
+    P.O = oz->nocc;
+    P.S = oz->slices;
+    P.dp = oz->dp;
+    const unsigned rb = (unsigned)((2 * oz->nvir + 31) / 32);
+    cudaStream_t st = (cudaStream_t)stream;
+    P.out = oz->sa;
+    P.scale = oz->ea;
+    oz::oz_slice_kernel<0><<<dim3(rb, (unsigned)oz->nocc), 256, 0, st>>>(P);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return (int)e;
+    P.out = oz->sb;
+    P.scale = oz->eb;
+    oz::oz_slice_kernel<1><<<dim3(rb, (unsigned)(oz->nocc * oz->nocc)), 256, 0, st>>>(P);
+    return (int)cudaGetLastError();
+}
+
+extern "C" int trpdrv_launch_oz_gemm(const trpdrv_dev_system *h_sys, const trpdrv_oz_system *oz, const void *maps,
+                                     int64_t pos0, int npos, double *fbuf, int *status, void *stream)
+{
+    if (npos <= 0) return 0;
+    oz::GemmParams P;
+    memcpy(&P.mapA, maps, sizeof(CUtensorMap));
+    memcpy(&P.mapB, static_cast<const char *>(maps) + sizeof(CUtensorMap), sizeof(CUtensorMap));
+    P.ea = oz->ea;
+    P.eb = oz->eb;
+    P.triples = h_sys->triples;
+    P.order = h_sys->order;
+    P.pos0 = pos0;
+    P.ntriples = h_sys->ntriples;
+    P.fbuf = fbuf;
+    P.V = oz->nvir;
+    P.O = oz->nocc;
+    P.nks = oz->dp / oz::KSTEP;
+    P.mtiles = (2 * oz->nvir + oz::BM - 1) / oz::BM;
+    P.status = status;
+    const int ntiles = (2 * oz->nvir + oz::BN - 1) / oz::BN;
+    const dim3 grid((unsigned)(P.mtiles * ntiles), (unsigned)(2 * npos));
+    cudaStream_t st = (cudaStream_t)stream;
+    switch (oz->slices) {
+    case 4: return oz::launch_gemm<4>(P, grid, st);
+    case 5: return oz::launch_gemm<5>(P, grid, st);
+    case 6: return oz::launch_gemm<6>(P, grid, st);
+    case 7: return oz::launch_gemm<7>(P, grid, st);
+    case 8: return oz::launch_gemm<8>(P, grid, st);
+    default: return (int)cudaErrorInvalidValue;
+    }
+}
+
+extern "C" int trpdrv_launch_oz_tengy(const trpdrv_dev_system *h_sys, int64_t pos0, int npos, const double *fbuf,
+                                      void *stream)
+{
+    if (npos <= 0) return 0;
+    oz::TengyParams P;
+    P.sys = *h_sys;
+    P.pos0 = pos0;
+    P.fbuf = fbuf;
+    oz::oz_tengy_kernel<<<dim3((unsigned)h_sys->npairs, (unsigned)npos), oz::TNTHREAD, oz::TSMEM_BYTES,
+                          (cudaStream_t)stream>>>(P);
+    return (int)cudaGetLastError();
+}
+
+extern "C" int trpdrv_oz_init(void)
+{
+    int e;
+    if ((e = oz::set_attr<4>()) != 0) return e;
+    if ((e = oz::set_attr<5>()) != 0) return e;
+    if ((e = oz::set_attr<6>()) != 0) return e;
+    if ((e = oz::set_attr<7>()) != 0) return e;
+    if ((e = oz::set_attr<8>()) != 0) return e;
+    return (int)cudaFuncSetAttribute(oz::oz_tengy_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)oz::TSMEM_BYTES);
+}

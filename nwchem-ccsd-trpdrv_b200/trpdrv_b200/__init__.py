@@ -20,6 +20,7 @@ INCLUDE_DIR = os.path.join(os.path.dirname(os.path.dirname(_HERE)), "include")
 
 MODE_PLAIN = 0
 MODE_FUSED = 1
+MODE_EMULATED = 2
 DIST_UNIFORM = 0
 DIST_LOGUNIFORM = 1
 
@@ -55,7 +56,8 @@ class SystemStruct(C.Structure):
 class OptionsStruct(C.Structure):
     _fields_ = [("mode", C.c_int), ("nkpass", C.c_int), ("rank", C.c_int), ("world", C.c_int),
                 ("device", C.c_int), ("tile", C.c_int), ("ctas_per_sm", C.c_int),
-                ("use_graph", C.c_int), ("mma_k", C.c_int), ("staging", C.c_int), ("reserved", C.c_int * 6)]
+                ("use_graph", C.c_int), ("mma_k", C.c_int), ("staging", C.c_int), ("slices", C.c_int),
+                ("batch", C.c_int), ("reserved", C.c_int * 4)]
 
 STAGING_AUTO, STAGING_CPASYNC, STAGING_TMA = 0, 1, 2
 
@@ -306,13 +308,17 @@ def tengy(f8: np.ndarray, vecs: Sequence[np.ndarray], eorb: np.ndarray, eaijk: f
 # plans
 # --------------------------------------------------------------------------------------------
 def options(mode=MODE_FUSED, nkpass=1, rank=0, world=1, device=-1, ctas_per_sm=0, use_graph=1,
-            mma_k=0, staging=STAGING_AUTO) -> OptionsStruct:
+            mma_k=0, staging=STAGING_AUTO, slices=0, batch=0) -> OptionsStruct:
     o = OptionsStruct()
     lib.trpdrv_options_default(C.byref(o))
     o.mode, o.nkpass, o.rank, o.world, o.device = mode, nkpass, rank, world, device
     o.ctas_per_sm, o.use_graph, o.staging = ctas_per_sm, use_graph, staging
     if mma_k:
         o.mma_k = mma_k
+    if slices:
+        o.slices = slices
+    if batch:
+        o.batch = batch
     return o
 
 

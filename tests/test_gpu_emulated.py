@@ -1,0 +1,89 @@
+"""GPU parity of the emulated-FP64 form (TRPDRV_MODE_EMULATED: Ozaki int8 digit slices on the
+tcgen05 tensor cores, exact int32 sums, FP64 recombination and FP64 energies) against the reference's
+golden vectors and the native FP64 paths.
+
+Bars: with 7 or 8 slices the emulated form meets the native bars (emp4/emp5 totals within 1e-11
+relative, per-triple records within 1e-11 normwise per column); fewer slices give errors that fall
+by about 2^-7 per slice, which the sweep checks and reports.
+"""
+import numpy as np
+import pytest
+
+from conftest import (RECORD_RTOL, TOTAL_RTOL, assert_records_close, assert_total_close, golden_cases, load_golden,
+                      system_from_golden)
+
+pytestmark = pytest.mark.gpu
+
+
+def _run(T, systems, mode=None, **opt):
+    with T.Plan(systems, mode=T.MODE_EMULATED if mode is None else mode, **opt) as p:
+        p.upload()
+        p.execute()
+        e4, e5 = p.energies()
+        recs = [p.triple_energies(q) for q in range(len(systems))]
+        launches = p.last_launches()
+    return e4, e5, recs, launches
+
+
+@pytest.mark.parametrize("slices", [7, 8])
+@pytest.mark.parametrize("name", golden_cases())
+def test_emulated_matches_reference_golden(T, name, slices):
+    g = load_golden(name)
+    s = system_from_golden(g)
+    e4, e5, recs, launches = _run(T, [s], nkpass=g["nkpass"], slices=slices)
+    assert launches > 0
+    assert_records_close(recs[0], g["records"])
+    assert_total_close(e4[0], g["emp4"], what="emp4")
+    assert_total_close(e5[0], g["emp5"], what="emp5")
+
+
+@pytest.mark.parametrize("name", ["g_o10_v60", "g_o4_v30_log"])
+def test_emulated_error_falls_with_slices(T, name):
+    g = load_golden(name)
+    s = system_from_golden(g)
+    ref = np.asarray(g["records"], dtype=np.float64)
+    errs = []
+    for sl in range(4, 9):
+        _, _, recs, _ = _run(T, [s], nkpass=g["nkpass"], slices=sl)
+        errs.append(float(np.max(np.abs(recs[0] - ref)) / np.max(np.abs(ref))))
+    print(name, ["%.2e" % e for e in errs])
+    floor = 1e-14
+    for a, b in zip(errs, errs[1:]):
+        assert b <= max(a / 16.0, floor), errs
+    assert errs[0] < 1e-6  # four digits: 28 bits of every operand
+
+
+@pytest.mark.parametrize("nocc,nvir,seed,ncor", [(8, 100, 41, 0), (5, 129, 42, 1), (6, 200, 43, 0), (3, 8, 44, 0)])
+def test_emulated_matches_fused_on_other_shapes(T, nocc, nvir, seed, ncor):
+    s = T.synth_system(nocc, nvir, seed=seed, ncor=ncor)
+    e4f, e5f, recf, _ = _run(T, [s], mode=T.MODE_FUSED)
+    e4, e5, rec, _ = _run(T, [s], slices=8)
+    assert_records_close(rec[0], recf[0])
+    assert_total_close(e4[0], e4f[0], what="emp4")
+    assert_total_close(e5[0], e5f[0], what="emp5")
+
+
+def test_emulated_batches_and_shards_recombine(T):
+    s = T.synth_system(7, 64, seed=45)
+    e4, e5, rec, _ = _run(T, [s], slices=7, batch=5)
+    e4b, e5b, recb, _ = _run(T, [s], slices=7, batch=64)
+    assert np.array_equal(rec[0], recb[0])  # the batch size changes no arithmetic
+    parts = [_run(T, [s], slices=7, rank=r, world=3)[2][0] for r in range(3)]
+    assert np.array_equal(np.concatenate(parts), rec[0])
+
+
+def test_emulated_uneven_systems_equal_single_runs(T):
+    systems = [T.synth_system(4, 40, seed=46), T.synth_system(6, 90, seed=47, ncor=2), T.synth_system(3, 17, seed=48)]
+    e4b, e5b, recb, _ = _run(T, systems, slices=7)
+    for q, s in enumerate(systems):
+        e4, e5, rec, _ = _run(T, [s], slices=7)
+        assert np.array_equal(recb[q], rec[0])
+        assert e4b[q] == e4[0] and e5b[q] == e5[0]
+
+
+def test_emulated_rejects_bad_slice_counts(T):
+    s = T.synth_system(2, 8, seed=1)
+    for bad in (3, 9):
+        with pytest.raises(T.TrpdrvError) as ei:
+            T.Plan([s], mode=T.MODE_EMULATED, slices=bad)
+        assert ei.value.status == 1

@@ -588,7 +588,7 @@ static int enqueue_emulated(trpdrv_plan *p, cudaStream_t st, int capturing)
         ++launches;
         for (int64_t pos = 0; pos < d->ntriples; pos += p->opt.batch) {
             const int n = (int)(d->ntriples - pos < p->opt.batch ? d->ntriples - pos : p->opt.batch);
-            LAUNCH_TRY(trpdrv_launch_oz_gemm(d, &b->oz, b->oz_maps, pos, n, p->d_fbuf, p->d_status, st));
+            LAUNCH_TRY(trpdrv_launch_oz_gemm(d, &b->oz, b->oz_maps, pos, n, p->d_fbuf, p->d_status, p->nsm, st));
             LAUNCH_TRY(trpdrv_launch_oz_tengy(d, pos, n, p->d_fbuf, st));
             launches += 2;
         }

@@ -84,7 +84,7 @@ size_t trpdrv_oz_maps_bytes(void);
 int trpdrv_oz_prepare(const trpdrv_oz_system *oz, void *maps_out);
 int trpdrv_launch_oz_slices(const trpdrv_dev_system *h_sys, const trpdrv_oz_system *oz, void *stream);
 int trpdrv_launch_oz_gemm(const trpdrv_dev_system *h_sys, const trpdrv_oz_system *oz, const void *maps,
-                          int64_t pos0, int npos, double *fbuf, int *status, void *stream);
+                          int64_t pos0, int npos, double *fbuf, int *status, int grid, void *stream);
 int trpdrv_launch_oz_tengy(const trpdrv_dev_system *h_sys, int64_t pos0, int npos, const double *fbuf,
                            void *stream);
 int trpdrv_oz_init(void);

@@ -23,12 +23,13 @@
 // product [A1; A2] [B1 | B3] holds the four f of the group in its quadrants:
 //   f1n = A1 B1, f2n = A2 B1, f3n = A1 B3, f4n = A2 B3 (and f1t..f4t likewise).
 //
-// Contraction kernel: one CTA per 128 x 64 output tile of one (triple, group).  Warp 0 issues TMA
-// loads (64-byte swizzle) of all S digit slices of A and B for 64 contraction indices per stage;
-// warp 1 allocates tensor memory and one of its threads issues every MMA (M=128, N=64, K=32) into S
-// level accumulators (S*64 columns); warps 2-5 wait for the last MMA, read the accumulators with
-// tcgen05.ld and recombine them in FP64.  Every wait is bounded (globaltimer) and reports through
-// *status; tensor memory is released on every path.
+// Contraction kernel: persistent, one CTA per SM walking 128 x 64 output tiles of the batch's
+// (triple, group) products.  Warp 0 issues TMA loads (64-byte swizzle) of all S digit slices of A and
+// B for 64 contraction indices per stage and runs ahead across tiles; warp 1 allocates tensor memory
+// and one of its threads issues every MMA (M=128, N=64, K=32) into S level accumulators (S*64
+// columns); warps 2-5 wait for a tile's last MMA, drain the accumulators with tcgen05.ld, release
+// them to the next tile and then scale and store in FP64 while its MMAs run.  Every wait is bounded
+// (globaltimer) and reports through *status; tensor memory is released on every path.
 
 #include <cuda.h>
 #include <cudaTypedefs.h>
@@ -72,7 +73,7 @@ struct GemmParams {
     const int32_t *triples, *order;
     long long pos0, ntriples;
     double *fbuf;            // [batch][8][V][V]
-    int V, O, nks, mtiles;
+    int V, O, nks, mtiles, ntiles, tiles;  // tiles = 2 * npos * mtiles * ntiles
     int *status;
 };
 
@@ -177,8 +178,8 @@ __device__ __forceinline__ void mma_commit(unsigned long long *bar)
                  : "memory");
 }
 
-// 32 lanes x 16 columns of 32 bits; the wait names the registers so that no use moves above it
-__device__ __forceinline__ void tmem_ld16(unsigned taddr, unsigned (&v)[16])
+// 32 lanes x 16 columns of 32 bits into v (valid only after tmem_wait_ld and reg_fence16)
+__device__ __forceinline__ void tmem_ld16_nowait(unsigned taddr, unsigned (&v)[16])
 {
     asm volatile(
         "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
@@ -186,39 +187,73 @@ __device__ __forceinline__ void tmem_ld16(unsigned taddr, unsigned (&v)[16])
         : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
           "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
         : "r"(taddr));
-    asm volatile("tcgen05.wait::ld.sync.aligned;"
+}
+
+__device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
+
+// Orders every use of v after the preceding tcgen05.wait::ld (volatile asm keeps its place in
+// program order, and the registers pass through it).
+__device__ __forceinline__ void reg_fence16(unsigned (&v)[16])
+{
+    asm volatile(""
                  : "+r"(v[0]), "+r"(v[1]), "+r"(v[2]), "+r"(v[3]), "+r"(v[4]), "+r"(v[5]), "+r"(v[6]), "+r"(v[7]),
                    "+r"(v[8]), "+r"(v[9]), "+r"(v[10]), "+r"(v[11]), "+r"(v[12]), "+r"(v[13]), "+r"(v[14]),
-                   "+r"(v[15])
-                 :
-                 : "memory");
+                   "+r"(v[15]));
+}
+
+__device__ __forceinline__ void mbar_arrive(unsigned long long *b)
+{
+    asm volatile("mbarrier.arrive.shared.b64 _, [%0];" ::"r"(saddr(b)) : "memory");
+}
+
+// weight of level L (0-based, slices p + q = L + 2 in 1-based digits): 2^(-7 (L + 2)), exact
+__device__ __forceinline__ double level_weight(int L)
+{
+    double w = 1.0 / 16384.0;
+    for (int l = 0; l < L; ++l) w *= 1.0 / 128.0;
+    return w;
 }
 
 // ------------------------------------------------------------------------------------------------
-// contraction kernel
+// contraction kernel (persistent: CTA b takes tiles b, b + grid, ...)
 // ------------------------------------------------------------------------------------------------
+struct Tile {
+    int ok, y, grp, planeA, planeB, m0, n0;
+};
+
+__device__ __forceinline__ Tile decode_tile(const GemmParams &P, int t)
+{
+    Tile d;
+    const int per = P.mtiles * P.ntiles;
+    d.y = t / per;
+    const int rem = t - d.y * per;
+    d.m0 = (rem % P.mtiles) * BM;
+    d.n0 = (rem / P.mtiles) * BN;
+    d.grp = d.y & 1;
+    const long long pos = P.pos0 + (d.y >> 1);
+    const long long tt = (pos < P.ntriples) ? (P.order ? (long long)P.order[pos] : pos) : -1;
+    const int packed = (tt >= 0 && tt < P.ntriples) ? P.triples[tt] : -1;
+    const int i = packed & 1023, j = (packed >> 10) & 1023, k = (packed >> 20) & 1023;
+    d.ok = packed >= 0 && i < P.O && j < P.O && k < P.O;
+    d.planeA = d.grp ? k : i;
+    d.planeB = j * P.O + (d.grp ? i : k);
+    return d;
+}
+
+// level accumulators are drained in groups of up to 4: X = sum_l C_l 128^(last - l) is exact in
+// int64 and below 2^53 (|C_l| < 2^24), so one exact conversion and one FMA cover the group
+constexpr int LGROUP = 4;
+
 template <int S>
 __global__ void __launch_bounds__(NTHREAD, 1) oz_gemm_kernel(const __grid_constant__ GemmParams P)
 {
     using C = Cfg<S>;
     extern __shared__ char smem_raw[];
-    __shared__ __align__(8) unsigned long long full[C::STAGES], empty[C::STAGES], accf[1];
+    __shared__ __align__(8) unsigned long long full[C::STAGES], empty[C::STAGES], tfull[1], tempty[1], done[1];
     __shared__ unsigned tmem_sh;
     char *stages = reinterpret_cast<char *>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~(uintptr_t)1023);
 
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    const int y = blockIdx.y, grp = y & 1;
-    const long long pos = P.pos0 + (y >> 1);
-    const long long tt = (pos < P.ntriples) ? (P.order ? (long long)P.order[pos] : pos) : -1;
-    const int packed = (tt >= 0 && tt < P.ntriples) ? P.triples[tt] : -1;
-    const int i = packed & 1023, j = (packed >> 10) & 1023, k = (packed >> 20) & 1023;
-    if (packed < 0 || i >= P.O || j >= P.O || k >= P.O) {  // uniform over the CTA: nothing allocated yet
-        if (tid == 0) atomicOr(P.status, 1);
-        return;
-    }
-    const int planeA = grp ? k : i, planeB = j * P.O + (grp ? i : k);
-    const int mt = blockIdx.x % P.mtiles, nt = blockIdx.x / P.mtiles;
-    const int m0 = mt * BM, n0 = nt * BN;
     const int nchunks = (P.nks * KSTEP + KC - 1) / KC;
 
     if (tid == 0) {
@@ -226,7 +261,9 @@ __global__ void __launch_bounds__(NTHREAD, 1) oz_gemm_kernel(const __grid_consta
             mbar_init(&full[s], 1);
             mbar_init(&empty[s], 1);
         }
-        mbar_init(accf, 1);
+        mbar_init(tfull, 1);
+        mbar_init(tempty, 4);  // one arrival per recombination warp
+        mbar_init(done, 1);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     if (warp == 1) {
@@ -239,22 +276,33 @@ __global__ void __launch_bounds__(NTHREAD, 1) oz_gemm_kernel(const __grid_consta
     const unsigned tmem = tmem_sh;
 
     if (warp == 0) {
-        if (lane == 0) {  // TMA producer
+        if (lane == 0) {  // TMA producer: runs ahead across tiles, bounded by the stage ring
             int stage = 0;
             unsigned phase = 0;
-            for (int kc = 0; kc < nchunks; ++kc) {
-                if (!mbar_wait(&empty[stage], phase ^ 1, P.status)) break;
-                mbar_arrive_expect_tx(&full[stage], C::STAGE);
-                char *sA = stages + (size_t)stage * C::STAGE, *sB = sA + S * SLICE_A;
+            bool alive = true;
+            for (int t = blockIdx.x; alive && t < P.tiles; t += gridDim.x) {
+                const Tile d = decode_tile(P, t);
+                if (!d.ok) {
+                    atomicOr(P.status, 1);
+                    continue;
+                }
+                for (int kc = 0; kc < nchunks; ++kc) {
+                    if (!mbar_wait(&empty[stage], phase ^ 1, P.status)) {
+                        alive = false;
+                        break;
+                    }
+                    mbar_arrive_expect_tx(&full[stage], C::STAGE);
+                    char *sA = stages + (size_t)stage * C::STAGE, *sB = sA + S * SLICE_A;
 #pragma unroll
-                for (int p = 0; p < S; ++p)
-                    tma_load_3d(sA + p * SLICE_A, &P.mapA, &full[stage], kc * KC, m0, planeA * S + p);
+                    for (int p = 0; p < S; ++p)
+                        tma_load_3d(sA + p * SLICE_A, &P.mapA, &full[stage], kc * KC, d.m0, d.planeA * S + p);
 #pragma unroll
-                for (int q = 0; q < S; ++q)
-                    tma_load_3d(sB + q * SLICE_B, &P.mapB, &full[stage], kc * KC, n0, planeB * S + q);
-                if (++stage == C::STAGES) {
-                    stage = 0;
-                    phase ^= 1;
+                    for (int q = 0; q < S; ++q)
+                        tma_load_3d(sB + q * SLICE_B, &P.mapB, &full[stage], kc * KC, d.n0, d.planeB * S + q);
+                    if (++stage == C::STAGES) {
+                        stage = 0;
+                        phase ^= 1;
+                    }
                 }
             }
         }
@@ -263,64 +311,103 @@ __global__ void __launch_bounds__(NTHREAD, 1) oz_gemm_kernel(const __grid_consta
         if (lane == 0) {  // MMA issuer: level L = p + q (0-based) accumulates at columns L*BN..
             int stage = 0;
             unsigned phase = 0;
-            for (int kc = 0; kc < nchunks; ++kc) {
-                if (!mbar_wait(&full[stage], phase, P.status)) break;
+            bool alive = true;
+            int it = 0;
+            for (int t = blockIdx.x; alive && t < P.tiles; t += gridDim.x, ++it) {
+                const Tile d = decode_tile(P, t);
+                // the accumulators are free once the previous tile has been drained
+                if (!mbar_wait(tempty, (it & 1) ^ 1, P.status)) break;
                 tc_fence_after();
-                const char *sA = stages + (size_t)stage * C::STAGE, *sB = sA + S * SLICE_A;
-                const unsigned long long dA = sdesc_sw64(sA), dB = sdesc_sw64(sB);
+                if (d.ok) {
+                    for (int kc = 0; kc < nchunks; ++kc) {
+                        if (!mbar_wait(&full[stage], phase, P.status)) {
+                            alive = false;
+                            break;
+                        }
+                        tc_fence_after();
+                        const char *sA = stages + (size_t)stage * C::STAGE, *sB = sA + S * SLICE_A;
+                        const unsigned long long dA = sdesc_sw64(sA), dB = sdesc_sw64(sB);
 #pragma unroll
-                for (int ks = 0; ks < KC / KSTEP; ++ks) {
-                    const int kg = kc * (KC / KSTEP) + ks;
-                    if (kg < P.nks) {
+                        for (int ks = 0; ks < KC / KSTEP; ++ks) {
+                            const int kg = kc * (KC / KSTEP) + ks;
+                            if (kg < P.nks) {
 #pragma unroll
-                        for (int p = 0; p < S; ++p)
+                                for (int p = 0; p < S; ++p)
 #pragma unroll
-                            for (int q = 0; p + q < S; ++q)
-                                mma_i8(tmem + (unsigned)((p + q) * BN),
-                                       dA + (unsigned long long)(p * (SLICE_A >> 4) + ks * (KSTEP >> 4)),
-                                       dB + (unsigned long long)(q * (SLICE_B >> 4) + ks * (KSTEP >> 4)),
-                                       (kg > 0 || p > 0) ? 1 : 0);
+                                    for (int q = 0; p + q < S; ++q)
+                                        mma_i8(tmem + (unsigned)((p + q) * BN),
+                                               dA + (unsigned long long)(p * (SLICE_A >> 4) + ks * (KSTEP >> 4)),
+                                               dB + (unsigned long long)(q * (SLICE_B >> 4) + ks * (KSTEP >> 4)),
+                                               (kg > 0 || p > 0) ? 1 : 0);
+                            }
+                        }
+                        mma_commit(&empty[stage]);  // the stage is free once these MMAs have read it
+                        if (++stage == C::STAGES) {
+                            stage = 0;
+                            phase ^= 1;
+                        }
                     }
                 }
-                mma_commit(&empty[stage]);  // the stage is free once these MMAs have read it
-                if (++stage == C::STAGES) {
-                    stage = 0;
-                    phase ^= 1;
-                }
+                mma_commit(tfull);  // this tile's sums are complete (or the tile was skipped)
             }
-            mma_commit(accf);  // tracks every MMA issued, also after an early stop
+            mma_commit(done);  // every MMA issued by this thread has completed when `done` flips
+            mbar_wait(done, 0, P.status);
         }
         __syncwarp();
     } else {  // recombination: this warp reads TMEM lanes 32*(warp%4)..
         const int qd = warp & 3;
-        const bool ok = mbar_wait(accf, 0, P.status);
-        tc_fence_after();
-        if (ok) {
+        const int V = P.V;
+        const size_t vv = (size_t)V * V;
+        int it = 0;
+        for (int t = blockIdx.x; t < P.tiles; t += gridDim.x, ++it) {
+            const Tile d = decode_tile(P, t);
+            if (!mbar_wait(tfull, it & 1, P.status)) break;
+            tc_fence_after();
             double acc[BN];
 #pragma unroll
             for (int c = 0; c < BN; ++c) acc[c] = 0.0;
-            double w = 1.0 / 16384.0;  // level 0 (p = q = 1) carries 2^-14; each level after it 2^-7 less
-#pragma unroll
-            for (int L = 0; L < S; ++L) {
+            if (d.ok) {
 #pragma unroll
                 for (int cb = 0; cb < BN / 16; ++cb) {
-                    unsigned v[16];
-                    tmem_ld16(tmem + ((unsigned)(qd * 32) << 16) + (unsigned)(L * BN + cb * 16), v);
 #pragma unroll
-                    for (int u = 0; u < 16; ++u) acc[cb * 16 + u] = fma((double)(int)v[u], w, acc[cb * 16 + u]);
+                    for (int g0 = 0; g0 < S; g0 += LGROUP) {
+                        const int g1 = (g0 + LGROUP < S) ? g0 + LGROUP : S;  // levels g0..g1-1
+                        unsigned v[LGROUP][16];
+#pragma unroll
+                        for (int l = 0; l < LGROUP; ++l)
+                            if (g0 + l < g1)
+                                tmem_ld16_nowait(tmem + ((unsigned)(qd * 32) << 16) + (unsigned)((g0 + l) * BN + cb * 16),
+                                                 v[l]);
+                        tmem_wait_ld();
+#pragma unroll
+                        for (int l = 0; l < LGROUP; ++l)
+                            if (g0 + l < g1) reg_fence16(v[l]);
+                        // weight of the group's last level: 2^(-7 (g1 - 1 + 2))
+                        const double w = level_weight(g1 - 1);
+#pragma unroll
+                        for (int u = 0; u < 16; ++u) {
+                            long long x = 0;
+#pragma unroll
+                            for (int l = 0; l < LGROUP; ++l)
+                                if (g0 + l < g1) x = x * 128 + (long long)(int)v[l][u];
+                            acc[cb * 16 + u] = fma((double)x, w, acc[cb * 16 + u]);
+                        }
+                    }
                 }
-                w *= 1.0 / 128.0;
             }
-            const int V = P.V, r = m0 + qd * 32 + lane;
-            if (r < 2 * V) {
-                const size_t vv = (size_t)V * V;
-                const double sa = P.ea[(size_t)planeA * 2 * V + r];
+            // the accumulators may be overwritten by the next tile from here on
+            tc_fence_before();
+            __syncwarp();
+            if (lane == 0) mbar_arrive(tempty);
+            const int r = d.m0 + qd * 32 + lane;
+            if (d.ok && r < 2 * V) {
+                const double sa = P.ea[(size_t)d.planeA * 2 * V + r];
                 const int rh = r >= V ? 1 : 0, b = r - rh * V;
-                double *fj = P.fbuf + (size_t)(y >> 1) * 8 * vv + (size_t)grp * 4 * vv;
-                const double *eb = P.eb + (size_t)planeB * 2 * V;
+                double *fj = P.fbuf + (size_t)(d.y >> 1) * 8 * vv + (size_t)d.grp * 4 * vv;
+                const double *eb = P.eb + (size_t)d.planeB * 2 * V;
 #pragma unroll
                 for (int c = 0; c < BN; ++c) {
-                    const int col = n0 + c;
+                    const int col = d.n0 + c;
                     if (col < 2 * V) {
                         const int ch = col >= V ? 1 : 0, cc = col - ch * V;
                         fj[(size_t)(rh + 2 * ch) * vv + b + (size_t)cc * V] = acc[c] * sa * __ldg(eb + col);
@@ -610,7 +697,7 @@ extern "C" int trpdrv_launch_oz_slices(const trpdrv_dev_system *h_sys, const trp
 }
 
 extern "C" int trpdrv_launch_oz_gemm(const trpdrv_dev_system *h_sys, const trpdrv_oz_system *oz, const void *maps,
-                                     int64_t pos0, int npos, double *fbuf, int *status, void *stream)
+                                     int64_t pos0, int npos, double *fbuf, int *status, int grid, void *stream)
 {
     if (npos <= 0) return 0;
     oz::GemmParams P;
@@ -627,16 +714,18 @@ extern "C" int trpdrv_launch_oz_gemm(const trpdrv_dev_system *h_sys, const trpdr
     P.O = oz->nocc;
     P.nks = oz->dp / oz::KSTEP;
     P.mtiles = (2 * oz->nvir + oz::BM - 1) / oz::BM;
+    P.ntiles = (2 * oz->nvir + oz::BN - 1) / oz::BN;
+    P.tiles = 2 * npos * P.mtiles * P.ntiles;
     P.status = status;
-    const int ntiles = (2 * oz->nvir + oz::BN - 1) / oz::BN;
-    const dim3 grid((unsigned)(P.mtiles * ntiles), (unsigned)(2 * npos));
+    if (grid < 1) grid = 1;
+    if (grid > P.tiles) grid = P.tiles;
     cudaStream_t st = (cudaStream_t)stream;
     switch (oz->slices) {
-    case 4: return oz::launch_gemm<4>(P, grid, st);
-    case 5: return oz::launch_gemm<5>(P, grid, st);
-    case 6: return oz::launch_gemm<6>(P, grid, st);
-    case 7: return oz::launch_gemm<7>(P, grid, st);
-    case 8: return oz::launch_gemm<8>(P, grid, st);
+    case 4: return oz::launch_gemm<4>(P, dim3((unsigned)grid), st);
+    case 5: return oz::launch_gemm<5>(P, dim3((unsigned)grid), st);
+    case 6: return oz::launch_gemm<6>(P, dim3((unsigned)grid), st);
+    case 7: return oz::launch_gemm<7>(P, dim3((unsigned)grid), st);
+    case 8: return oz::launch_gemm<8>(P, dim3((unsigned)grid), st);
     default: return (int)cudaErrorInvalidValue;
     }
 }

@@ -320,9 +320,12 @@ static int plan_build(trpdrv_plan *p, const trpdrv_system *shape)
                                 cudaMemcpyHostToDevice));
             CUDA_TRY(cudaMalloc((void **)&b->rec, sizeof(double) * 4 * (size_t)b->ntriples));
             CUDA_TRY(cudaMemset(b->rec, 0, sizeof(double) * 4 * (size_t)b->ntriples));
-            if (o->mode != TRPDRV_MODE_PLAIN)
-                CUDA_TRY(cudaMalloc((void **)&b->partial, sizeof(double) * 4 * TRPDRV_FUSED_SLOTS *
-                                                       (size_t)b->ntriples * b->npairs));
+            if (o->mode != TRPDRV_MODE_PLAIN) {
+                const size_t pb = sizeof(double) * 4 * TRPDRV_FUSED_SLOTS * (size_t)b->ntriples * b->npairs;
+                CUDA_TRY(cudaMalloc((void **)&b->partial, pb));
+                /* the emulated form writes only some slots of each item; the rest stay zero */
+                CUDA_TRY(cudaMemset(b->partial, 0, pb));
+            }
         }
         const size_t ov = (size_t)nocc * nocc * nvir;
         if (o->mode == TRPDRV_MODE_EMULATED) {

@@ -68,9 +68,10 @@ int trpdrv_fused_tma_init(void);
  * eb [nocc*nocc][2 nvir].  trpdrv_oz_prepare encodes the two tensor maps into a host blob of
  * trpdrv_oz_maps_bytes() bytes (64-byte aligned).  A batch is npos consecutive positions of the
  * system's processing order starting at pos0: the contraction kernel writes their f into
- * fbuf [npos][8][nvir][nvir] and the tengy kernel writes each triple's energies into slot 0 of
- * its items in `partial` (slots 1..7 zero), for trpdrv_launch_item_reduce.  *status as the fused
- * kernels (bit 0 malformed entry, bit 1 a wait ran out). */
+ * fbuf [npos][8][nvir][nvir] and the tengy kernel writes the sums of each 16-wide tile pair into
+ * one slot of the triple's items in `partial` (the other slots must be zero), for
+ * trpdrv_launch_item_reduce.  *status as the fused kernels (bit 0 malformed entry, bit 1 a wait
+ * ran out).  The contraction kernel is persistent: grid = CTAs (one per SM). */
 #define TRPDRV_OZ_MIN_SLICES 4
 #define TRPDRV_OZ_MAX_SLICES 8
 typedef struct trpdrv_oz_system {

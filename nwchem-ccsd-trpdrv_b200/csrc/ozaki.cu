@@ -27,7 +27,7 @@
 // (triple, group) products.  Warp 0 issues TMA loads (64-byte swizzle) of all S digit slices of A and
 // B for 64 contraction indices per stage and runs ahead across tiles; warp 1 allocates tensor memory
 // and one of its threads issues every MMA (M=128, N=64, K=32) into S level accumulators (S*64
-// columns); warps 2-5 wait for a tile's last MMA, drain the accumulators with tcgen05.ld, release
+// columns); warps 2-9 wait for a tile's last MMA, drain the accumulators with tcgen05.ld, release
 // them to the next tile and then scale and store in FP64 while its MMAs run.  Every wait is bounded
 // (globaltimer) and reports through *status; tensor memory is released on every path.
 
@@ -45,7 +45,8 @@ constexpr int BM = 128;         // output rows per tile (TMEM lanes)
 constexpr int BN = 64;          // output columns per tile (TMEM columns per level)
 constexpr int KC = 64;          // contraction bytes (= int8 indices) per stage
 constexpr int KSTEP = 32;       // contraction indices per MMA
-constexpr int NTHREAD = 192;    // warp 0 TMA, warp 1 MMA + TMEM, warps 2-5 recombination
+constexpr int NREC = 8;         // recombination warps: two per TMEM lane quadrant, 32 columns each
+constexpr int NTHREAD = 32 * (2 + NREC);  // warp 0 TMA, warp 1 MMA + TMEM, warps 2.. recombination
 constexpr unsigned SLICE_A = BM * KC;
 constexpr unsigned SLICE_B = BN * KC;
 constexpr int SMEM_AVAIL = 227 * 1024 - 2048;
@@ -262,7 +263,7 @@ __global__ void __launch_bounds__(NTHREAD, 1) oz_gemm_kernel(const __grid_consta
             mbar_init(&empty[s], 1);
         }
         mbar_init(tfull, 1);
-        mbar_init(tempty, 4);  // one arrival per recombination warp
+        mbar_init(tempty, NREC);  // one arrival per recombination warp
         mbar_init(done, 1);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
@@ -354,8 +355,9 @@ __global__ void __launch_bounds__(NTHREAD, 1) oz_gemm_kernel(const __grid_consta
             mbar_wait(done, 0, P.status);
         }
         __syncwarp();
-    } else {  // recombination: this warp reads TMEM lanes 32*(warp%4)..
-        const int qd = warp & 3;
+    } else {  // recombination: this warp reads TMEM lanes 32*(warp%4).., columns 32*half..
+        const int qd = warp & 3, half = (warp - 2) >> 2;
+        constexpr int WC = BN / 2;  // columns per recombination warp
         const int V = P.V;
         const size_t vv = (size_t)V * V;
         int it = 0;
@@ -363,21 +365,20 @@ __global__ void __launch_bounds__(NTHREAD, 1) oz_gemm_kernel(const __grid_consta
             const Tile d = decode_tile(P, t);
             if (!mbar_wait(tfull, it & 1, P.status)) break;
             tc_fence_after();
-            double acc[BN];
+            double acc[WC];
 #pragma unroll
-            for (int c = 0; c < BN; ++c) acc[c] = 0.0;
+            for (int c = 0; c < WC; ++c) acc[c] = 0.0;
             if (d.ok) {
+                const unsigned base = tmem + ((unsigned)(qd * 32) << 16) + (unsigned)(half * WC);
 #pragma unroll
-                for (int cb = 0; cb < BN / 16; ++cb) {
+                for (int cb = 0; cb < WC / 16; ++cb) {
 #pragma unroll
                     for (int g0 = 0; g0 < S; g0 += LGROUP) {
                         const int g1 = (g0 + LGROUP < S) ? g0 + LGROUP : S;  // levels g0..g1-1
                         unsigned v[LGROUP][16];
 #pragma unroll
                         for (int l = 0; l < LGROUP; ++l)
-                            if (g0 + l < g1)
-                                tmem_ld16_nowait(tmem + ((unsigned)(qd * 32) << 16) + (unsigned)((g0 + l) * BN + cb * 16),
-                                                 v[l]);
+                            if (g0 + l < g1) tmem_ld16_nowait(base + (unsigned)((g0 + l) * BN + cb * 16), v[l]);
                         tmem_wait_ld();
 #pragma unroll
                         for (int l = 0; l < LGROUP; ++l)
@@ -406,8 +407,8 @@ __global__ void __launch_bounds__(NTHREAD, 1) oz_gemm_kernel(const __grid_consta
                 double *fj = P.fbuf + (size_t)(d.y >> 1) * 8 * vv + (size_t)d.grp * 4 * vv;
                 const double *eb = P.eb + (size_t)d.planeB * 2 * V;
 #pragma unroll
-                for (int c = 0; c < BN; ++c) {
-                    const int col = d.n0 + c;
+                for (int c = 0; c < WC; ++c) {
+                    const int col = d.n0 + half * WC + c;
                     if (col < 2 * V) {
                         const int ch = col >= V ? 1 : 0, cc = col - ch * V;
                         fj[(size_t)(rh + 2 * ch) * vv + b + (size_t)cc * V] = acc[c] * sa * __ldg(eb + col);
@@ -529,11 +530,14 @@ __global__ void __launch_bounds__(256) oz_slice_kernel(const SliceParams P)
 }
 
 // ------------------------------------------------------------------------------------------------
-// batched tengy over the f of a batch: one CTA per (tile pair, triple); the CTA's four sums go to
-// slot 0 of the triple's item (the other slots are zero), so item_reduce sums them in fixed order
+// batched tengy over the f of a batch: one CTA per (16-wide tile pair, triple), six or more CTAs per
+// SM.  A CTA's four sums go to its own slot of the triple's items (slot index = tile-pair index; the
+// 16-wide pairs fit in the 8 slots of each 32-wide item, and the slots no CTA writes are zero from
+// plan creation), so item_reduce sums them in a fixed order.
 // ------------------------------------------------------------------------------------------------
-constexpr int TNTHREAD = 512;
-constexpr size_t TSMEM_BYTES = (size_t)16 * TPTILE * sizeof(double);
+constexpr int TW = 16;
+constexpr int TNTHREAD = 256;
+constexpr size_t TSMEM_BYTES = (size_t)16 * TW * (TW + 1) * sizeof(double);
 
 struct TengyParams {
     trpdrv_dev_system sys;
@@ -541,12 +545,14 @@ struct TengyParams {
     const double *fbuf;
 };
 
-__global__ void __launch_bounds__(TNTHREAD, 1) oz_tengy_kernel(const TengyParams P)
+__global__ void __launch_bounds__(TNTHREAD) oz_tengy_kernel(const TengyParams P)
 {
     extern __shared__ __align__(16) double park[];
     __shared__ double red[4 * (TNTHREAD / 32)];
+    constexpr int TP = TW + 1, TILE = TW * TP;
     const trpdrv_dev_system &S = P.sys;
-    const int nvir = S.nvir, nb = S.nb, tid = threadIdx.x;
+    const int nvir = S.nvir, tid = threadIdx.x;
+    const int nb = (nvir + TW - 1) / TW;
     const long long pos = P.pos0 + blockIdx.y;
     if (pos >= S.ntriples) return;
     const long long tt = S.order ? (long long)S.order[pos] : pos;
@@ -560,24 +566,24 @@ __global__ void __launch_bounds__(TNTHREAD, 1) oz_tengy_kernel(const TengyParams
         ++B;
     }
     const int Cb = B + rem;
-    const int b0 = B * TT, c0 = Cb * TT;
+    const int b0 = B * TW, c0 = Cb * TW;
     const bool diag = (B == Cb);
     const size_t lnvv = (size_t)nvir * nvir;
     const double *f = P.fbuf + (size_t)blockIdx.y * 8 * lnvv;
 
+    // park f(B,C) (o = 0) and f(C,B) (o = 1) tiles of all eight f; column q of a tile is contiguous in f
     const int ntiles = diag ? 8 : 16;
-    for (int idx = tid; idx < ntiles * TT * TT; idx += TNTHREAD) {
-        const int tile = idx >> 10, q = (idx >> 5) & 31, r = idx & 31;
+    for (int idx = tid; idx < ntiles * TW * TW; idx += TNTHREAD) {
+        const int tile = idx / (TW * TW), q = (idx / TW) % TW, r = idx % TW;
         const int o = tile >> 3, xf = tile & 7;
         const int row = (o ? c0 : b0) + r, col = (o ? b0 : c0) + q;
         double v = 0.0;
         if (row < nvir && col < nvir) v = f[(size_t)xf * lnvv + row + (size_t)col * nvir];
-        park[tile * TPTILE + r * TPP + q] = v;
+        park[tile * TILE + r * TP + q] = v;
     }
     __syncthreads();
 
     TengyVecs v;
-    const int O = S.nocc;
     v.eorb = S.eorb;
     v.dintc1 = S.dintc + (size_t)i * nvir;
     v.dintx1 = S.dintx + (size_t)i * nvir;
@@ -585,22 +591,27 @@ __global__ void __launch_bounds__(TNTHREAD, 1) oz_tengy_kernel(const TengyParams
     v.dintc2 = S.dintc + (size_t)k * nvir;
     v.dintx2 = S.dintx + (size_t)k * nvir;
     v.t1v2 = S.t1v + (size_t)k * nvir;
-    v.voff = S.ncor + O;
+    v.voff = S.ncor + S.nocc;
     v.nvir = nvir;
     // omp/ccsd_trpdrv_omp_cbody.c:126 (a is 1-based, i/j/k here 0-based)
     v.eaijk = S.eorb[S.a - 1] - (S.eorb[S.ncor + i] + S.eorb[S.ncor + j] + S.eorb[S.ncor + k]);
     TengySums su = {0.0, 0.0, 0.0, 0.0};
-    tengy_tile_pair(park, b0, c0, diag, v, tid, TNTHREAD, su);
+    tengy_tile_pair_w<TW>(park, b0, c0, diag, v, tid, TNTHREAD, su);
     const TengySums tot = block_sum4(su, red);
-    double *out = S.partial + ((size_t)tt * S.npairs + blockIdx.x) * TRPDRV_FUSED_SLOTS * 4;
     if (tid == 0) {  // block_sum4's result is valid in thread 0
+        double *out = S.partial + ((size_t)tt * S.npairs * TRPDRV_FUSED_SLOTS + blockIdx.x) * 4;
         out[0] = tot.e4i;
         out[1] = tot.e5i;
         out[2] = tot.e4k;
         out[3] = tot.e5k;
-    } else if (tid >= 4 && tid < TRPDRV_FUSED_SLOTS * 4) {
-        out[tid] = 0.0;
     }
+}
+
+// number of 16-wide tile pairs (must fit in the npairs * TRPDRV_FUSED_SLOTS slots of a triple)
+static int tengy_pairs(int nvir)
+{
+    const int nb = (nvir + TW - 1) / TW;
+    return nb * (nb + 1) / 2;
 }
 
 // ------------------------------------------------------------------------------------------------
@@ -734,12 +745,13 @@ extern "C" int trpdrv_launch_oz_tengy(const trpdrv_dev_system *h_sys, int64_t po
                                       void *stream)
 {
     if (npos <= 0) return 0;
+    const int np = oz::tengy_pairs(h_sys->nvir);
+    if (np > h_sys->npairs * TRPDRV_FUSED_SLOTS) return (int)cudaErrorInvalidValue;
     oz::TengyParams P;
     P.sys = *h_sys;
     P.pos0 = pos0;
     P.fbuf = fbuf;
-    oz::oz_tengy_kernel<<<dim3((unsigned)h_sys->npairs, (unsigned)npos), oz::TNTHREAD, oz::TSMEM_BYTES,
-                          (cudaStream_t)stream>>>(P);
+    oz::oz_tengy_kernel<<<dim3((unsigned)np, (unsigned)npos), oz::TNTHREAD, oz::TSMEM_BYTES, (cudaStream_t)stream>>>(P);
     return (int)cudaGetLastError();
 }
 

@@ -20,27 +20,38 @@ struct TengyVecs {
     int nvir;
 };
 
-__device__ __forceinline__ void tengy_tile_pair(const double *park, int b0, int c0, bool diag,
-                                                const TengyVecs &v, int tid, int nthreads, TengySums &su)
+// Tengy terms of one tile pair {B, C} of width W from tiles parked in shared memory: park holds the
+// eight f tiles of orientation (B, C) followed (off the diagonal) by the eight of (C, B), each tile
+// W x (W + 1) doubles, element (row r, column q) at r * (W + 1) + q.
+template <int W>
+__device__ __forceinline__ void tengy_tile_pair_w(const double *park, int b0, int c0, bool diag, const TengyVecs &v,
+                                                  int tid, int nthreads, TengySums &su)
 {
-    const int nterm = diag ? TT * TT : 2 * TT * TT;
+    constexpr int P = W + 1, TILE = W * P;
+    const int nterm = diag ? W * W : 2 * W * W;
     for (int idx = tid; idx < nterm; idx += nthreads) {
-        const int s = idx >> 10, r = (idx >> 5) & 31, q = idx & 31;
+        const int s = idx / (W * W), r = (idx / W) % W, q = idx % W;
         const int b = (s ? c0 : b0) + r, c = (s ? b0 : c0) + q;
         if (b < v.nvir && c < v.nvir) {
-            const double *bcT = park + (s * 8) * TPTILE + r * TPP + q;
-            const double *cbT = park + ((diag ? 0 : 1 - s) * 8) * TPTILE + q * TPP + r;
+            const double *bcT = park + (s * 8) * TILE + r * P + q;
+            const double *cbT = park + ((diag ? 0 : 1 - s) * 8) * TILE + q * P + r;
             double fbc[8], fcb[8];
 #pragma unroll
             for (int f = 0; f < 8; ++f) {
-                fbc[f] = bcT[f * TPTILE];
-                fcb[f] = cbT[f * TPTILE];
+                fbc[f] = bcT[f * TILE];
+                fcb[f] = cbT[f * TILE];
             }
             const double denom = -1.0 / (__ldg(v.eorb + v.voff + b) + __ldg(v.eorb + v.voff + c) + v.eaijk);
             tengy_term(fbc, fcb, denom, __ldg(v.t1v1 + b), __ldg(v.t1v2 + b), __ldg(v.dintx1 + c),
                        __ldg(v.dintx2 + c), __ldg(v.dintc1 + c), __ldg(v.dintc2 + c), su);
         }
     }
+}
+
+__device__ __forceinline__ void tengy_tile_pair(const double *park, int b0, int c0, bool diag,
+                                                const TengyVecs &v, int tid, int nthreads, TengySums &su)
+{
+    tengy_tile_pair_w<TT>(park, b0, c0, diag, v, tid, nthreads, su);
 }
 
 }  // namespace trpdrv

@@ -4,7 +4,7 @@ Default workload: the fused persistent FP64 kernel over every (i,j,k) triple of 
 nocc=40, nvir=300 (32,800 triples, 16.06 TFLOP per step), seeded synthetic inputs resident in HBM
 (1.52 GB > the 126 MB L2, so no L2 flush is needed between steps).
 
-  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference] [--workload c2|c3|c4]
 
 --impl b200 (default): `value` = triples/s of the fused kernel on device-resident inputs (CUDA events,
   max over ranks); `e2e` = the same metric through the C ABI with host buffers (pinned host -> device
@@ -16,6 +16,15 @@ nocc=40, nvir=300 (32,800 triples, 16.06 TFLOP per step), seeded synthetic input
 --impl reference: the reference's CPU path alone (oracle/_ref/libtrpdrv_ref.so: the reference
   omp/ccsd_trpdrv_omp_cbody.c + omp/ccsd_tengy_c99.c compiled unmodified), each step a bounded sample of
   the same workload's triples; rank 0 only.
+  The default line also carries `emulated`: the emulated-FP64 form (Ozaki int8 digit slices on the
+  tcgen05 tensor cores, TRPDRV_MODE_EMULATED) on the same inputs for 5..8 slices, with its speedup over
+  the native FP64 fused kernel and its error against it.
+--workload c3: the emulated form at nocc=30, nvir=400 with log-uniform integral magnitudes in
+  [1e-6, 1]: `value` = triples/s of the emulated form (7 slices), beside the native FP64 fused kernel
+  on the same system and the slice sweep with its errors.
+--workload c4: six systems of uneven size, (8,80) (12,150) (16,220) (24,310) (32,380) (40,450), in
+  one fused FP64 launch: `value` = aggregate triples/s; per-system energies checked against
+  single-system plans; compared with one plain FP64 launch pair per triple, serially per system.
 With torchrun (N > 1) the triples are split over ranks (strong scaling) and the two energies are summed
 with one NCCL all-reduce per step.
 """
@@ -34,6 +43,10 @@ sys.path.insert(0, os.path.join(ROOT, "nwchem-ccsd-trpdrv_b200"))
 
 METRIC = "(T) triples/s & FP64-equiv TFLOP/s, fused/emulated vs plain FP64 GPU"
 NOCC, NVIR, SEED = 40, 300, 2024
+C3 = (30, 400)
+C4 = [(8, 80), (12, 150), (16, 220), (24, 310), (32, 380), (40, 450)]
+SLICES = (5, 6, 7, 8)
+DEFAULT_SLICES = 7
 
 
 def parse():
@@ -47,11 +60,15 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--mma-k", type=int, default=8, choices=[4, 8], help="FP64 MMA shape of the fused kernel")
+    ap.add_argument("--workload", default="c2", choices=["c2", "c3", "c4"])
+    ap.add_argument("--no-emulated", action="store_true", help="skip the emulated-FP64 sweep of the default line")
     ap.add_argument("--profile", action="store_true",
                     help="fused steps only (no probes, e2e, plain or CPU legs): the command profiled with ncu")
     args = ap.parse_args()
     if args.profile:
-        args.no_cpu_baseline = args.no_plain = True
+        args.no_cpu_baseline = args.no_plain = args.no_emulated = True
+    if args.workload == "c3":
+        args.nocc, args.nvir = C3
     return args
 
 
@@ -101,27 +118,37 @@ def run_reference_arm(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    n_all = args.nocc * args.nocc * (args.nocc + 1) // 2
-    vals = []
-    per_step = None
+    shapes = C4 if args.workload == "c4" else [(args.nocc, args.nvir)]
+    counts = [o * o * (o + 1) // 2 for o, _ in shapes]
+    n_all = sum(counts)
+    flop_all = sum(c * 16.0 * v * v * (v + o) for c, (o, v) in zip(counts, shapes))
+    budget = 8.0 / len(shapes)
+    vals, per_step = [], None
     for step in range(args.warmup + args.steps):
-        v, n, el, ncpu = time_reference_cpu(args.nocc, args.nvir, budget_s=8.0)
-        per_step = (n, el, ncpu)
+        sec, timed, ncpu = 0.0, 0, os.cpu_count()
+        for c, (o, v) in zip(counts, shapes):
+            rate, n, el, ncpu = time_reference_cpu(o, v, budget_s=budget)
+            sec += c / rate  # the system's full triple count at the sampled rate
+            timed += n
+        per_step = (timed, ncpu)
         if step >= args.warmup:
-            vals.append(v)
+            vals.append(n_all / sec)
     value = statistics.median(vals)
+    cfg = workload(args.nocc, args.nvir) if args.workload != "c4" else {
+        "workload": "six systems of uneven size: " + ", ".join(f"({o},{v})" for o, v in C4),
+        "triples_per_step": n_all, "flop_per_step": flop_all}
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": "triples/s", "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * n_all / value,
         "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic (seeded counter-based generator, reference config distributions)",
-        "config": workload(args.nocc, args.nvir),
-        "cpu_baseline": {"value": value, "unit": "triples/s", "cores": per_step[2], "kind": "reference",
-                         "sample": f"{per_step[0]} consecutive triples per step (of {n_all}), serial calls of the "
-                                   f"reference body with {per_step[2]} OpenMP + OpenBLAS threads, ~8 s per step; "
-                                   f"ms_per_step extrapolates to the full workload"},
+        "config": cfg,
+        "cpu_baseline": {"value": value, "unit": "triples/s", "cores": per_step[1], "kind": "reference",
+                         "sample": f"{per_step[0]} consecutive triples per step (of {n_all}, every system sampled), "
+                                   f"serial calls of the reference body with {per_step[1]} OpenMP + OpenBLAS "
+                                   f"threads, ~8 s per step; ms_per_step extrapolates to the full workload"},
         "e2e": {"value": value, "unit": "triples/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
-        "tflops_fp64_equiv": value * 16.0 * args.nvir ** 2 * (args.nvir + args.nocc) / 1e12,
+        "tflops_fp64_equiv": value * flop_all / n_all / 1e12,
     }
     print(json.dumps(line), flush=True)
 
@@ -183,187 +210,379 @@ def read_profile_traffic():
     return None
 
 
+class Ranks:
+    """torch.distributed plumbing: one process per GPU, NCCL; everything here is a no-op at N = 1."""
+
+    def __init__(self):
+        import torch
+        import torch.distributed as dist
+        self.torch, self.dist = torch, dist
+        self.world = int(os.environ.get("WORLD_SIZE", "1"))
+        self.rank = int(os.environ.get("RANK", "0"))
+        self.local = int(os.environ.get("LOCAL_RANK", "0"))
+        torch.cuda.set_device(self.local)
+        self.dev = torch.device("cuda", self.local)
+        if self.world > 1:
+            import datetime
+            dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=self.dev)
+        # a stream of our own: the library's launches and the timing events go to the same stream (a
+        # handle of 0 would make each plan fall back to its own stream, which the events would not see)
+        self.stream = torch.cuda.Stream(device=self.dev)
+        self.sp = self.stream.cuda_stream
+        assert self.sp != 0
+
+    def barrier(self):
+        if self.world > 1:
+            self.dist.barrier()
+
+    def sum(self, vals):
+        if self.world == 1:
+            return list(vals)
+        t = self.torch.tensor(list(vals), dtype=self.torch.float64, device=self.dev)
+        self.dist.all_reduce(t)
+        return t.tolist()
+
+    def max(self, v):
+        if self.world == 1:
+            return v
+        t = self.torch.tensor([v], dtype=self.torch.float64, device=self.dev)
+        self.dist.all_reduce(t, op=self.dist.ReduceOp.MAX)
+        return float(t.item())
+
+    def close(self):
+        if self.world > 1:
+            self.dist.destroy_process_group()
+
+
+def measure_peaks(T, R, skip):
+    """FP64: the library's probes (DMMA m16n8k4/k8/k16, DFMA) and cuBLAS DGEMM 8192^3; int8: cuBLASLt
+    int8 GEMM 8192^3 (torch._int_mm), the denominator of the emulated form's tensor-pipe fraction."""
+    torch = R.torch
+    probe, cublas_dgemm, int8 = {1: 0.0, 2: 0.0, 3: 0.0, 4: 0.0}, 0.0, None
+    if skip:
+        return probe, cublas_dgemm, int8
+    probe = {k: T.probe_fp64_peak(k, R.local) for k in (1, 2, 3, 4)}
+
+    def best_of(fn, flop, reps=3):
+        fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(reps):
+            fn()
+        e1.record()
+        torch.cuda.synchronize()
+        return reps * flop / (e0.elapsed_time(e1) * 1e-3) / 1e12
+
+    a = torch.randn(8192, 8192, dtype=torch.float64, device=R.dev)
+    cublas_dgemm = best_of(lambda: torch.matmul(a, a), 2 * 8192 ** 3)
+    del a
+    try:
+        ai = torch.randint(-64, 65, (8192, 8192), dtype=torch.int8, device=R.dev)
+        int8 = best_of(lambda: torch._int_mm(ai, ai), 2 * 8192 ** 3, reps=10)
+        del ai
+    except Exception:
+        int8 = None
+    return probe, cublas_dgemm, int8
+
+
+def time_plan(T, R, plan, steps, warmup):
+    """Device time per step (CUDA events on the launching stream, max over ranks), the plan's kernel time
+    per step (events around its launches), launches, and the all-reduced per-system energies."""
+    torch = R.torch
+
+    def step():
+        plan.execute(stream=R.sp)
+        e4, e5 = plan.energies()
+        return R.sum(list(e4) + list(e5))
+
+    for _ in range(warmup):
+        step()
+    torch.cuda.synchronize()
+    R.barrier()
+    torch.cuda.synchronize()
+    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    kernel_ms, launches, tot = [], 0, None
+    start.record(R.stream)
+    for _ in range(steps):
+        tot = step()
+        kernel_ms.append(plan.last_kernel_ms())
+        launches += plan.last_launches()
+    end.record(R.stream)
+    torch.cuda.synchronize()
+    R.barrier()
+    torch.cuda.synchronize()
+    elapsed = R.max(start.elapsed_time(end) * 1e-3)
+    n = len(plan.systems)
+    return elapsed / steps, statistics.mean(kernel_ms), launches, tot[:n], tot[n:]
+
+
+def time_e2e(T, R, plan, steps, warmup):
+    """Through the C ABI with host buffers: pinned host -> device copy of every input (trpdrv_plan_upload),
+    execute, device -> host read of the energies; seconds per step, max over ranks."""
+    torch = R.torch
+    times = []
+    for it in range(warmup + steps):
+        torch.cuda.synchronize()
+        R.barrier()
+        t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        t0.record(R.stream)
+        plan.upload(stream=R.sp)
+        plan.execute(stream=R.sp)
+        e4, e5 = plan.energies()
+        t1.record(R.stream)
+        torch.cuda.synchronize()
+        R.sum(list(e4) + list(e5))
+        el = R.max(t0.elapsed_time(t1) * 1e-3)
+        if it >= warmup:
+            times.append(el)
+    return statistics.mean(times)
+
+
+def emulated_ops_per_triple(nocc, nvir, slices):
+    """Algorithmic int8 operations of one triple in the emulated form: two 2V x 2V x (V + O) products
+    per digit pair, slices (slices + 1) / 2 digit pairs, 2 operations per multiply-add."""
+    return 2 * (2 * nvir) ** 2 * (nvir + nocc) * 2 * slices * (slices + 1) / 2
+
+
+def emulated_sweep(T, R, systems, ref_e4, ref_e5, steps, warmup, slice_list, int8_peak):
+    """The emulated form on the same systems for each slice count: triples/s, FP64-equivalent TFLOP/s,
+    int8 tensor-pipe rate and its error against the native FP64 fused result."""
+    out = {}
+    n_all = sum(T.count_triples(s.nocc) for s in systems)
+    flop = sum(T.count_triples(s.nocc) * T.triple_flops(s.nocc, s.nvir) for s in systems)
+    for sl in slice_list:
+        with T.Plan(systems, mode=T.MODE_EMULATED, slices=sl, rank=R.rank, world=R.world, device=R.local) as p:
+            p.upload(stream=R.sp)
+            sec, kms, launches, e4, e5 = time_plan(T, R, p, steps, warmup)
+            mine = sum(p.num_triples(q) * emulated_ops_per_triple(s.nocc, s.nvir, sl) for q, s in enumerate(systems))
+        ops = R.sum([mine])[0]
+        r4 = max(abs(a - b) / abs(b) for a, b in zip(e4, ref_e4))
+        r5 = max(abs(a - b) / abs(b) for a, b in zip(e5, ref_e5))
+        int8_tops = ops / sec / 1e12
+        out[str(sl)] = {"value": n_all / sec, "unit": "triples/s", "ms_per_step": 1e3 * sec,
+                        "tflops_fp64_equiv": flop / sec / 1e12, "kernel_ms": kms, "gpu_launches": launches,
+                        "int8_tops": int8_tops, "int8_frac": (int8_tops / int8_peak) if int8_peak else None,
+                        "emp4_rel_err_vs_fp64": r4, "emp5_rel_err_vs_fp64": r5}
+    return out
+
+
+def plain_sample(T, R, s, flop_triple, frac=16):
+    """The plain per-triple path (BASELINE config 1's method) on 1/frac of one system's triples."""
+    torch = R.torch
+    with T.Plan([s], mode=T.MODE_PLAIN, rank=0, world=frac, device=R.local) as pp:
+        pp.upload(stream=R.sp)
+        pp.execute(stream=R.sp)
+        pp.energies()
+        pe0, pe1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        pe0.record(R.stream)
+        pp.execute(stream=R.sp)
+        pe1.record(R.stream)
+        pp.energies()
+        pms = pe0.elapsed_time(pe1)
+        nplain = pp.num_triples(0)
+    return {"value": nplain / (pms * 1e-3), "unit": "triples/s",
+            "sample": f"{nplain} triples (1/{frac} of nocc={s.nocc} nvir={s.nvir}, driver order), one grouped "
+                      f"16-GEMM launch + one tengy launch per triple",
+            "tflops_fp64_equiv": nplain * flop_triple / (pms * 1e-3) / 1e12}
+
+
+def cpu_leg(args, R, nocc, nvir):
+    if R.rank != 0 or R.world != 1 or args.no_cpu_baseline:
+        return None
+    try:
+        v, n, el, ncpu = time_reference_cpu(nocc, nvir, budget_s=15.0)
+        return {"value": v, "unit": "triples/s", "cores": ncpu, "kind": "reference",
+                "sample": f"{n} consecutive triples of nocc={nocc} nvir={nvir}, serial calls of the reference body "
+                          f"(oracle/_ref: omp/ccsd_trpdrv_omp_cbody.c + omp/ccsd_tengy_c99.c, OpenBLAS 0.3.30), "
+                          f"{ncpu} OpenMP + OpenBLAS threads, {el:.1f} s"}
+    except Exception as ex:  # the reference build is missing
+        return {"value": None, "unit": "triples/s", "cores": os.cpu_count(), "kind": "reference",
+                "sample": f"unavailable: {ex}"}
+
+
+def base_line(args, R, value, sec, config):
+    return {"metric": METRIC, "value": value, "unit": "triples/s", "n_gpus": R.world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1e3 * sec, "higher_is_better": True, "scaling": "strong",
+            "vs_baseline": None, "data": "synthetic (seeded counter-based generator, reference config distributions)",
+            "config": config}
+
+
+def fp64_roofline(achieved, peak, traffic, kms):
+    return {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
+            "traffic": traffic,
+            "peak_source": "measured live on this device: max of the library's FP64 probes (DMMA m16n8k4/k8/k16 "
+                           "and DFMA, register operands, 50 ms bursts) and cuBLAS DGEMM 8192^3; "
+                           "MEASURED_PEAKS.json has no FP64 entry",
+            "kernel_ms": kms}
+
+
 def run_b200_arm(args):
-    import torch
-    import torch.distributed as dist
     import trpdrv_b200 as T
-
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    torch.cuda.set_device(local)
-    if world > 1:
-        import datetime
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=torch.device("cuda", local))
-    dev = torch.device("cuda", local)
-    stream = torch.cuda.current_stream(dev)
-    sp = stream.cuda_stream
-
-    wl = workload(args.nocc, args.nvir)
-    n_all = wl["triples_per_step"]
-    flop_triple = wl["flop_per_triple"]
+    R = Ranks()
 
     # inputs in pinned host memory (the e2e leg copies them every step)
     pinned = []
 
     def alloc(n):
-        t = torch.empty(n, dtype=torch.float64).pin_memory()
+        t = R.torch.empty(n, dtype=R.torch.float64).pin_memory()
         pinned.append(t)
         return t.numpy()
 
-    s = T.synth_system(args.nocc, args.nvir, seed=SEED, alloc=alloc)
-    in_bytes = s.nbytes()
+    if args.workload == "c4":
+        systems = [T.synth_system(o, v, seed=SEED + q, alloc=alloc) for q, (o, v) in enumerate(C4)]
+    else:
+        dist = T.DIST_LOGUNIFORM if args.workload == "c3" else T.DIST_UNIFORM
+        systems = [T.synth_system(args.nocc, args.nvir, seed=SEED, dist=dist, alloc=alloc)]
+    in_bytes = sum(s.nbytes() for s in systems)
+    n_all = sum(T.count_triples(s.nocc) for s in systems)
+    flop_all = sum(T.count_triples(s.nocc) * T.triple_flops(s.nocc, s.nvir) for s in systems)
 
-    # FP64 peak of this device (library probe; best of the DMMA shapes) and cuBLAS DGEMM for context
-    probe, cublas_dgemm = {1: 0.0, 2: 0.0, 3: 0.0, 4: 0.0}, 0.0
-    if not args.profile:
-        probe = {k: T.probe_fp64_peak(k, local) for k in (1, 2, 3, 4)}
-        a = torch.randn(8192, 8192, dtype=torch.float64, device=dev)
-        torch.matmul(a, a)
-        torch.cuda.synchronize()
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record()
-        for _ in range(3):
-            torch.matmul(a, a)
-        e1.record()
-        torch.cuda.synchronize()
-        cublas_dgemm = 3 * 2 * 8192 ** 3 / (e0.elapsed_time(e1) * 1e-3) / 1e12
-        del a
-    # roofline denominator: the best FP64 rate measured on this device (DMMA shapes, DFMA, cuBLAS DGEMM)
+    probe, cublas_dgemm, int8_peak = measure_peaks(T, R, args.profile)
     peak = max(max(probe.values()), cublas_dgemm) or 1.0
+    fp64_probe = {"dmma_m16n8k4": probe[1], "dmma_m16n8k8": probe[2], "dmma_m16n8k16": probe[3],
+                  "dfma": probe[4], "cublas_dgemm_8192": cublas_dgemm}
 
-    plan = T.Plan([s], mode=T.MODE_FUSED, rank=rank, world=world, device=local, mma_k=args.mma_k)
-    plan.upload(stream=sp)
-    my_triples = plan.num_triples(0)
-
-    def barrier():
-        if world > 1:
-            dist.barrier()
-
-    def step():
-        plan.execute(stream=sp)
-        e4, e5 = plan.energies()
-        if world > 1:
-            t = torch.tensor([e4[0], e5[0]], dtype=torch.float64, device=dev)
-            dist.all_reduce(t)
-            return t
-        return None
-
-    for _ in range(args.warmup):
-        step()
-    torch.cuda.synchronize()
-    barrier()
-    torch.cuda.synchronize()
-    clocks = ClockSampler(local)
-    clocks.start()
-    time.sleep(0.3)
-    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    kernel_ms, launches = [], 0
-    start.record(stream)
-    for _ in range(args.steps):
-        step()
-        kernel_ms.append(plan.last_kernel_ms())
-        launches += plan.last_launches()
-    end.record(stream)
-    torch.cuda.synchronize()
-    barrier()
-    torch.cuda.synchronize()
-    ck = clocks.stop()
-    elapsed = start.elapsed_time(end) * 1e-3
-    if world > 1:
-        t = torch.tensor([elapsed], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        elapsed = float(t.item())
-    value = n_all / (elapsed / args.steps)
-    e4, e5 = plan.energies()
-
-    # e2e through the C ABI with host buffers: H2D of every input + execute + D2H of the energies
-    e2e_times = []
-    for it in range(0 if args.profile else args.warmup + args.steps):
-        torch.cuda.synchronize()
-        barrier()
-        t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        t0.record(stream)
-        plan.upload(stream=sp)
-        step()
-        t1.record(stream)
-        torch.cuda.synchronize()
-        el = t0.elapsed_time(t1) * 1e-3
-        if world > 1:
-            tt = torch.tensor([el], dtype=torch.float64, device=dev)
-            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-            el = float(tt.item())
-        if it >= args.warmup:
-            e2e_times.append(el)
-    e2e_value = n_all / statistics.mean(e2e_times) if e2e_times else None
+    # the native FP64 fused kernel (the headline of c2 and c4, the comparison of c3)
+    plan = T.Plan(systems, mode=T.MODE_FUSED, rank=R.rank, world=R.world, device=R.local, mma_k=args.mma_k)
+    plan.upload(stream=R.sp)
+    my_flop = sum(plan.num_triples(q) * T.triple_flops(s.nocc, s.nvir) for q, s in enumerate(systems))
+    clocks = None
+    if args.workload != "c3":
+        clocks = ClockSampler(R.local)
+        clocks.start()
+        time.sleep(0.3)
+    sec, kms, launches, e4, e5 = time_plan(T, R, plan, args.steps, args.warmup)
+    ck = clocks.stop() if clocks else None
+    e2e_sec = None
+    if not args.profile and args.workload != "c3":
+        e2e_sec = time_e2e(T, R, plan, args.steps, args.warmup)
+    # per-system energies of the batch against single-system plans (c4)
+    singles = None
+    if args.workload == "c4":
+        singles = []
+        for q, s in enumerate(systems):
+            with T.Plan([s], mode=T.MODE_FUSED, rank=R.rank, world=R.world, device=R.local) as p1:
+                p1.upload(stream=R.sp)
+                _, _, _, a4, a5 = time_plan(T, R, p1, 1, 0)
+            singles.append(bool(a4[0] == e4[q] and a5[0] == e5[q]))
     plan.close()
+    achieved = my_flop / (kms * 1e-3) / 1e12
 
-    # plain per-triple GPU path on a bounded sample of the same workload (1/16 of the triples)
+    # emulated-FP64 form on the same systems
+    emulated = None
+    if not args.no_emulated and args.workload in ("c2", "c3"):
+        if args.workload == "c3":
+            clocks = ClockSampler(R.local)
+            clocks.start()
+            time.sleep(0.3)
+        emulated = emulated_sweep(T, R, systems, e4, e5, args.steps, args.warmup, SLICES, int8_peak)
+        if args.workload == "c3":
+            ck = clocks.stop()
+    emu_e2e_sec = None
+    if args.workload == "c3" and not args.no_emulated:
+        with T.Plan(systems, mode=T.MODE_EMULATED, slices=DEFAULT_SLICES, rank=R.rank, world=R.world,
+                    device=R.local) as p:
+            p.upload(stream=R.sp)
+            emu_e2e_sec = time_e2e(T, R, p, args.steps, args.warmup)
+
+    # plain per-triple GPU path: a bounded sample of each system, serially
     plain = None
-    if not args.no_plain and rank == 0:
-        with T.Plan([s], mode=T.MODE_PLAIN, rank=0, world=16, device=local) as pp:
-            pp.upload(stream=sp)
-            pp.execute(stream=sp)
-            pp.energies()
-            pe0, pe1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            pe0.record(stream)
-            pp.execute(stream=sp)
-            pe1.record(stream)
-            pp.energies()
-            pms = pe0.elapsed_time(pe1)
-            nplain = pp.num_triples(0)
-        plain = {"value": nplain / (pms * 1e-3), "unit": "triples/s", "sample": f"{nplain} triples (1/16 of the "
-                 f"workload, driver order), one grouped 16-GEMM launch + one tengy launch per triple",
-                 "tflops_fp64_equiv": nplain * flop_triple / (pms * 1e-3) / 1e12}
+    if not args.no_plain and R.rank == 0:
+        if args.workload == "c4":
+            per = [plain_sample(T, R, s, T.triple_flops(s.nocc, s.nvir), frac=32) for s in systems]
+            serial_sec = sum(T.count_triples(s.nocc) / pl["value"] for s, pl in zip(systems, per))
+            plain = {"value": n_all / serial_sec, "unit": "triples/s",
+                     "sample": "1/32 of each system's triples, one grouped 16-GEMM launch + one tengy launch per "
+                               "triple, systems one after another; serial time extrapolated by triple counts",
+                     "tflops_fp64_equiv": flop_all / serial_sec / 1e12, "per_system": per}
+        else:
+            s = systems[0]
+            plain = plain_sample(T, R, s, T.triple_flops(s.nocc, s.nvir))
 
-    cpu = None
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        try:
-            v, n, el, ncpu = time_reference_cpu(args.nocc, args.nvir, budget_s=15.0)
-            cpu = {"value": v, "unit": "triples/s", "cores": ncpu, "kind": "reference",
-                   "sample": f"{n} consecutive triples of the same system, serial calls of the reference body "
-                             f"(oracle/_ref: omp/ccsd_trpdrv_omp_cbody.c + omp/ccsd_tengy_c99.c, OpenBLAS 0.3.30), "
-                             f"{ncpu} OpenMP + OpenBLAS threads, {el:.1f} s"}
-        except Exception as ex:  # the reference build is missing
-            cpu = {"value": None, "unit": "triples/s", "cores": os.cpu_count(), "kind": "reference",
-                   "sample": f"unavailable: {ex}"}
-
-    if rank != 0:
-        if world > 1:
-            dist.destroy_process_group()
+    if R.rank != 0:
+        R.close()
         return
-    kms = statistics.mean(kernel_ms)
-    achieved = my_triples * flop_triple / (kms * 1e-3) / 1e12
-    traffic = read_profile_traffic()
-    line = {
-        "metric": METRIC, "value": value, "unit": "triples/s", "n_gpus": world, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": 1e3 * elapsed / args.steps, "higher_is_better": True,
-        "scaling": "strong", "vs_baseline": None, "dtype": "f64",
-        "data": "synthetic (seeded counter-based generator, reference config distributions)",
-        "config": dict(wl, parallelism=f"triples sharded over {world} rank(s), one 2-double all-reduce per step",
-                       mma=f"m16n8k{args.mma_k} f64"),
-        "tflops_fp64_equiv": value * flop_triple / 1e12,
-        "emp4": e4[0], "emp5": e5[0],
-        "roofline": {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
-                     "frac": achieved / peak, "traffic": traffic,
-                     "peak_source": "measured live on this device: max of the library's FP64 probes (DMMA "
-                                    "m16n8k4/k8/k16 and DFMA, register operands, 50 ms bursts) and cuBLAS DGEMM "
-                                    "8192^3; MEASURED_PEAKS.json has no FP64 entry",
-                     "kernel_ms": kms},
-        "fp64_probe_tflops": {"dmma_m16n8k4": probe[1], "dmma_m16n8k8": probe[2], "dmma_m16n8k16": probe[3],
-                              "dfma": probe[4], "cublas_dgemm_8192": cublas_dgemm},
-        "e2e": {"value": e2e_value, "unit": "triples/s", "h2d_bytes_per_step": in_bytes,
-                "d2h_bytes_per_step": 16, "path": "trpdrv_plan_upload (pinned host) + trpdrv_plan_execute + "
-                                                  "trpdrv_plan_energies"},
-        "gpu_launches": launches,
-        "clocks": ck,
-        "plain_gpu": plain,
-        "speedup_vs_plain": (value / plain["value"]) if plain else None,
-        "cpu_baseline": cpu,
-    }
+    traffic = read_profile_traffic() if args.workload == "c2" else None
+    if args.workload == "c3":
+        emu = emulated[str(DEFAULT_SLICES)] if emulated else None
+        value = emu["value"] if emu else n_all / sec
+        wsec = (emu["ms_per_step"] * 1e-3) if emu else sec
+        cfg = {"workload": f"emulated-FP64 triples body (Ozaki int8 digit slices on tcgen05, {DEFAULT_SLICES} slices, "
+                           f"FP64 energies), nocc={args.nocc} nvir={args.nvir}, log-uniform integral magnitudes "
+                           f"in [1e-6, 1], all {n_all} (i,j,k) triples of one a per step",
+               "nocc": args.nocc, "nvir": args.nvir, "triples_per_step": n_all, "slices": DEFAULT_SLICES,
+               "flop_per_triple": T.triple_flops(args.nocc, args.nvir),
+               "l2": "inputs resident in HBM exceed the 126 MB L2; no flush between steps",
+               "parallelism": f"triples sharded over {R.world} rank(s), one 2-double all-reduce per step"}
+        line = base_line(args, R, value, wsec, cfg)
+        line.update({
+            "dtype": "int8 (emulated f64)",
+            "tflops_fp64_equiv": flop_all / wsec / 1e12,
+            "roofline": {"bound": "tensor", "achieved": emu["int8_tops"] if emu else None, "peak": int8_peak,
+                         "unit": "TOPS (int8)", "frac": emu["int8_frac"] if emu else None, "traffic": None,
+                         "peak_source": "cuBLASLt int8 GEMM 8192^3 (torch._int_mm) measured live on this device; "
+                                        "achieved = algorithmic int8 operations of the digit-pair products over the "
+                                        "whole step (slicing, products and FP64 energies)",
+                         "kernel_ms": emu["kernel_ms"] if emu else None},
+            "fp64_fused": {"value": n_all / sec, "unit": "triples/s", "ms_per_step": 1e3 * sec,
+                           "tflops_fp64_equiv": flop_all / sec / 1e12, "roofline_frac": achieved / peak,
+                           "emp4": e4[0], "emp5": e5[0]},
+            "speedup_vs_fp64_fused": (value / (n_all / sec)),
+            "emulated_slices": emulated,
+            "int8_peak_tops": int8_peak, "fp64_probe_tflops": fp64_probe,
+            "e2e": {"value": (n_all / emu_e2e_sec) if emu_e2e_sec else None, "unit": "triples/s",
+                    "h2d_bytes_per_step": in_bytes, "d2h_bytes_per_step": 16,
+                    "path": "trpdrv_plan_upload (pinned host) + trpdrv_plan_execute + trpdrv_plan_energies"},
+            "gpu_launches": emu["gpu_launches"] if emu else launches,
+            "clocks": ck, "plain_gpu": plain,
+            "speedup_vs_plain": (value / plain["value"]) if plain else None,
+            "cpu_baseline": cpu_leg(args, R, args.nocc, args.nvir),
+        })
+    else:
+        value = n_all / sec
+        if args.workload == "c4":
+            cfg = {"workload": "fused persistent FP64 triples body over six systems of uneven size in one launch: "
+                               + ", ".join(f"({o},{v})" for o, v in C4) + f"; all {n_all} triples of one a each",
+                   "systems": [{"nocc": s.nocc, "nvir": s.nvir, "triples": T.count_triples(s.nocc)} for s in systems],
+                   "triples_per_step": n_all, "flop_per_step": flop_all,
+                   "l2": "inputs resident in HBM exceed the 126 MB L2; no flush between steps",
+                   "parallelism": f"triples sharded over {R.world} rank(s), one all-reduce of 12 doubles per step"}
+        else:
+            cfg = dict(workload(args.nocc, args.nvir),
+                       parallelism=f"triples sharded over {R.world} rank(s), one 2-double all-reduce per step")
+        cfg["mma"] = f"m16n8k{args.mma_k} f64"
+        line = base_line(args, R, value, sec, cfg)
+        line.update({
+            "dtype": "f64",
+            "tflops_fp64_equiv": flop_all / sec / 1e12,
+            "roofline": fp64_roofline(achieved, peak, traffic, kms),
+            "fp64_probe_tflops": fp64_probe,
+            "e2e": {"value": (n_all / e2e_sec) if e2e_sec else None, "unit": "triples/s",
+                    "h2d_bytes_per_step": in_bytes, "d2h_bytes_per_step": 16 * len(systems),
+                    "path": "trpdrv_plan_upload (pinned host) + trpdrv_plan_execute + trpdrv_plan_energies"},
+            "gpu_launches": launches,
+            "clocks": ck,
+            "plain_gpu": plain,
+            "speedup_vs_plain": (value / plain["value"]) if plain else None,
+        })
+        if args.workload == "c4":
+            line["emp4"], line["emp5"] = e4, e5
+            line["per_system_equals_single_runs"] = singles
+            line["cpu_baseline"] = cpu_leg(args, R, *C4[-1])
+            if line["cpu_baseline"]:
+                line["cpu_baseline"]["sample"] += " (largest system only)"
+        else:
+            line["emp4"], line["emp5"] = e4[0], e5[0]
+            line["cpu_baseline"] = cpu_leg(args, R, args.nocc, args.nvir)
+            if emulated:
+                emu = emulated[str(DEFAULT_SLICES)]
+                line["emulated"] = {"default_slices": DEFAULT_SLICES, "value": emu["value"], "unit": "triples/s",
+                                    "speedup_vs_fp64_fused": emu["value"] / value,
+                                    "speedup_vs_plain": (emu["value"] / plain["value"]) if plain else None,
+                                    "int8_peak_tops": int8_peak, "slices": emulated}
     print(json.dumps(line), flush=True)
-    if world > 1:
-        dist.destroy_process_group()
+    R.close()
 
 
 def main():

@@ -55,20 +55,23 @@ def parse():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--nocc", type=int, default=NOCC)
-    ap.add_argument("--nvir", type=int, default=NVIR)
+    ap.add_argument("--nocc", type=int, default=None, help="default 40 (c2) / 30 (c3)")
+    ap.add_argument("--nvir", type=int, default=None, help="default 300 (c2) / 400 (c3)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--mma-k", type=int, default=8, choices=[4, 8], help="FP64 MMA shape of the fused kernel")
     ap.add_argument("--workload", default="c2", choices=["c2", "c3", "c4"])
     ap.add_argument("--no-emulated", action="store_true", help="skip the emulated-FP64 sweep of the default line")
     ap.add_argument("--profile", action="store_true",
-                    help="fused steps only (no probes, e2e, plain or CPU legs): the command profiled with ncu")
+                    help="the timed plan only (c2/c4: fused FP64; c3: emulated, 7 slices), no probes, e2e, plain "
+                         "or CPU legs: the command profiled with ncu")
     args = ap.parse_args()
     if args.profile:
-        args.no_cpu_baseline = args.no_plain = args.no_emulated = True
-    if args.workload == "c3":
-        args.nocc, args.nvir = C3
+        args.no_cpu_baseline = args.no_plain = True
+        args.no_emulated = args.workload != "c3"
+    dn, dv = C3 if args.workload == "c3" else (NOCC, NVIR)
+    args.nocc = dn if args.nocc is None else args.nocc
+    args.nvir = dv if args.nvir is None else args.nvir
     return args
 
 
@@ -442,6 +445,17 @@ def run_b200_arm(args):
     peak = max(max(probe.values()), cublas_dgemm) or 1.0
     fp64_probe = {"dmma_m16n8k4": probe[1], "dmma_m16n8k8": probe[2], "dmma_m16n8k16": probe[3],
                   "dfma": probe[4], "cublas_dgemm_8192": cublas_dgemm}
+
+    if args.profile and args.workload == "c3":
+        with T.Plan(systems, mode=T.MODE_EMULATED, slices=DEFAULT_SLICES, rank=R.rank, world=R.world,
+                    device=R.local) as p:
+            p.upload(stream=R.sp)
+            sec, kms, launches, e4, e5 = time_plan(T, R, p, args.steps, args.warmup)
+        if R.rank == 0:
+            print(json.dumps({"profile": "emulated", "slices": DEFAULT_SLICES, "nocc": args.nocc, "nvir": args.nvir,
+                              "ms_per_step": 1e3 * sec, "kernel_ms": kms, "gpu_launches": launches}), flush=True)
+        R.close()
+        return
 
     # the native FP64 fused kernel (the headline of c2 and c4, the comparison of c3)
     plan = T.Plan(systems, mode=T.MODE_FUSED, rank=R.rank, world=R.world, device=R.local, mma_k=args.mma_k)

@@ -214,6 +214,26 @@ int64_t trpdrv_plan_last_launches(const trpdrv_plan *plan);
 int trpdrv_plan_last_kernel_ms(trpdrv_plan *plan, double *ms);
 int trpdrv_plan_destroy(trpdrv_plan *plan);
 
+/* Autotuner: times every compiled variant of the plan's mode on a sample of the plan's own work and
+ * keeps the fastest (FUSED: TMA vs cp.async staging, FP64 MMA shape m16n8k8 vs m16n8k4, CTAs per SM;
+ * EMULATED: triples per launch pair, 4 / 8 / 16).  Needs a bound plan (after upload or bind); each
+ * system is sampled (about 1/8 of its fused items, 64 triples in the emulated form) and the per-
+ * system times are scaled to its full work.  The choice is cached per device and set of shapes for
+ * the life of the process; a later plan with the same key takes it without timing.  No counterpart
+ * in the reference (its BLAS call sites have nothing to tune).  `result` may be NULL. */
+typedef struct trpdrv_tune_candidate {
+    int staging;          /* FUSED: 1 cp.async, 2 TMA; 0 otherwise */
+    int mma_k;            /* FUSED cp.async MMA shape */
+    int ctas_per_sm;      /* FUSED cp.async grid */
+    int batch;            /* EMULATED: triples per launch pair */
+    double ms_estimate;   /* estimated device time of one execution with this candidate */
+} trpdrv_tune_candidate;
+typedef struct trpdrv_tune_result {
+    int ncand, chosen, from_cache;
+    trpdrv_tune_candidate cand[8];
+} trpdrv_tune_result;
+int trpdrv_plan_autotune(trpdrv_plan *plan, trpdrv_tune_result *result);
+
 /* One call from host tensors to totals: create, upload, execute, energies, destroy. */
 int trpdrv_run(const trpdrv_system *host, int nsys, const trpdrv_options *opt,
                double *emp4, double *emp5);

@@ -164,6 +164,8 @@ static int pack_triple(int i, int j, int k) { return (i - 1) | ((j - 1) << 10) |
 /* plans                                                                                        */
 /* ------------------------------------------------------------------------------------------ */
 
+#define TUNE_MAX_BATCH 16 /* largest emulated batch the autotuner tries */
+
 typedef struct sysbuf {
     trpdrv_system shape;
     const double *t[TRPDRV_T_COUNT]; /* device tensors in use (owned or bound) */
@@ -198,7 +200,9 @@ struct trpdrv_plan {
     int64_t last_launches;
     cudaStream_t last_stream;
     int use_tma;        /* the fused launch stages panels with TMA (fused_tma.cu) */
-    double *d_fbuf;     /* emulated form: f of one batch of triples [batch][8][nvir][nvir] */
+    double *d_fbuf;     /* emulated form: f of one batch of triples [fbuf_batch][8][nvir][nvir] */
+    int fbuf_batch;     /* triples d_fbuf holds (>= opt.batch, and room for the autotuner's batches) */
+    int tuned_staging;  /* FUSED staging chosen by the autotuner (1 cp.async, 2 TMA), 0 = none */
     void *tma_maps;     /* tensor maps of every system, passed by value to each launch */
 };
 
@@ -370,8 +374,10 @@ static int plan_build(trpdrv_plan *p, const trpdrv_system *shape)
     CUDA_TRY(cudaMemset(p->d_status, 0, sizeof(int)));
     CUDA_TRY(cudaMalloc((void **)&p->d_tot, sizeof(double) * 4 * (size_t)p->nsys));
     CUDA_TRY(cudaMemset(p->d_tot, 0, sizeof(double) * 4 * (size_t)p->nsys));
-    if (o->mode == TRPDRV_MODE_EMULATED)
-        CUDA_TRY(cudaMalloc((void **)&p->d_fbuf, sizeof(double) * 8 * (size_t)o->batch * maxv * maxv));
+    if (o->mode == TRPDRV_MODE_EMULATED) {
+        p->fbuf_batch = o->batch > TUNE_MAX_BATCH ? o->batch : TUNE_MAX_BATCH;
+        CUDA_TRY(cudaMalloc((void **)&p->d_fbuf, sizeof(double) * 8 * (size_t)p->fbuf_batch * maxv * maxv));
+    }
     if (o->mode == TRPDRV_MODE_PLAIN) {
         CUDA_TRY(cudaMalloc((void **)&p->d_f, sizeof(double) * 8 * (size_t)maxv * maxv));
         CUDA_TRY(cudaMalloc((void **)&p->d_bpart, sizeof(double) * 4 * (size_t)maxpairs));
@@ -476,11 +482,12 @@ static int plan_publish(trpdrv_plan *p)
     }
     if (p->opt.mode == TRPDRV_MODE_FUSED) {
         const int want = p->opt.staging;
-        const int ok = want != 1 && trpdrv_tma_supported(p->h_dev, p->nsys);
-        if (want == 2 && !ok)
+        const int tma_ok = want != 1 && trpdrv_tma_supported(p->h_dev, p->nsys);
+        const int ok = tma_ok && p->tuned_staging != 1;
+        if (want == 2 && !tma_ok)
             return fail(TRPDRV_ERR_UNSUPPORTED, "TMA staging needs even nvir and nocc, 16-byte aligned tensors "
                                                 "and at most %d systems", TRPDRV_TMA_MAX_SYSTEMS);
-        if (ok) {
+        if (tma_ok) { /* maps whenever TMA is possible, so that the autotuner can time it */
             if (!p->tma_maps) {
                 p->tma_maps = aligned_alloc(64, (trpdrv_tma_maps_bytes() + 63) & ~(size_t)63);
                 if (!p->tma_maps) return fail(TRPDRV_ERR_NOMEM, "host allocation failed");
@@ -794,6 +801,208 @@ int trpdrv_plan_last_kernel_ms(trpdrv_plan *p, double *ms)
     float f = 0.0f;
     CUDA_TRY(cudaEventElapsedTime(&f, p->ev0, p->ev1));
     *ms = (double)f;
+    return TRPDRV_OK;
+}
+
+/* ------------------------------------------------------------------------------------------ */
+/* autotuner                                                                                    */
+/* ------------------------------------------------------------------------------------------ */
+
+typedef struct tune_entry {
+    int used, dev, mode, slices, world, rank, nsys, staging;
+    int shape[3 * TRPDRV_TMA_MAX_SYSTEMS];
+    trpdrv_tune_candidate best;
+} tune_entry;
+
+static tune_entry g_tune[64];
+static pthread_mutex_t g_tune_mu = PTHREAD_MUTEX_INITIALIZER;
+
+static void tune_key(const trpdrv_plan *p, tune_entry *k)
+{
+    memset(k, 0, sizeof *k);
+    k->dev = p->device;
+    k->mode = p->opt.mode;
+    k->slices = p->opt.mode == TRPDRV_MODE_EMULATED ? p->opt.slices : 0;
+    k->world = p->opt.world;
+    k->rank = p->opt.rank;
+    k->nsys = p->nsys;
+    k->staging = p->opt.staging; /* a forced staging limits the candidates */
+    for (int q = 0; q < p->nsys && q < TRPDRV_TMA_MAX_SYSTEMS; ++q) {
+        k->shape[3 * q] = p->s[q].shape.nocc;
+        k->shape[3 * q + 1] = p->s[q].shape.nvir;
+        k->shape[3 * q + 2] = p->opt.nkpass;
+    }
+}
+
+static int tune_same(const tune_entry *a, const tune_entry *b)
+{
+    return a->dev == b->dev && a->mode == b->mode && a->slices == b->slices && a->world == b->world &&
+           a->rank == b->rank && a->nsys == b->nsys && a->staging == b->staging && memcmp(a->shape, b->shape, sizeof a->shape) == 0;
+}
+
+/* sets the plan's launch configuration to candidate c */
+static void tune_apply(trpdrv_plan *p, const trpdrv_tune_candidate *c)
+{
+    if (p->opt.mode == TRPDRV_MODE_FUSED) {
+        p->use_tma = c->staging == 2;
+        p->tuned_staging = c->staging; /* a later upload/bind keeps it where TMA remains possible */
+        if (c->staging == 1) {
+            p->opt.mma_k = c->mma_k;
+            p->opt.ctas_per_sm = c->ctas_per_sm;
+            int64_t grid = (int64_t)c->ctas_per_sm * p->nsm;
+            if (grid > p->total_items) grid = p->total_items;
+            p->grid = (int)(grid > 0 ? grid : 0);
+        }
+    } else if (p->opt.mode == TRPDRV_MODE_EMULATED) {
+        p->opt.batch = c->batch;
+    }
+    if (p->graph_ready) {
+        cudaGraphExecDestroy(p->gexec);
+        cudaGraphDestroy(p->graph);
+        p->gexec = NULL;
+        p->graph = NULL;
+        p->graph_ready = 0;
+    }
+}
+
+static int tune_elapsed(trpdrv_plan *p, float *ms)
+{
+    CUDA_TRY(cudaEventSynchronize(p->ev1));
+    CUDA_TRY(cudaEventElapsedTime(ms, p->ev0, p->ev1));
+    return TRPDRV_OK;
+}
+
+/* estimated device time of one execution with candidate c: each system timed on a sample (after one
+ * untimed run of the same sample) and scaled to its full work */
+static int tune_time(trpdrv_plan *p, const trpdrv_tune_candidate *c, double *est)
+{
+    cudaStream_t st = p->stream;
+    *est = 0.0;
+    for (int q = 0; q < p->nsys; ++q) {
+        const trpdrv_dev_system *d = &p->h_dev[q];
+        if (d->ntriples <= 0) continue;
+        float ms = 0.0f;
+        if (p->opt.mode == TRPDRV_MODE_FUSED) {
+            const int64_t items = d->ntriples * d->npairs;
+            int64_t sample = items / 8;
+            if (sample < (int64_t)p->nsm * 64) sample = (int64_t)p->nsm * 64;
+            if (sample > items) sample = items;
+            const unsigned long long first = (unsigned long long)d->item_begin;
+            int grid = c->staging == 2 ? p->nsm : c->ctas_per_sm * p->nsm;
+            if (grid > sample) grid = (int)sample;
+            for (int rep = 0; rep < 2; ++rep) {
+                CUDA_TRY(cudaMemcpyAsync(p->d_counter, &first, sizeof first, cudaMemcpyHostToDevice, st));
+                CUDA_TRY(cudaStreamSynchronize(st)); /* `first` is a host stack value */
+                CUDA_TRY(cudaEventRecord(p->ev0, st));
+                if (c->staging == 2)
+                    LAUNCH_TRY(trpdrv_launch_fused_tma(p->d_dev, p->nsys, d->item_begin + sample, p->d_counter,
+                                                       p->d_status, grid, p->tma_maps, st));
+                else
+                    LAUNCH_TRY(trpdrv_launch_fused(p->d_dev, p->nsys, d->item_begin + sample, p->d_counter,
+                                                   p->d_status, grid, p->vec2, c->mma_k, st));
+                CUDA_TRY(cudaEventRecord(p->ev1, st));
+                TRY(tune_elapsed(p, &ms));
+            }
+            *est += (double)ms * (double)items / (double)sample;
+        } else {
+            const sysbuf *b = &p->s[q];
+            const int64_t n = d->ntriples < 64 ? d->ntriples : 64;
+            LAUNCH_TRY(trpdrv_launch_oz_slices(d, &b->oz, st));
+            for (int rep = 0; rep < 2; ++rep) {
+                CUDA_TRY(cudaEventRecord(p->ev0, st));
+                for (int64_t pos = 0; pos < n; pos += c->batch) {
+                    const int m = (int)(n - pos < c->batch ? n - pos : c->batch);
+                    LAUNCH_TRY(trpdrv_launch_oz_gemm(d, &b->oz, b->oz_maps, pos, m, p->d_fbuf, p->d_status, p->nsm, st));
+                    LAUNCH_TRY(trpdrv_launch_oz_tengy(d, pos, m, p->d_fbuf, st));
+                }
+                CUDA_TRY(cudaEventRecord(p->ev1, st));
+                TRY(tune_elapsed(p, &ms));
+            }
+            *est += (double)ms * (double)d->ntriples / (double)n;
+        }
+    }
+    return TRPDRV_OK;
+}
+
+int trpdrv_plan_autotune(trpdrv_plan *p, trpdrv_tune_result *result)
+{
+    trpdrv_tune_result local;
+    trpdrv_tune_result *r = result ? result : &local;
+    memset(r, 0, sizeof *r);
+    if (!p) return fail(TRPDRV_ERR_ARG, "NULL plan");
+    if (!p->bound) return fail(TRPDRV_ERR_STATE, "autotune before upload/bind");
+    if (p->opt.mode == TRPDRV_MODE_PLAIN) return TRPDRV_OK; /* one compiled form: nothing to choose */
+    CUDA_TRY(cudaSetDevice(p->device));
+    p->events_valid = 0; /* the timing below reuses the plan's events */
+
+    tune_entry key;
+    tune_key(p, &key);
+    const int cacheable = p->nsys <= TRPDRV_TMA_MAX_SYSTEMS;
+    if (cacheable) {
+        pthread_mutex_lock(&g_tune_mu);
+        int hit = -1;
+        for (int e = 0; e < (int)(sizeof g_tune / sizeof g_tune[0]); ++e)
+            if (g_tune[e].used && tune_same(&g_tune[e], &key)) hit = e;
+        trpdrv_tune_candidate best;
+        memset(&best, 0, sizeof best);
+        if (hit >= 0) best = g_tune[hit].best;
+        pthread_mutex_unlock(&g_tune_mu);
+        /* a cached TMA choice applies only where this plan can stage with TMA */
+        if (hit >= 0 && best.staging == 2 && !(p->tma_maps && trpdrv_tma_supported(p->h_dev, p->nsys))) hit = -1;
+        if (hit >= 0) {
+            r->ncand = 1;
+            r->chosen = 0;
+            r->from_cache = 1;
+            r->cand[0] = best;
+            tune_apply(p, &best);
+            return TRPDRV_OK;
+        }
+    }
+
+    /* candidates */
+    trpdrv_tune_candidate *c = r->cand;
+    int n = 0;
+    if (p->opt.mode == TRPDRV_MODE_FUSED) {
+        int occ = 1;
+        if (trpdrv_fused_max_ctas_per_sm(&occ) != 0 || occ < 1) occ = 1;
+        if (p->opt.staging != 1 && trpdrv_tma_supported(p->h_dev, p->nsys) && p->tma_maps) {
+            c[n++] = (trpdrv_tune_candidate){2, 0, 1, 0, 0.0};
+        }
+        if (p->opt.staging != 2) {
+            c[n++] = (trpdrv_tune_candidate){1, 8, occ, 0, 0.0};
+            c[n++] = (trpdrv_tune_candidate){1, 4, occ, 0, 0.0};
+            if (occ > 1) c[n++] = (trpdrv_tune_candidate){1, 8, 1, 0, 0.0};
+        }
+    } else {
+        static const int batches[3] = {4, 8, 16};
+        for (int k = 0; k < 3; ++k)
+            if (batches[k] <= p->fbuf_batch) c[n++] = (trpdrv_tune_candidate){0, 0, 0, batches[k], 0.0};
+    }
+    r->ncand = n;
+    if (n == 0) return TRPDRV_OK;
+
+    CUDA_TRY(cudaMemsetAsync(p->d_status, 0, sizeof(int), p->stream));
+    int best = 0;
+    for (int k = 0; k < n; ++k) {
+        TRY(tune_time(p, &c[k], &c[k].ms_estimate));
+        if (c[k].ms_estimate < c[best].ms_estimate) best = k;
+    }
+    int status = 0;
+    CUDA_TRY(cudaMemcpy(&status, p->d_status, sizeof(int), cudaMemcpyDeviceToHost));
+    if (status) return fail(TRPDRV_ERR_DEVICE, "a device kernel reported status %d while autotuning", status);
+    r->chosen = best;
+    tune_apply(p, &c[best]);
+    if (cacheable) {
+        pthread_mutex_lock(&g_tune_mu);
+        int slot = -1;
+        for (int e = 0; e < (int)(sizeof g_tune / sizeof g_tune[0]) && slot < 0; ++e)
+            if (!g_tune[e].used) slot = e;
+        if (slot < 0) slot = 0; /* full: overwrite the oldest slot */
+        g_tune[slot] = key;
+        g_tune[slot].used = 1;
+        g_tune[slot].best = c[best];
+        pthread_mutex_unlock(&g_tune_mu);
+    }
     return TRPDRV_OK;
 }
 

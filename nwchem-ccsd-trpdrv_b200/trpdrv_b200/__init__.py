@@ -96,6 +96,18 @@ _proto("trpdrv_plan_triples", C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_int32
 _proto("trpdrv_plan_triple_energies", C.c_int, [C.c_void_p, C.c_int, _dp])
 _proto("trpdrv_plan_last_launches", C.c_int64, [C.c_void_p])
 _proto("trpdrv_plan_staging", C.c_int, [C.c_void_p])
+
+
+class TuneCandidate(C.Structure):
+    _fields_ = [("staging", C.c_int), ("mma_k", C.c_int), ("ctas_per_sm", C.c_int), ("batch", C.c_int),
+                ("ms_estimate", C.c_double)]
+
+
+class TuneResult(C.Structure):
+    _fields_ = [("ncand", C.c_int), ("chosen", C.c_int), ("from_cache", C.c_int), ("cand", TuneCandidate * 8)]
+
+
+_proto("trpdrv_plan_autotune", C.c_int, [C.c_void_p, C.POINTER(TuneResult)])
 _proto("trpdrv_plan_last_kernel_ms", C.c_int, [C.c_void_p, _dp])
 _proto("trpdrv_plan_destroy", C.c_int, [C.c_void_p])
 _proto("trpdrv_run", C.c_int, [C.POINTER(SystemStruct), C.c_int, C.POINTER(OptionsStruct), _dp, _dp])
@@ -368,6 +380,15 @@ class Plan:
         out = np.zeros((max(n, 1), 4))
         _check(lib.trpdrv_plan_triple_energies(self.h, sys, out.ctypes.data_as(_dp)))
         return out[:n]
+
+    def autotune(self) -> dict:
+        """trpdrv_plan_autotune: times the compiled variants on a sample of this plan's work and keeps the
+        fastest.  Returns {"candidates": [...], "chosen": i, "from_cache": bool}."""
+        r = TuneResult()
+        _check(lib.trpdrv_plan_autotune(self.h, C.byref(r)))
+        cands = [{"staging": c.staging, "mma_k": c.mma_k, "ctas_per_sm": c.ctas_per_sm, "batch": c.batch,
+                  "ms_estimate": c.ms_estimate} for c in r.cand[:r.ncand]]
+        return {"candidates": cands, "chosen": r.chosen, "from_cache": bool(r.from_cache)}
 
     def staging(self) -> int:
         """1 = cp.async, 2 = TMA staging in the fused kernel (0 for plain plans)."""

@@ -134,3 +134,10 @@ def test_processing_order_rejects_bad_arguments(T):
     assert T.lib.trpdrv_processing_order(None, 3, 0, None) == -1
     assert T.lib.trpdrv_processing_order(None, -1, 0, None) == -1
     assert len(T.processing_order(np.zeros((0, 3), np.int32))) == 0
+
+
+def test_autotune_rejects_a_null_plan(T):
+    import ctypes as C
+    r = T.TuneResult()
+    assert T.lib.trpdrv_plan_autotune(None, C.byref(r)) == 1
+    assert r.ncand == 0

@@ -178,7 +178,12 @@ typedef struct trpdrv_options {
                          or fail with TRPDRV_ERR_UNSUPPORTED */
     int slices;       /* EMULATED: base-128 digits per operand element, 4..8; 0 = default (7) */
     int batch;        /* EMULATED: triples whose f share one device buffer per launch pair; 0 = default (8) */
-    int reserved[4];
+    int a_count;      /* full (T) sweep: every system covers the virtual indices a .. a + a_count - 1 (1-based,
+                         all within the basis).  The a-dependent tensors (trpdrv_tensor_a_dependent: jvv,
+                         kvv, dintc, dintx, t1v) then hold a_count consecutive blocks, a-major; the others
+                         are shared.  Energies sum over every (a, i, j, k); per-triple records are
+                         [a][triple].  0 or 1 = the single `a` of the reference driver (default). */
+    int reserved[3];
 } trpdrv_options;
 
 void trpdrv_options_default(trpdrv_options *opt);
@@ -271,6 +276,9 @@ enum { TRPDRV_T_EORB = 0, TRPDRV_T_T2, TRPDRV_T_JVV, TRPDRV_T_KVV, TRPDRV_T_TOV,
        TRPDRV_T_JOV, TRPDRV_T_KOV, TRPDRV_T_DINTC, TRPDRV_T_DINTX, TRPDRV_T_T1V, TRPDRV_T_COUNT };
 enum { TRPDRV_DIST_UNIFORM = 0, TRPDRV_DIST_LOGUNIFORM = 1 };
 size_t trpdrv_tensor_elems(int tensor, int ncor, int nocc, int nvir);
+/* 1 if the tensor carries the virtual index a in a sweep (options.a_count > 1: a_count blocks of
+ * trpdrv_tensor_elems each), else 0.  No counterpart in the reference (its driver fixes a). */
+int trpdrv_tensor_a_dependent(int tensor);
 int trpdrv_synth_fill(int tensor, int ncor, int nocc, int nvir, uint64_t seed, int dist,
                       double *out, size_t n);
 

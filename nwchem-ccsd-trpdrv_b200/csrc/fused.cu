@@ -186,10 +186,12 @@ __device__ __forceinline__ void prepare_item(const trpdrv_dev_system *__restrict
     while (s + 1 < nsys && item >= sys[s + 1].item_begin) ++s;
     const trpdrv_dev_system &S = sys[s];
     const long long local = item - S.item_begin;
-    const long long qpos = local / S.npairs;  // processing order; energies go to the triple's own items
+    const long long qpos = local / S.npairs;  // processing position over the system's records
     const int p = (int)(local - qpos * S.npairs);
-    const long long tt = (S.order && local >= 0 && qpos < S.ntriples) ? (long long)S.order[qpos] : qpos;
-    const long long own = tt * S.npairs + p;
+    const long long ai = S.nt > 0 ? qpos / S.nt : 0;  // a index: records are [a][triple]
+    const long long tpos = qpos - ai * S.nt;
+    const long long tt = (S.order && local >= 0 && qpos < S.ntriples) ? (long long)S.order[tpos] : tpos;
+    const long long own = (ai * S.nt + tt) * S.npairs + p;  // energies go to the record's own items
     int B = 0, rem = p;
     while (B < S.nb && rem >= S.nb - B) {
         rem -= S.nb - B;
@@ -197,7 +199,7 @@ __device__ __forceinline__ void prepare_item(const trpdrv_dev_system *__restrict
     }
     const int C = B + rem;
     const int O = S.nocc, V = S.nvir;
-    const bool in_range = local >= 0 && qpos < S.ntriples && tt >= 0 && tt < S.ntriples;
+    const bool in_range = local >= 0 && qpos < S.ntriples && tt >= 0 && tt < S.nt && ai < S.n_a;
     const int packed = in_range ? S.triples[tt] : 0;
     const int i = packed & 1023, j = (packed >> 10) & 1023, k = (packed >> 20) & 1023;
     const bool ok = in_range && B < S.nb && C < S.nb && i < O && j < O && k < O && k <= i;
@@ -211,19 +213,19 @@ __device__ __forceinline__ void prepare_item(const trpdrv_dev_system *__restrict
         return;
     }
     const size_t lnvv = (size_t)V * V, lnov = (size_t)O * V;
-    const size_t jo = (size_t)j * O;
+    const size_t jo = (size_t)j * O, ao = (size_t)ai * O;  // ao: the a block of J, K and the vectors
     const int B0 = B * T, C0 = C * T;
     {
         const int ph = lane >> 4, pnl = lane & 15, fam = pnl >> 3, q = pnl & 7;
         const double *Aj, *Ak, *B1, *B3;
         if (fam == 0) {
-            Aj = ph ? S.ntov + (size_t)i * lnov : S.jvv + (size_t)i * lnvv;
-            Ak = ph ? S.nxov + (size_t)i * lnov : S.kvv + (size_t)i * lnvv;
+            Aj = ph ? S.ntov + (size_t)i * lnov : S.jvv + (ao + i) * lnvv;
+            Ak = ph ? S.nxov + (size_t)i * lnov : S.kvv + (ao + i) * lnvv;
             B1 = ph ? S.kov + (jo + k) * lnov : S.t2 + (jo + k) * lnvv;
             B3 = ph ? S.jov + (jo + k) * lnov : S.t2 + (jo + k) * lnvv;
         } else {
-            Aj = ph ? S.ntov + (size_t)k * lnov : S.jvv + (size_t)k * lnvv;
-            Ak = ph ? S.nxov + (size_t)k * lnov : S.kvv + (size_t)k * lnvv;
+            Aj = ph ? S.ntov + (size_t)k * lnov : S.jvv + (ao + k) * lnvv;
+            Ak = ph ? S.nxov + (size_t)k * lnov : S.kvv + (ao + k) * lnvv;
             B1 = ph ? S.kov + (jo + i) * lnov : S.t2 + (jo + i) * lnvv;
             B3 = ph ? S.jov + (jo + i) * lnov : S.t2 + (jo + i) * lnvv;
         }
@@ -258,15 +260,15 @@ __device__ __forceinline__ void prepare_item(const trpdrv_dev_system *__restrict
     }
     if (lane == 0) {
         cx.eorb = S.eorb;
-        cx.dintc1 = S.dintc + (size_t)i * V;
-        cx.dintx1 = S.dintx + (size_t)i * V;
-        cx.t1v1 = S.t1v + (size_t)i * V;
-        cx.dintc2 = S.dintc + (size_t)k * V;
-        cx.dintx2 = S.dintx + (size_t)k * V;
-        cx.t1v2 = S.t1v + (size_t)k * V;
+        cx.dintc1 = S.dintc + (ao + i) * V;
+        cx.dintx1 = S.dintx + (ao + i) * V;
+        cx.t1v1 = S.t1v + (ao + i) * V;
+        cx.dintc2 = S.dintc + (ao + k) * V;
+        cx.dintx2 = S.dintx + (ao + k) * V;
+        cx.t1v2 = S.t1v + (ao + k) * V;
         cx.out = S.partial + (size_t)own * NWARP * 4;
         // omp/ccsd_trpdrv_omp_cbody.c:126 (a is 1-based, i/j/k here 0-based)
-        cx.eaijk = S.eorb[S.a - 1] - (S.eorb[S.ncor + i] + S.eorb[S.ncor + j] + S.eorb[S.ncor + k]);
+        cx.eaijk = S.eorb[S.a - 1 + ai] - (S.eorb[S.ncor + i] + S.eorb[S.ncor + j] + S.eorb[S.ncor + k]);
         cx.ncor = S.ncor;
         cx.nocc = O;
         cx.nvir = V;

@@ -288,10 +288,12 @@ __device__ __forceinline__ void producer(const trpdrv_dev_system *__restrict__ s
         while (s + 1 < nsys && item >= sys[s + 1].item_begin) ++s;
         const trpdrv_dev_system &S = sys[s];
         const long long local = item - S.item_begin;
-        const long long qpos = local / S.npairs;  // processing order; energies go to the triple's own items
+        const long long qpos = local / S.npairs;  // processing position over the system's records
         const int p = (int)(local - qpos * S.npairs);
-        const long long tt = (S.order && local >= 0 && qpos < S.ntriples) ? (long long)S.order[qpos] : qpos;
-        const long long own = tt * S.npairs + p;
+        const long long ai = S.nt > 0 ? qpos / S.nt : 0;  // a index: records are [a][triple]
+        const long long tpos = qpos - ai * S.nt;
+        const long long tt = (S.order && local >= 0 && qpos < S.ntriples) ? (long long)S.order[tpos] : tpos;
+        const long long own = (ai * S.nt + tt) * S.npairs + p;  // energies go to the record's own items
         int B = 0, rem = p;
         while (B < S.nb && rem >= S.nb - B) {
             rem -= S.nb - B;
@@ -299,7 +301,7 @@ __device__ __forceinline__ void producer(const trpdrv_dev_system *__restrict__ s
         }
         const int C = B + rem;
         const int O = S.nocc, V = S.nvir;
-        const bool in_range = local >= 0 && qpos < S.ntriples && tt >= 0 && tt < S.ntriples;
+        const bool in_range = local >= 0 && qpos < S.ntriples && tt >= 0 && tt < S.nt && ai < S.n_a;
         const int packed = in_range ? S.triples[tt] : 0;
         const int i = packed & 1023, j = (packed >> 10) & 1023, k = (packed >> 20) & 1023;
         const bool ok = in_range && B < S.nb && C < S.nb && i < O && j < O && k < O && k <= i && s < TRPDRV_TMA_MAX_SYSTEMS;
@@ -323,15 +325,16 @@ __device__ __forceinline__ void producer(const trpdrv_dev_system *__restrict__ s
         const bool diag = (B == C);
         if (lane == 0) {
             cx.eorb = S.eorb;
-            cx.dintc1 = S.dintc + (size_t)i * V;
-            cx.dintx1 = S.dintx + (size_t)i * V;
-            cx.t1v1 = S.t1v + (size_t)i * V;
-            cx.dintc2 = S.dintc + (size_t)k * V;
-            cx.dintx2 = S.dintx + (size_t)k * V;
-            cx.t1v2 = S.t1v + (size_t)k * V;
+            const size_t ao = (size_t)ai * O;  // the a block of the a-dependent vectors
+            cx.dintc1 = S.dintc + (ao + i) * V;
+            cx.dintx1 = S.dintx + (ao + i) * V;
+            cx.t1v1 = S.t1v + (ao + i) * V;
+            cx.dintc2 = S.dintc + (ao + k) * V;
+            cx.dintx2 = S.dintx + (ao + k) * V;
+            cx.t1v2 = S.t1v + (ao + k) * V;
             cx.out = S.partial + (size_t)own * NCW * 4;
             // omp/ccsd_trpdrv_omp_cbody.c:126 (a is 1-based, i/j/k here 0-based)
-            cx.eaijk = S.eorb[S.a - 1] - (S.eorb[S.ncor + i] + S.eorb[S.ncor + j] + S.eorb[S.ncor + k]);
+            cx.eaijk = S.eorb[S.a - 1 + ai] - (S.eorb[S.ncor + i] + S.eorb[S.ncor + j] + S.eorb[S.ncor + k]);
             cx.ncor = S.ncor;
             cx.nocc = O;
             cx.nvir = V;
@@ -346,6 +349,7 @@ __device__ __forceinline__ void producer(const trpdrv_dev_system *__restrict__ s
         // per-lane box: A_J (slots 0,1), A_K (2,3) rows; B_1 (4,5) and B_3 (6) columns
         const CUtensorMap *mp = maps.m[s];
         const int za = fam ? k : i;                      // A operands: Jia/Kia (n), Jka/Kka (t)
+        const int zaj = za + (int)ai * O;                // J/K carry the a index, -T/-X do not
         const int zb = fam ? j * O + i : j * O + k;      // B operands: Tkj/Kkj/Jkj (n), Tij/Kij/Jij (t)
         const int ra = o ? C0 : B0;                      // A rows: B for (B,C), C for (C,B)
         const int cb = o ? B0 : C0;                      // B columns: C for (B,C), B for (C,B)
@@ -363,7 +367,7 @@ __device__ __forceinline__ void producer(const trpdrv_dev_system *__restrict__ s
             if (mine) {
                 if (slot < 4) {  // A rows, K-major (J/K in the virtual phase, -T/-X in the occupied one)
                     const CUtensorMap *m = &mp[slot < 2 ? (ph1 ? M_NT : M_J) : (ph1 ? M_NX : M_K)];
-                    tma_load_3d(dst + half * KBOX, m, &full[stage], ra + 16 * half, kk0, za);
+                    tma_load_3d(dst + half * KBOX, m, &full[stage], ra + 16 * half, kk0, ph1 ? za : zaj);
                 } else if (slot < 6) {  // B_1 columns: T(c,d) K-major, or K(m,c) X-major (one box)
                     if (!ph1)
                         tma_load_3d(dst + half * KBOX, &mp[M_T2K], &full[stage], cb + 16 * half, kk0, zb);
@@ -592,8 +596,9 @@ extern "C" int trpdrv_tma_prepare(const trpdrv_dev_system *h_sys, int nsys, void
         const unsigned long long V = S.nvir, O = S.nocc, O2 = O * O;
         CUtensorMap *m = M->m[s];
         int e = 0;
-        e |= tma::make_map(&m[tma::M_J], S.jvv, V, V, O, 16, tma::DK, true);    // [i][d][b]
-        e |= tma::make_map(&m[tma::M_K], S.kvv, V, V, O, 16, tma::DK, true);
+        const unsigned long long OA = O * (unsigned long long)(S.n_a > 0 ? S.n_a : 1);
+        e |= tma::make_map(&m[tma::M_J], S.jvv, V, V, OA, 16, tma::DK, true);    // [a][i][d][b]
+        e |= tma::make_map(&m[tma::M_K], S.kvv, V, V, OA, 16, tma::DK, true);
         e |= tma::make_map(&m[tma::M_NT], S.ntov, V, O, O, 16, tma::DK, true);  // [i][m][b]
         e |= tma::make_map(&m[tma::M_NX], S.nxov, V, O, O, 16, tma::DK, true);
         e |= tma::make_map(&m[tma::M_T2K], S.t2, V, V, O2, 16, tma::DK, true);  // [jx][d][c]: T(c,d)

@@ -175,7 +175,9 @@ typedef struct sysbuf {
     int32_t *d_order;                /* fused/emulated processing order (trpdrv_processing_order) */
     trpdrv_oz_system oz;             /* emulated form: digit slices and scales (device) */
     void *oz_maps;                   /* emulated form: tensor maps of oz.sa / oz.sb (host blob) */
-    int64_t ntriples;
+    int64_t ntriples;                /* records: n_a * nt */
+    int64_t nt;                      /* triples per a (this rank's share) */
+    int n_a;                         /* virtual indices swept (options.a_count) */
     double *partial, *rec;
     int nb, npairs;
 } sysbuf;
@@ -290,7 +292,9 @@ static int plan_build(trpdrv_plan *p, const trpdrv_system *shape)
         /* the reference driver's order, then this rank's contiguous share (uniform cost per system) */
         const int64_t n = trpdrv_shard_triples(nocc, o->nkpass, o->rank, o->world, NULL);
         if (n < 0) return fail(TRPDRV_ERR_ARG, "system %d: cannot shard triples", q);
-        b->ntriples = n;
+        b->nt = n;
+        b->n_a = o->a_count;
+        b->ntriples = n * o->a_count;
         int32_t *ijk = (int32_t *)malloc(sizeof(int32_t) * 3 * (size_t)(n > 0 ? n : 1));
         b->h_triples = (int32_t *)malloc(sizeof(int32_t) * (size_t)(n > 0 ? n : 1));
         if (!ijk || !b->h_triples) {
@@ -319,8 +323,8 @@ static int plan_build(trpdrv_plan *p, const trpdrv_system *shape)
         }
 
         if (b->ntriples > 0) {
-            CUDA_TRY(cudaMalloc((void **)&b->d_triples, sizeof(int32_t) * (size_t)b->ntriples));
-            CUDA_TRY(cudaMemcpy(b->d_triples, b->h_triples, sizeof(int32_t) * (size_t)b->ntriples,
+            CUDA_TRY(cudaMalloc((void **)&b->d_triples, sizeof(int32_t) * (size_t)b->nt));
+            CUDA_TRY(cudaMemcpy(b->d_triples, b->h_triples, sizeof(int32_t) * (size_t)b->nt,
                                 cudaMemcpyHostToDevice));
             CUDA_TRY(cudaMalloc((void **)&b->rec, sizeof(double) * 4 * (size_t)b->ntriples));
             CUDA_TRY(cudaMemset(b->rec, 0, sizeof(double) * 4 * (size_t)b->ntriples));
@@ -338,10 +342,11 @@ static int plan_build(trpdrv_plan *p, const trpdrv_system *shape)
             z->nvir = nvir;
             z->slices = o->slices;
             z->dp = trpdrv_oz_dp(nocc, nvir);
+            z->n_a = o->a_count;
             const size_t rows = 2 * (size_t)nvir, per = (size_t)o->slices * rows * (size_t)z->dp;
-            CUDA_TRY(cudaMalloc((void **)&z->sa, per * (size_t)nocc));
+            CUDA_TRY(cudaMalloc((void **)&z->sa, per * (size_t)nocc * (size_t)z->n_a));
             CUDA_TRY(cudaMalloc((void **)&z->sb, per * (size_t)nocc * nocc));
-            CUDA_TRY(cudaMalloc((void **)&z->ea, sizeof(double) * rows * (size_t)nocc));
+            CUDA_TRY(cudaMalloc((void **)&z->ea, sizeof(double) * rows * (size_t)nocc * (size_t)z->n_a));
             CUDA_TRY(cudaMalloc((void **)&z->eb, sizeof(double) * rows * (size_t)nocc * nocc));
             b->oz_maps = aligned_alloc(64, (trpdrv_oz_maps_bytes() + 63) & ~(size_t)63);
             if (!b->oz_maps) return fail(TRPDRV_ERR_NOMEM, "host allocation failed");
@@ -357,6 +362,8 @@ static int plan_build(trpdrv_plan *p, const trpdrv_system *shape)
         d->nb = b->nb;
         d->npairs = b->npairs;
         d->ntriples = b->ntriples;
+        d->nt = b->nt;
+        d->n_a = b->n_a;
         d->item_begin = item;
         d->triples = b->d_triples;
         d->order = b->d_order;
@@ -417,6 +424,8 @@ int trpdrv_plan_create(trpdrv_plan **plan, const trpdrv_system *shape, int nsys,
     if (!trpdrv_oz_slices_supported(o.slices))
         return fail(TRPDRV_ERR_ARG, "slices %d: must be %d..%d", o.slices, TRPDRV_OZ_MIN_SLICES, TRPDRV_OZ_MAX_SLICES);
     if (o.batch < 1 || o.batch > 4096) return fail(TRPDRV_ERR_ARG, "batch %d: must be 1..4096", o.batch);
+    if (o.a_count == 0) o.a_count = 1;
+    if (o.a_count < 1 || o.a_count > 1023) return fail(TRPDRV_ERR_ARG, "a_count %d: must be 1..1023", o.a_count);
     if (o.world < 1 || o.rank < 0 || o.rank >= o.world)
         return fail(TRPDRV_ERR_ARG, "rank %d / world %d", o.rank, o.world);
     if (o.tile != 0 && o.tile != TRPDRV_TILE)
@@ -425,7 +434,13 @@ int trpdrv_plan_create(trpdrv_plan **plan, const trpdrv_system *shape, int nsys,
     if (o.mma_k == 0) o.mma_k = 8;
     if (o.mma_k != 4 && o.mma_k != 8) return fail(TRPDRV_ERR_ARG, "mma_k %d: must be 4 or 8", o.mma_k);
     if (o.staging < 0 || o.staging > 2) return fail(TRPDRV_ERR_ARG, "staging %d: must be 0, 1 or 2", o.staging);
-    for (int q = 0; q < nsys; ++q) TRY(check_shape(&shape[q], q));
+    for (int q = 0; q < nsys; ++q) {
+        TRY(check_shape(&shape[q], q));
+        const int nbf = shape[q].ncor + shape[q].nocc + shape[q].nvir;
+        if (shape[q].a + o.a_count - 1 > nbf)
+            return fail(TRPDRV_ERR_ARG, "system %d: a=%d with a_count=%d passes the basis size %d", q, shape[q].a,
+                        o.a_count, nbf);
+    }
 
     int dev = 0, nsm = 0;
     TRY(ensure_device(o.device, &dev, &nsm));
@@ -517,7 +532,8 @@ int trpdrv_plan_upload(trpdrv_plan *p, const trpdrv_system *host, void *stream)
         for (int w = 0; w < TRPDRV_T_COUNT; ++w) {
             const double *src = sys_tensor(h, w);
             if (!src) return fail(TRPDRV_ERR_ARG, "system %d: tensor %d is NULL", q, w);
-            const size_t n = trpdrv_tensor_elems(w, b->shape.ncor, b->shape.nocc, b->shape.nvir);
+            const size_t n = trpdrv_tensor_elems(w, b->shape.ncor, b->shape.nocc, b->shape.nvir) *
+                             (trpdrv_tensor_a_dependent(w) ? (size_t)b->n_a : 1);
             if (!b->own[w]) CUDA_TRY(cudaMalloc((void **)&b->own[w], sizeof(double) * n));
             CUDA_TRY(cudaMemcpyAsync(b->own[w], src, sizeof(double) * n, cudaMemcpyHostToDevice, st));
             b->t[w] = b->own[w];
@@ -575,7 +591,7 @@ static int enqueue_fused(trpdrv_plan *p, cudaStream_t st, int capturing)
     for (int q = 0; q < p->nsys; ++q) {
         if (p->h_dev[q].ntriples <= 0) continue;
         LAUNCH_TRY(trpdrv_launch_item_reduce(&p->h_dev[q], st));
-        LAUNCH_TRY(trpdrv_launch_system_reduce(p->s[q].rec, p->s[q].d_triples, p->s[q].ntriples, p->d_tot + 4 * q, st));
+        LAUNCH_TRY(trpdrv_launch_system_reduce(p->s[q].rec, p->s[q].d_triples, p->s[q].ntriples, p->s[q].nt, p->d_tot + 4 * q, st));
         launches += 2;
     }
     p->last_launches = launches;
@@ -607,7 +623,7 @@ static int enqueue_emulated(trpdrv_plan *p, cudaStream_t st, int capturing)
     for (int q = 0; q < p->nsys; ++q) {
         if (p->h_dev[q].ntriples <= 0) continue;
         LAUNCH_TRY(trpdrv_launch_item_reduce(&p->h_dev[q], st));
-        LAUNCH_TRY(trpdrv_launch_system_reduce(p->s[q].rec, p->s[q].d_triples, p->s[q].ntriples, p->d_tot + 4 * q, st));
+        LAUNCH_TRY(trpdrv_launch_system_reduce(p->s[q].rec, p->s[q].d_triples, p->s[q].ntriples, p->s[q].nt, p->d_tot + 4 * q, st));
         launches += 2;
     }
     p->last_launches = launches;
@@ -644,12 +660,13 @@ static int enqueue_plain(trpdrv_plan *p, cudaStream_t st)
         ta.eorb = b->t[TRPDRV_T_EORB];
         ta.block_partial = p->d_bpart;
         ta.counter = p->d_tcount;
-        for (int64_t t = 0; t < b->ntriples; ++t) {
+        for (int64_t r = 0; r < b->ntriples; ++r) {
+            const int64_t ai = r / b->nt, t = r - ai * b->nt; /* records are [a][triple] */
             const int pk = b->h_triples[t];
             const int i = pk & 1023, j = (pk >> 10) & 1023, k = (pk >> 20) & 1023; /* 0-based */
-            const size_t jo = (size_t)j * O;
-            const double *jia = b->t[TRPDRV_T_JVV] + i * lnvv, *kia = b->t[TRPDRV_T_KVV] + i * lnvv;
-            const double *jka = b->t[TRPDRV_T_JVV] + k * lnvv, *kka = b->t[TRPDRV_T_KVV] + k * lnvv;
+            const size_t jo = (size_t)j * O, ao = (size_t)ai * O;
+            const double *jia = b->t[TRPDRV_T_JVV] + (ao + i) * lnvv, *kia = b->t[TRPDRV_T_KVV] + (ao + i) * lnvv;
+            const double *jka = b->t[TRPDRV_T_JVV] + (ao + k) * lnvv, *kka = b->t[TRPDRV_T_KVV] + (ao + k) * lnvv;
             const double *tij = b->t[TRPDRV_T_T2] + (jo + i) * lnvv, *tkj = b->t[TRPDRV_T_T2] + (jo + k) * lnvv;
             const double *ntia = b->ntov + i * lnov, *nxia = b->nxov + i * lnov;
             const double *ntka = b->ntov + k * lnov, *nxka = b->nxov + k * lnov;
@@ -669,16 +686,17 @@ static int enqueue_plain(trpdrv_plan *p, cudaStream_t st)
                 ga.b2[x] = b2[x];
             }
             LAUNCH_TRY(trpdrv_launch_plain_gemm(&ga, p->vec2, st));
+            ta.a = b->shape.a + (int)ai;
             ta.i = i + 1;
             ta.j = j + 1;
             ta.k = k + 1;
-            ta.dintc1 = b->t[TRPDRV_T_DINTC] + (size_t)i * V;
-            ta.dintx1 = b->t[TRPDRV_T_DINTX] + (size_t)i * V;
-            ta.t1v1 = b->t[TRPDRV_T_T1V] + (size_t)i * V;
-            ta.dintc2 = b->t[TRPDRV_T_DINTC] + (size_t)k * V;
-            ta.dintx2 = b->t[TRPDRV_T_DINTX] + (size_t)k * V;
-            ta.t1v2 = b->t[TRPDRV_T_T1V] + (size_t)k * V;
-            ta.out4 = b->rec + 4 * t;
+            ta.dintc1 = b->t[TRPDRV_T_DINTC] + (ao + i) * V;
+            ta.dintx1 = b->t[TRPDRV_T_DINTX] + (ao + i) * V;
+            ta.t1v1 = b->t[TRPDRV_T_T1V] + (ao + i) * V;
+            ta.dintc2 = b->t[TRPDRV_T_DINTC] + (ao + k) * V;
+            ta.dintx2 = b->t[TRPDRV_T_DINTX] + (ao + k) * V;
+            ta.t1v2 = b->t[TRPDRV_T_T1V] + (ao + k) * V;
+            ta.out4 = b->rec + 4 * r;
             LAUNCH_TRY(trpdrv_launch_tengy(&ta, st));
             launches += 2;
         }
@@ -686,7 +704,7 @@ static int enqueue_plain(trpdrv_plan *p, cudaStream_t st)
     CUDA_TRY(cudaEventRecord(p->ev1, st));
     for (int q = 0; q < p->nsys; ++q) {
         if (p->s[q].ntriples <= 0) continue;
-        LAUNCH_TRY(trpdrv_launch_system_reduce(p->s[q].rec, p->s[q].d_triples, p->s[q].ntriples, p->d_tot + 4 * q, st));
+        LAUNCH_TRY(trpdrv_launch_system_reduce(p->s[q].rec, p->s[q].d_triples, p->s[q].ntriples, p->s[q].nt, p->d_tot + 4 * q, st));
         ++launches;
     }
     p->last_launches = launches;
@@ -767,7 +785,7 @@ int trpdrv_plan_triples(const trpdrv_plan *p, int sys, int32_t *ijk)
     if (!p || sys < 0 || sys >= p->nsys || !ijk) return fail(TRPDRV_ERR_ARG, "bad plan/sys/output");
     const sysbuf *b = &p->s[sys];
     for (int64_t t = 0; t < b->ntriples; ++t) {
-        const int pk = b->h_triples[t];
+        const int pk = b->h_triples[t % b->nt]; /* records are [a][triple] */
         ijk[3 * t + 0] = (pk & 1023) + 1;
         ijk[3 * t + 1] = ((pk >> 10) & 1023) + 1;
         ijk[3 * t + 2] = ((pk >> 20) & 1023) + 1;

@@ -28,7 +28,9 @@ typedef struct trpdrv_dev_system {
     int ncor, nocc, nvir, a;
     int nb;              /* ceil(nvir / TRPDRV_TILE) */
     int npairs;          /* nb*(nb+1)/2 tile pairs (B <= C) */
-    int64_t ntriples;    /* triples of this system in the plan (this rank's share) */
+    int64_t ntriples;    /* records of this system in the plan: n_a * nt */
+    int64_t nt;          /* triples per a (this rank's share): the length of `triples` and `order` */
+    int n_a;             /* virtual indices a .. a + n_a - 1 swept (1 = the reference driver's single a) */
     int64_t item_begin;  /* first fused work item of this system */
     const double *eorb, *t2, *jvv, *kvv, *ntov, *nxov, *jov, *kov, *dintc, *dintx, *t1v;
     const int32_t *triples; /* packed triples, driver order (energies are stored in this order) */
@@ -75,7 +77,7 @@ int trpdrv_fused_tma_init(void);
 #define TRPDRV_OZ_MIN_SLICES 4
 #define TRPDRV_OZ_MAX_SLICES 8
 typedef struct trpdrv_oz_system {
-    int nocc, nvir, slices, dp;
+    int nocc, nvir, slices, dp, n_a;  /* n_a: a values swept; sa holds n_a * nocc planes */
     signed char *sa, *sb;
     double *ea, *eb;
 } trpdrv_oz_system;
@@ -95,7 +97,7 @@ int trpdrv_launch_item_reduce(const trpdrv_dev_system *h_sys, void *stream);
 
 /* Compensated per-system total over rec: out[0..3] = emp4 hi, emp4 lo, emp5 hi, emp5 lo, where the
  * total is emp4i + [i != k] emp4k summed over the triples. */
-int trpdrv_launch_system_reduce(const double *rec, const int32_t *triples, int64_t ntriples,
+int trpdrv_launch_system_reduce(const double *rec, const int32_t *triples, int64_t ntriples, int64_t nt,
                                 double *out, void *stream);
 
 /* dst[i] = -src[i]. */

@@ -72,7 +72,7 @@ struct GemmParams {
     CUtensorMap mapA, mapB;  // 64-byte aligned members first
     const double *ea, *eb;   // power-of-two scales per A row / B column
     const int32_t *triples, *order;
-    long long pos0, ntriples;
+    long long pos0, ntriples, nt;  // ntriples records = n_a * nt triples per a
     double *fbuf;            // [batch][8][V][V]
     int V, O, nks, mtiles, ntiles, tiles;  // tiles = 2 * npos * mtiles * ntiles
     int *status;
@@ -231,12 +231,13 @@ __device__ __forceinline__ Tile decode_tile(const GemmParams &P, int t)
     d.m0 = (rem % P.mtiles) * BM;
     d.n0 = (rem / P.mtiles) * BN;
     d.grp = d.y & 1;
-    const long long pos = P.pos0 + (d.y >> 1);
-    const long long tt = (pos < P.ntriples) ? (P.order ? (long long)P.order[pos] : pos) : -1;
-    const int packed = (tt >= 0 && tt < P.ntriples) ? P.triples[tt] : -1;
+    const long long pos = P.pos0 + (d.y >> 1);  // a position over the records ([a][triple])
+    const long long ai = P.nt > 0 ? pos / P.nt : 0, tpos = pos - ai * P.nt;
+    const long long tt = (pos < P.ntriples) ? (P.order ? (long long)P.order[tpos] : tpos) : -1;
+    const int packed = (tt >= 0 && tt < P.nt) ? P.triples[tt] : -1;
     const int i = packed & 1023, j = (packed >> 10) & 1023, k = (packed >> 20) & 1023;
     d.ok = packed >= 0 && i < P.O && j < P.O && k < P.O;
-    d.planeA = d.grp ? k : i;
+    d.planeA = (int)ai * P.O + (d.grp ? k : i);  // the A operands carry the a index
     d.planeB = j * P.O + (d.grp ? i : k);
     return d;
 }
@@ -444,7 +445,7 @@ __device__ __forceinline__ double slice_src(const SliceParams &P, int plane, int
     const size_t vv = (size_t)V * V, ov = (size_t)O * V;
     if (SIDE == 0) {
         if (d < V) return (h ? P.kvv : P.jvv)[plane * vv + x + (size_t)d * V];
-        return (h ? P.nxov : P.ntov)[plane * ov + x + (size_t)(d - V) * V];
+        return (h ? P.nxov : P.ntov)[(size_t)(plane % O) * ov + x + (size_t)(d - V) * V];  // shared over a
     }
     if (d < V) return h ? P.t2[plane * vv + d + (size_t)x * V] : P.t2[plane * vv + x + (size_t)d * V];
     return (h ? P.jov : P.kov)[plane * ov + (d - V) + (size_t)x * O];
@@ -553,10 +554,11 @@ __global__ void __launch_bounds__(TNTHREAD) oz_tengy_kernel(const TengyParams P)
     const trpdrv_dev_system &S = P.sys;
     const int nvir = S.nvir, tid = threadIdx.x;
     const int nb = (nvir + TW - 1) / TW;
-    const long long pos = P.pos0 + blockIdx.y;
-    if (pos >= S.ntriples) return;
-    const long long tt = S.order ? (long long)S.order[pos] : pos;
-    if (tt < 0 || tt >= S.ntriples) return;
+    const long long pos = P.pos0 + blockIdx.y;  // a position over the records ([a][triple])
+    if (pos >= S.ntriples || S.nt <= 0) return;
+    const long long ai = pos / S.nt, tpos = pos - ai * S.nt;
+    const long long tt = S.order ? (long long)S.order[tpos] : tpos;
+    if (tt < 0 || tt >= S.nt) return;
     const int packed = S.triples[tt];
     const int i = packed & 1023, j = (packed >> 10) & 1023, k = (packed >> 20) & 1023;
 
@@ -585,21 +587,22 @@ __global__ void __launch_bounds__(TNTHREAD) oz_tengy_kernel(const TengyParams P)
 
     TengyVecs v;
     v.eorb = S.eorb;
-    v.dintc1 = S.dintc + (size_t)i * nvir;
-    v.dintx1 = S.dintx + (size_t)i * nvir;
-    v.t1v1 = S.t1v + (size_t)i * nvir;
-    v.dintc2 = S.dintc + (size_t)k * nvir;
-    v.dintx2 = S.dintx + (size_t)k * nvir;
-    v.t1v2 = S.t1v + (size_t)k * nvir;
+    const size_t ao = (size_t)ai * S.nocc;  // the a block of the a-dependent vectors
+    v.dintc1 = S.dintc + (ao + i) * nvir;
+    v.dintx1 = S.dintx + (ao + i) * nvir;
+    v.t1v1 = S.t1v + (ao + i) * nvir;
+    v.dintc2 = S.dintc + (ao + k) * nvir;
+    v.dintx2 = S.dintx + (ao + k) * nvir;
+    v.t1v2 = S.t1v + (ao + k) * nvir;
     v.voff = S.ncor + S.nocc;
     v.nvir = nvir;
     // omp/ccsd_trpdrv_omp_cbody.c:126 (a is 1-based, i/j/k here 0-based)
-    v.eaijk = S.eorb[S.a - 1] - (S.eorb[S.ncor + i] + S.eorb[S.ncor + j] + S.eorb[S.ncor + k]);
+    v.eaijk = S.eorb[S.a - 1 + ai] - (S.eorb[S.ncor + i] + S.eorb[S.ncor + j] + S.eorb[S.ncor + k]);
     TengySums su = {0.0, 0.0, 0.0, 0.0};
     tengy_tile_pair_w<TW>(park, b0, c0, diag, v, tid, TNTHREAD, su);
     const TengySums tot = block_sum4(su, red);
     if (tid == 0) {  // block_sum4's result is valid in thread 0
-        double *out = S.partial + ((size_t)tt * S.npairs * TRPDRV_FUSED_SLOTS + blockIdx.x) * 4;
+        double *out = S.partial + ((size_t)(ai * S.nt + tt) * S.npairs * TRPDRV_FUSED_SLOTS + blockIdx.x) * 4;
         out[0] = tot.e4i;
         out[1] = tot.e5i;
         out[2] = tot.e4k;
@@ -675,7 +678,8 @@ extern "C" int trpdrv_oz_prepare(const trpdrv_oz_system *oz, void *maps_out)
 {
     CUtensorMap *m = static_cast<CUtensorMap *>(maps_out);
     const unsigned long long R = 2ull * oz->nvir, O = (unsigned long long)oz->nocc, S = (unsigned long long)oz->slices;
-    int e = oz::make_map_i8(&m[0], oz->sa, (unsigned long long)oz->dp, R, O * S, oz::BM);
+    const unsigned long long NA = (unsigned long long)(oz->n_a > 0 ? oz->n_a : 1);
+    int e = oz::make_map_i8(&m[0], oz->sa, (unsigned long long)oz->dp, R, NA * O * S, oz::BM);
     if (e) return e;
     return oz::make_map_i8(&m[1], oz->sb, (unsigned long long)oz->dp, R, O * O * S, oz::BN);
 }
@@ -698,7 +702,7 @@ extern "C" int trpdrv_launch_oz_slices(const trpdrv_dev_system *h_sys, const trp
     cudaStream_t st = (cudaStream_t)stream;
     P.out = oz->sa;
     P.scale = oz->ea;
-    oz::oz_slice_kernel<0><<<dim3(rb, (unsigned)oz->nocc), 256, 0, st>>>(P);
+    oz::oz_slice_kernel<0><<<dim3(rb, (unsigned)(oz->nocc * (oz->n_a > 0 ? oz->n_a : 1))), 256, 0, st>>>(P);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return (int)e;
     P.out = oz->sb;
@@ -720,6 +724,7 @@ extern "C" int trpdrv_launch_oz_gemm(const trpdrv_dev_system *h_sys, const trpdr
     P.order = h_sys->order;
     P.pos0 = pos0;
     P.ntriples = h_sys->ntriples;
+    P.nt = h_sys->nt;
     P.fbuf = fbuf;
     P.V = oz->nvir;
     P.O = oz->nocc;

@@ -50,13 +50,13 @@ __device__ __forceinline__ void dd_add(double &hi, double &lo, double x)
 constexpr int RED_THREADS = 1024;
 
 __global__ void __launch_bounds__(RED_THREADS)
-system_reduce_kernel(const double *__restrict__ rec, const int32_t *__restrict__ triples, long long n,
+system_reduce_kernel(const double *__restrict__ rec, const int32_t *__restrict__ triples, long long n, long long nt,
                      double *__restrict__ out)
 {
     __shared__ double sh[4][RED_THREADS];
     double h4 = 0.0, l4 = 0.0, h5 = 0.0, l5 = 0.0;
     for (long long t = threadIdx.x; t < n; t += RED_THREADS) {
-        const int packed = triples[t];
+        const int packed = triples[t % nt];  // records are [a][triple]
         const int i = packed & 1023, k = (packed >> 20) & 1023;
         dd_add(h4, l4, rec[4 * t + 0]);
         dd_add(h5, l5, rec[4 * t + 1]);
@@ -114,10 +114,12 @@ extern "C" int trpdrv_launch_item_reduce(const trpdrv_dev_system *h_sys, void *s
     return (int)cudaGetLastError();
 }
 
-extern "C" int trpdrv_launch_system_reduce(const double *rec, const int32_t *triples, int64_t ntriples,
+extern "C" int trpdrv_launch_system_reduce(const double *rec, const int32_t *triples, int64_t ntriples, int64_t nt,
                                            double *out, void *stream)
 {
-    system_reduce_kernel<<<1, RED_THREADS, 0, (cudaStream_t)stream>>>(rec, triples, (long long)ntriples, out);
+    if (nt <= 0) return 0;
+    system_reduce_kernel<<<1, RED_THREADS, 0, (cudaStream_t)stream>>>(rec, triples, (long long)ntriples, (long long)nt,
+                                                                     out);
     return (int)cudaGetLastError();
 }
 

@@ -148,6 +148,12 @@ double trpdrv_triple_flops(int nocc, int nvir)
     return 16.0 * (double)nvir * (double)nvir * ((double)nvir + (double)nocc);
 }
 
+int trpdrv_tensor_a_dependent(int tensor)
+{
+    return tensor == TRPDRV_T_JVV || tensor == TRPDRV_T_KVV || tensor == TRPDRV_T_DINTC || tensor == TRPDRV_T_DINTX ||
+           tensor == TRPDRV_T_T1V;
+}
+
 size_t trpdrv_tensor_elems(int tensor, int ncor, int nocc, int nvir)
 {
     const size_t o = (size_t)(nocc > 0 ? nocc : 0), v = (size_t)(nvir > 0 ? nvir : 0);

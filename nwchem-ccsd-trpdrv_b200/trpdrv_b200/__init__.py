@@ -57,7 +57,7 @@ class OptionsStruct(C.Structure):
     _fields_ = [("mode", C.c_int), ("nkpass", C.c_int), ("rank", C.c_int), ("world", C.c_int),
                 ("device", C.c_int), ("tile", C.c_int), ("ctas_per_sm", C.c_int),
                 ("use_graph", C.c_int), ("mma_k", C.c_int), ("staging", C.c_int), ("slices", C.c_int),
-                ("batch", C.c_int), ("reserved", C.c_int * 4)]
+                ("batch", C.c_int), ("a_count", C.c_int), ("reserved", C.c_int * 3)]
 
 STAGING_AUTO, STAGING_CPASYNC, STAGING_TMA = 0, 1, 2
 
@@ -115,6 +115,7 @@ _proto("trpdrv_count_triples", C.c_int64, [C.c_int])
 _proto("trpdrv_enumerate_triples", C.c_int64, [C.c_int, C.c_int, C.POINTER(C.c_int32)])
 _proto("trpdrv_partition", C.c_int, [_dp, C.c_int64, C.c_int, C.POINTER(C.c_int64)])
 _proto("trpdrv_shard_triples", C.c_int64, [C.c_int, C.c_int, C.c_int, C.c_int, C.POINTER(C.c_int32)])
+_proto("trpdrv_tensor_a_dependent", C.c_int, [C.c_int])
 _proto("trpdrv_processing_order", C.c_int, [C.POINTER(C.c_int32), C.c_int64, C.c_int, C.POINTER(C.c_int32)])
 _proto("trpdrv_triple_flops", C.c_double, [C.c_int, C.c_int])
 _proto("trpdrv_tensor_elems", C.c_size_t, [C.c_int, C.c_int, C.c_int, C.c_int])
@@ -206,17 +207,35 @@ def tensor_elems(tensor: int, ncor: int, nocc: int, nvir: int) -> int:
     return int(lib.trpdrv_tensor_elems(tensor, ncor, nocc, nvir))
 
 
+def tensor_a_dependent(tensor: int) -> bool:
+    """Whether the tensor holds one block per virtual index in an a sweep (options a_count)."""
+    return bool(lib.trpdrv_tensor_a_dependent(tensor))
+
+
 # --------------------------------------------------------------------------------------------
 # systems
 # --------------------------------------------------------------------------------------------
 @dataclass
 class System:
-    """One system (all triples of one `a`) in the library's slice layout (trpdrv.h)."""
+    """One system in the library's slice layout (trpdrv.h): all triples of the virtual indices
+    a .. a + a_count - 1; the a-dependent tensors hold a_count blocks (plans need a_count=a_count)."""
     ncor: int
     nocc: int
     nvir: int
     a: int
     arrays: dict = field(default_factory=dict)  # name -> contiguous float64 ndarray (host) or device ptr
+    a_count: int = 1
+
+    def a_view(self, ai: int) -> "System":
+        """The single-`a` system of virtual index a + ai (views of the a-dependent blocks)."""
+        out = System(self.ncor, self.nocc, self.nvir, self.a + ai)
+        for t, name in enumerate(TENSOR_NAMES):
+            arr = self.arrays[name]
+            if tensor_a_dependent(t):
+                n = tensor_elems(t, self.ncor, self.nocc, self.nvir)
+                arr = arr[ai * n:(ai + 1) * n]
+            out.arrays[name] = arr
+        return out
 
     def struct(self, device_ptrs: Optional[dict] = None) -> SystemStruct:
         s = SystemStruct()
@@ -234,17 +253,21 @@ class System:
 
 
 def synth_system(nocc: int, nvir: int, seed: int = 1, ncor: int = 0, dist: int = DIST_UNIFORM,
-                 a: Optional[int] = None, alloc=None) -> System:
+                 a: Optional[int] = None, alloc=None, a_count: int = 1) -> System:
     """Seeded synthetic system.  `a` defaults to the first virtual orbital (ncor+nocc+1), which keeps
     every denominator e_b + e_c + eaijk >= 2.1 under these distributions.  `alloc(n)` may return a
-    preallocated (e.g. pinned) float64 buffer of n elements."""
+    preallocated (e.g. pinned) float64 buffer of n elements.  With a_count > 1 the a-dependent
+    tensors get a_count blocks; block 0 is the a_count = 1 system's, block m is generated from seed
+    + 7919 m."""
     if a is None:
         a = ncor + nocc + 1
-    sysm = System(ncor, nocc, nvir, a)
+    sysm = System(ncor, nocc, nvir, a, a_count=a_count)
     for t, name in enumerate(TENSOR_NAMES):
         n = tensor_elems(t, ncor, nocc, nvir)
-        buf = alloc(n) if alloc is not None else np.empty(n, dtype=np.float64)
-        _check(lib.trpdrv_synth_fill(t, ncor, nocc, nvir, seed, dist, _ptr(buf), n))
+        blocks = a_count if tensor_a_dependent(t) else 1
+        buf = alloc(n * blocks) if alloc is not None else np.empty(n * blocks, dtype=np.float64)
+        for m in range(blocks):
+            _check(lib.trpdrv_synth_fill(t, ncor, nocc, nvir, seed + 7919 * m, dist, _ptr(buf[m * n:]), n))
         sysm.arrays[name] = buf
     return sysm
 
@@ -320,7 +343,7 @@ def tengy(f8: np.ndarray, vecs: Sequence[np.ndarray], eorb: np.ndarray, eaijk: f
 # plans
 # --------------------------------------------------------------------------------------------
 def options(mode=MODE_FUSED, nkpass=1, rank=0, world=1, device=-1, ctas_per_sm=0, use_graph=1,
-            mma_k=0, staging=STAGING_AUTO, slices=0, batch=0) -> OptionsStruct:
+            mma_k=0, staging=STAGING_AUTO, slices=0, batch=0, a_count=1) -> OptionsStruct:
     o = OptionsStruct()
     lib.trpdrv_options_default(C.byref(o))
     o.mode, o.nkpass, o.rank, o.world, o.device = mode, nkpass, rank, world, device
@@ -331,6 +354,7 @@ def options(mode=MODE_FUSED, nkpass=1, rank=0, world=1, device=-1, ctas_per_sm=0
         o.slices = slices
     if batch:
         o.batch = batch
+    o.a_count = a_count
     return o
 
 
@@ -343,6 +367,11 @@ class Plan:
         for q, s in enumerate(self.systems):
             st = self._shapes[q]
             st.ncor, st.nocc, st.nvir, st.a = s.ncor, s.nocc, s.nvir, s.a
+        if "a_count" not in opt:  # the systems' a sweep (all alike)
+            counts = {getattr(s, "a_count", 1) for s in self.systems}
+            if len(counts) != 1:
+                raise TrpdrvError(1, f"systems of one plan must share a_count, got {sorted(counts)}")
+            opt["a_count"] = counts.pop()
         self.opt = options(**opt)
         self.h = C.c_void_p()
         _check(lib.trpdrv_plan_create(C.byref(self.h), self._shapes, len(self.systems), C.byref(self.opt)))

@@ -141,3 +141,30 @@ def test_autotune_rejects_a_null_plan(T):
     r = T.TuneResult()
     assert T.lib.trpdrv_plan_autotune(None, C.byref(r)) == 1
     assert r.ncand == 0
+
+
+def test_a_sweep_synthetic_blocks_and_views(T):
+    one = T.synth_system(4, 20, seed=9)
+    three = T.synth_system(4, 20, seed=9, a_count=3)
+    for t, name in enumerate(T.TENSOR_NAMES):
+        n = T.tensor_elems(t, 0, 4, 20)
+        dep = T.tensor_a_dependent(t)
+        assert three.arrays[name].size == n * (3 if dep else 1)
+        assert np.array_equal(three.arrays[name][:n], one.arrays[name])  # block 0 is the single-a system
+        v = three.a_view(2)
+        assert v.a == three.a + 2 and v.arrays[name].size == n
+        if dep:
+            assert not np.array_equal(v.arrays[name], one.arrays[name])
+    assert [T.TENSOR_NAMES[t] for t in range(len(T.TENSOR_NAMES)) if T.tensor_a_dependent(t)] == \
+        ["jvv", "kvv", "dintc", "dintx", "t1v"]
+
+
+def test_a_sweep_range_is_checked_before_device_use(T):
+    s = T.synth_system(2, 8, seed=1, a_count=4)  # a = 3 (first virtual), basis 10: a + 3 <= 10 is fine
+    bad = T.synth_system(2, 8, seed=1, a=8, a_count=4)  # 8 + 3 > 10
+    with pytest.raises(T.TrpdrvError) as ei:
+        T.Plan([bad])
+    assert ei.value.status == 1 and "a_count" in str(ei.value)
+    with pytest.raises(T.TrpdrvError) as ei:
+        T.Plan([s, T.synth_system(2, 8, seed=2)])  # mixed a_count
+    assert ei.value.status == 1

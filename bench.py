@@ -392,6 +392,33 @@ def plain_sample(T, R, s, flop_triple, frac=16):
             "tflops_fp64_equiv": nplain * flop_triple / (pms * 1e-3) / 1e12}
 
 
+def dropin_leg(T, s, ntrip=256):
+    """The reference-facing entry point ccsd_trpdrv_omp_cbody_ called once per triple from host buffers,
+    as omp/test.c:160-195 calls it (wall clock: every call returns its energies to the host).  Timed with
+    per-call copies of the slices (the default) and with the system's arrays registered as unchanging
+    (trpdrv_register_host: no per-call transfer)."""
+    ijkl = T.enumerate_triples(s.nocc, 1)[:ntrip]
+    # pageable host memory, like the reference driver's own arrays (omp/test.c:112-146)
+    s = T.System(s.ncor, s.nocc, s.nvir, s.a, {k: np.array(v, copy=True) for k, v in s.arrays.items()})
+    out = {}
+    for label in ("per_call_copies", "registered_inputs"):
+        if label == "registered_inputs":
+            T.register_system(s)
+        for i, j, k, klo in ijkl[:8]:  # warm-up
+            T.cbody(s, int(i), int(j), int(k), int(klo))
+        t0 = time.perf_counter()
+        e4 = e5 = 0.0
+        for i, j, k, klo in ijkl:
+            e4, e5 = T.cbody(s, int(i), int(j), int(k), int(klo), e4, e5)
+        el = time.perf_counter() - t0
+        if label == "registered_inputs":
+            T.unregister_system(s)
+        out[label] = {"value": len(ijkl) / el, "unit": "triples/s", "emp4": e4, "emp5": e5}
+    out["sample"] = (f"the first {len(ijkl)} triples of the driver order at nocc={s.nocc} nvir={s.nvir}, one "
+                     f"ccsd_trpdrv_omp_cbody_ call each from pageable host buffers (wall clock, Python caller)")
+    return out
+
+
 def cpu_leg(args, R, nocc, nvir):
     if R.rank != 0 or R.world != 1 or args.no_cpu_baseline:
         return None
@@ -593,6 +620,8 @@ def run_b200_arm(args):
         else:
             line["emp4"], line["emp5"] = e4[0], e5[0]
             line["cpu_baseline"] = cpu_leg(args, R, args.nocc, args.nvir)
+            if not args.profile and not args.no_plain:
+                line["dropin"] = dropin_leg(T, systems[0])
             if emulated:
                 emu = emulated[str(DEFAULT_SLICES)]
                 line["emulated"] = {"default_slices": DEFAULT_SLICES, "value": emu["value"], "unit": "triples/s",

@@ -314,7 +314,22 @@ int trpdrv_body_device_noalloc(const trpdrv_body_device_args *args, void *stream
  * 3 = m16n8k16, 4 = scalar DFMA.  Writes the achieved TFLOP/s. */
 int trpdrv_probe_fp64_peak(int device, int kind, double *tflops);
 
-/* Releases the drop-in entry points' device state (buffers, stream).  Safe to call repeatedly. */
+/* ---- inputs that do not change between drop-in calls ----
+ * The drop-in entry points copy every input slice host -> device on each call, because the
+ * reference's callers may refill their buffers between calls (SURVEY of the NWChem driver: the same
+ * host buffers are refilled per (i, a) and (k, j) block).  A caller whose arrays stay fixed while
+ * it loops over triples (omp/test.c:160-195 passes slices of arrays allocated once) registers them:
+ * the library keeps a device copy of [ptr, ptr + bytes), and every drop-in pointer that lies inside
+ * a registered array is read from that copy, with no per-call transfer.  After changing a registered
+ * array, call trpdrv_refresh_host (or unregister it).  Ranges must not overlap; at most 64 arrays.
+ * trpdrv_finalize drops every registration.  No counterpart in the reference (its body reads host
+ * memory directly). */
+int trpdrv_register_host(const void *ptr, size_t bytes);
+int trpdrv_refresh_host(const void *ptr);
+int trpdrv_unregister_host(const void *ptr);
+
+/* Releases the drop-in entry points' device state (buffers, stream, registered arrays).  Safe to
+ * call repeatedly. */
 void trpdrv_finalize(void);
 
 #ifdef __cplusplus

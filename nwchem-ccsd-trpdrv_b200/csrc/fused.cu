@@ -188,7 +188,8 @@ __device__ __forceinline__ void prepare_item(const trpdrv_dev_system *__restrict
     const long long local = item - S.item_begin;
     const long long qpos = local / S.npairs;  // processing position over the system's records
     const int p = (int)(local - qpos * S.npairs);
-    const long long ai = S.nt > 0 ? qpos / S.nt : 0;  // a index: records are [a][triple]
+    // a index (records are [a][triple], fewer than 2^31: the host checks); no division for a single a
+    const long long ai = (S.nt > 0 && qpos >= S.nt) ? (long long)((unsigned)qpos / (unsigned)S.nt) : 0;
     const long long tpos = qpos - ai * S.nt;
     const long long tt = (S.order && local >= 0 && qpos < S.ntriples) ? (long long)S.order[tpos] : tpos;
     const long long own = (ai * S.nt + tt) * S.npairs + p;  // energies go to the record's own items

@@ -295,6 +295,7 @@ static int plan_build(trpdrv_plan *p, const trpdrv_system *shape)
         b->nt = n;
         b->n_a = o->a_count;
         b->ntriples = n * o->a_count;
+        if (b->ntriples > INT32_MAX) return fail(TRPDRV_ERR_ARG, "system %d: more than 2^31 (a, triple) records", q);
         int32_t *ijk = (int32_t *)malloc(sizeof(int32_t) * 3 * (size_t)(n > 0 ? n : 1));
         b->h_triples = (int32_t *)malloc(sizeof(int32_t) * (size_t)(n > 0 ? n : 1));
         if (!ijk || !b->h_triples) {
@@ -1118,10 +1119,38 @@ static int env_flag(const char *name, const char *value)
     return v && strcmp(v, value) == 0;
 }
 
+/* Host arrays registered as unchanging (trpdrv_register_host): device copies that the drop-in entry
+ * points read in place of per-call copies of any pointer inside them. */
+#define DI_MAX_REG 64
+static struct reg_entry {
+    const char *host;
+    size_t bytes;
+    char *dev;
+} g_reg[DI_MAX_REG];
+static int g_nreg;
+
+static void reg_release(void)
+{
+    for (int r = 0; r < g_nreg; ++r) cudaFree(g_reg[r].dev);
+    memset(g_reg, 0, sizeof g_reg);
+    g_nreg = 0;
+}
+
+/* device address of [p, p + n) if it lies inside a registered array, else NULL */
+static const double *reg_lookup(const double *p, size_t n)
+{
+    const char *c = (const char *)p;
+    for (int r = 0; r < g_nreg; ++r)
+        if (c >= g_reg[r].host && c + n * sizeof(double) <= g_reg[r].host + g_reg[r].bytes)
+            return (const double *)(g_reg[r].dev + (c - g_reg[r].host));
+    return NULL;
+}
+
 static void di_release(void)
 {
     if (!g_di.ready) return;
     cudaSetDevice(g_di.device);
+    reg_release();
     for (int q = 0; q < DI_NVV; ++q) cudaFree(g_di.vv[q]);
     for (int q = 0; q < DO_NOV; ++q) cudaFree(g_di.ov[q]);
     for (int q = 0; q < 4; ++q) cudaFree(g_di.nov[q]);
@@ -1134,6 +1163,83 @@ static void di_release(void)
     cudaFreeHost(g_di.h_out4);
     cudaStreamDestroy(g_di.stream);
     memset(&g_di, 0, sizeof g_di);
+}
+
+static int di_reserve(int nocc, int nvir, int nbf);
+
+int trpdrv_register_host(const void *ptr, size_t bytes)
+{
+    if (!ptr || bytes == 0) return fail(TRPDRV_ERR_ARG, "NULL pointer or empty range");
+    pthread_mutex_lock(&g_di_mu);
+    int rc = TRPDRV_OK;
+    if (g_nreg >= DI_MAX_REG) {
+        rc = fail(TRPDRV_ERR_ARG, "at most %d registered arrays", DI_MAX_REG);
+    } else {
+        const char *c = (const char *)ptr;
+        for (int r = 0; r < g_nreg && rc == TRPDRV_OK; ++r)
+            if (c < g_reg[r].host + g_reg[r].bytes && g_reg[r].host < c + bytes)
+                rc = fail(TRPDRV_ERR_ARG, "range overlaps a registered array");
+        if (rc == TRPDRV_OK) rc = di_reserve(1, 1, 1); /* device and stream of the drop-in entry points */
+        char *dev = NULL;
+        if (rc == TRPDRV_OK) {
+            cudaError_t e = cudaMalloc((void **)&dev, bytes);
+            if (e == cudaSuccess) e = cudaMemcpy(dev, ptr, bytes, cudaMemcpyHostToDevice);
+            if (e != cudaSuccess) {
+                if (dev) cudaFree(dev);
+                rc = fail(e == cudaErrorMemoryAllocation ? TRPDRV_ERR_NOMEM : TRPDRV_ERR_CUDA, "register: %s",
+                          cudaGetErrorString(e));
+            } else {
+                g_reg[g_nreg].host = c;
+                g_reg[g_nreg].bytes = bytes;
+                g_reg[g_nreg].dev = dev;
+                ++g_nreg;
+            }
+        }
+    }
+    pthread_mutex_unlock(&g_di_mu);
+    return rc;
+}
+
+static int reg_find(const void *ptr)
+{
+    for (int r = 0; r < g_nreg; ++r)
+        if (g_reg[r].host == (const char *)ptr) return r;
+    return -1;
+}
+
+int trpdrv_refresh_host(const void *ptr)
+{
+    pthread_mutex_lock(&g_di_mu);
+    const int r = reg_find(ptr);
+    int rc = TRPDRV_OK;
+    if (r < 0) {
+        rc = fail(TRPDRV_ERR_ARG, "not a registered array");
+    } else {
+        cudaSetDevice(g_di.device);
+        const cudaError_t e = cudaMemcpy(g_reg[r].dev, g_reg[r].host, g_reg[r].bytes, cudaMemcpyHostToDevice);
+        if (e != cudaSuccess) rc = fail(TRPDRV_ERR_CUDA, "refresh: %s", cudaGetErrorString(e));
+    }
+    pthread_mutex_unlock(&g_di_mu);
+    return rc;
+}
+
+int trpdrv_unregister_host(const void *ptr)
+{
+    pthread_mutex_lock(&g_di_mu);
+    const int r = reg_find(ptr);
+    int rc = TRPDRV_OK;
+    if (r < 0) {
+        rc = fail(TRPDRV_ERR_ARG, "not a registered array");
+    } else {
+        cudaSetDevice(g_di.device);
+        cudaStreamSynchronize(g_di.stream); /* no call in flight reads it */
+        cudaFree(g_reg[r].dev);
+        g_reg[r] = g_reg[g_nreg - 1];
+        memset(&g_reg[g_nreg - 1], 0, sizeof g_reg[0]);
+        --g_nreg;
+    }
+    pthread_mutex_unlock(&g_di_mu);
+    return rc;
 }
 
 void trpdrv_finalize(void)
@@ -1194,13 +1300,19 @@ static int di_reserve(int nocc, int nvir, int nbf)
     return TRPDRV_OK;
 }
 
-static int h2d(double *dst, const double *src, size_t n)
+/* Device copy of host [src, src + n): the registered copy when there is one, else a copy into `slot`. */
+static int h2d(const double **out, double *slot, const double *src, size_t n)
 {
-    CUDA_TRY(cudaMemcpyAsync(dst, src, sizeof(double) * n, cudaMemcpyHostToDevice, g_di.stream));
+    const double *d = reg_lookup(src, n);
+    if (!d) {
+        CUDA_TRY(cudaMemcpyAsync(slot, src, sizeof(double) * n, cudaMemcpyHostToDevice, g_di.stream));
+        d = slot;
+    }
+    *out = d;
     return TRPDRV_OK;
 }
 
-static int di_tengy_launch(int ncor, int nocc, int nvir, double eaijk)
+static int di_tengy_launch(int ncor, int nocc, int nvir, double eaijk, const double *const *vec, const double *eorb)
 {
     trpdrv_tengy_args ta;
     memset(&ta, 0, sizeof ta);
@@ -1210,13 +1322,13 @@ static int di_tengy_launch(int ncor, int nocc, int nvir, double eaijk)
     ta.use_eaijk = 1;
     ta.eaijk = eaijk;
     ta.f = g_di.f;
-    ta.eorb = g_di.eorb;
-    ta.dintc1 = g_di.vec[0];
-    ta.dintx1 = g_di.vec[1];
-    ta.t1v1 = g_di.vec[2];
-    ta.dintc2 = g_di.vec[3];
-    ta.dintx2 = g_di.vec[4];
-    ta.t1v2 = g_di.vec[5];
+    ta.eorb = eorb;
+    ta.dintc1 = vec[0];
+    ta.dintx1 = vec[1];
+    ta.t1v1 = vec[2];
+    ta.dintc2 = vec[3];
+    ta.dintx2 = vec[4];
+    ta.t1v2 = vec[5];
     ta.block_partial = g_di.bpart;
     ta.counter = g_di.tcount;
     ta.out4 = g_di.out4;
@@ -1256,33 +1368,34 @@ static int body_impl(double *f1n, double *f1t, double *f2n, double *f2t, double 
     TRY(di_reserve(nocc, nvir, nbf));
     const size_t lnvv = (size_t)nvir * nvir, lnov = (size_t)nocc * nvir;
     const size_t vv = (size_t)(k - klo) * lnvv, ov = (size_t)(k - klo) * lnov;
-    TRY(h2d(g_di.vv[DI_JIA], jia, lnvv));
-    TRY(h2d(g_di.vv[DI_KIA], kia, lnvv));
-    TRY(h2d(g_di.vv[DI_JKA], jka + vv, lnvv));
-    TRY(h2d(g_di.vv[DI_KKA], kka + vv, lnvv));
-    TRY(h2d(g_di.vv[DI_TIJ], tij, lnvv));
-    TRY(h2d(g_di.vv[DI_TKJ], tkj + vv, lnvv));
-    TRY(h2d(g_di.ov[DO_TIA], tia, lnov));
-    TRY(h2d(g_di.ov[DO_XIA], xia, lnov));
-    TRY(h2d(g_di.ov[DO_TKA], tka + ov, lnov));
-    TRY(h2d(g_di.ov[DO_XKA], xka + ov, lnov));
-    TRY(h2d(g_di.ov[DO_JIJ], jij, lnov));
-    TRY(h2d(g_di.ov[DO_JKJ], jkj + ov, lnov));
-    TRY(h2d(g_di.ov[DO_KIJ], kij, lnov));
-    TRY(h2d(g_di.ov[DO_KKJ], kkj + ov, lnov));
+    const double *dv[DI_NVV], *dov[DO_NOV], *dvec[6], *deorb;
+    TRY(h2d(&dv[DI_JIA], g_di.vv[DI_JIA], jia, lnvv));
+    TRY(h2d(&dv[DI_KIA], g_di.vv[DI_KIA], kia, lnvv));
+    TRY(h2d(&dv[DI_JKA], g_di.vv[DI_JKA], jka + vv, lnvv));
+    TRY(h2d(&dv[DI_KKA], g_di.vv[DI_KKA], kka + vv, lnvv));
+    TRY(h2d(&dv[DI_TIJ], g_di.vv[DI_TIJ], tij, lnvv));
+    TRY(h2d(&dv[DI_TKJ], g_di.vv[DI_TKJ], tkj + vv, lnvv));
+    TRY(h2d(&dov[DO_TIA], g_di.ov[DO_TIA], tia, lnov));
+    TRY(h2d(&dov[DO_XIA], g_di.ov[DO_XIA], xia, lnov));
+    TRY(h2d(&dov[DO_TKA], g_di.ov[DO_TKA], tka + ov, lnov));
+    TRY(h2d(&dov[DO_XKA], g_di.ov[DO_XKA], xka + ov, lnov));
+    TRY(h2d(&dov[DO_JIJ], g_di.ov[DO_JIJ], jij, lnov));
+    TRY(h2d(&dov[DO_JKJ], g_di.ov[DO_JKJ], jkj + ov, lnov));
+    TRY(h2d(&dov[DO_KIJ], g_di.ov[DO_KIJ], kij, lnov));
+    TRY(h2d(&dov[DO_KKJ], g_di.ov[DO_KKJ], kkj + ov, lnov));
     const double *vecs[6] = {dintc1, dintx1, t1v1, dintc2, dintx2, t1v2};
-    for (int q = 0; q < 6; ++q) TRY(h2d(g_di.vec[q], vecs[q], (size_t)nvir));
-    TRY(h2d(g_di.eorb, eorb, (size_t)nbf));
-    for (int q = 0; q < 4; ++q) LAUNCH_TRY(trpdrv_launch_negate(g_di.ov[q], g_di.nov[q], lnov, g_di.stream));
+    for (int q = 0; q < 6; ++q) TRY(h2d(&dvec[q], g_di.vec[q], vecs[q], (size_t)nvir));
+    TRY(h2d(&deorb, g_di.eorb, eorb, (size_t)nbf));
+    for (int q = 0; q < 4; ++q) LAUNCH_TRY(trpdrv_launch_negate(dov[q], g_di.nov[q], lnov, g_di.stream));
 
     trpdrv_plain_args ga;
     memset(&ga, 0, sizeof ga);
     ga.nocc = nocc;
     ga.nvir = nvir;
     ga.f = g_di.f;
-    double *const *V = g_di.vv;
+    const double *const *V = dv;
     double *const *N = g_di.nov;
-    double *const *Ob = g_di.ov;
+    const double *const *Ob = dov;
     const double *a1[8] = {V[DI_JIA], V[DI_KIA], V[DI_JIA], V[DI_KIA], V[DI_JKA], V[DI_KKA], V[DI_JKA], V[DI_KKA]};
     const double *b1[8] = {V[DI_TKJ], V[DI_TKJ], V[DI_TKJ], V[DI_TKJ], V[DI_TIJ], V[DI_TIJ], V[DI_TIJ], V[DI_TIJ]};
     const int nt[8] = {1, 1, 0, 0, 1, 1, 0, 0};
@@ -1300,7 +1413,7 @@ static int body_impl(double *f1n, double *f1t, double *f2n, double *f2t, double 
 
     /* omp/ccsd_trpdrv_omp_cbody.c:122-126 */
     const double eaijk = eorb[a - 1] - (eorb[ncor + i - 1] + eorb[ncor + j - 1] + eorb[ncor + k - 1]);
-    TRY(di_tengy_launch(ncor, nocc, nvir, eaijk));
+    TRY(di_tengy_launch(ncor, nocc, nvir, eaijk, dvec, deorb));
 
     if (write_f) {
         double *outs[8] = {f1n, f2n, f3n, f4n, f1t, f2t, f3t, f4t};
@@ -1371,11 +1484,15 @@ static int tengy_impl(const double *f1n, const double *f1t, const double *f2n, c
     TRY(di_reserve(nocc > 0 ? nocc : 1, nvir, nbf));
     const size_t lnvv = (size_t)nvir * nvir;
     const double *fs[8] = {f1n, f2n, f3n, f4n, f1t, f2t, f3t, f4t};
-    for (int x = 0; x < 8; ++x) TRY(h2d(g_di.f + (size_t)x * lnvv, fs[x], lnvv));
+    /* the tengy kernel reads the eight f as one contiguous block: always copied */
+    for (int x = 0; x < 8; ++x)
+        CUDA_TRY(cudaMemcpyAsync(g_di.f + (size_t)x * lnvv, fs[x], sizeof(double) * lnvv, cudaMemcpyHostToDevice,
+                                 g_di.stream));
     const double *vecs[6] = {dintc1, dintx1, t1v1, dintc2, dintx2, t1v2};
-    for (int q = 0; q < 6; ++q) TRY(h2d(g_di.vec[q], vecs[q], (size_t)nvir));
-    TRY(h2d(g_di.eorb, eorb, (size_t)nbf));
-    TRY(di_tengy_launch(ncor, nocc, nvir, eaijk));
+    const double *dvec[6], *deorb;
+    for (int q = 0; q < 6; ++q) TRY(h2d(&dvec[q], g_di.vec[q], vecs[q], (size_t)nvir));
+    TRY(h2d(&deorb, g_di.eorb, eorb, (size_t)nbf));
+    TRY(di_tengy_launch(ncor, nocc, nvir, eaijk, dvec, deorb));
     *emp4i = g_di.h_out4[0];
     *emp5i = g_di.h_out4[1];
     *emp4k = g_di.h_out4[2];

@@ -232,7 +232,9 @@ __device__ __forceinline__ Tile decode_tile(const GemmParams &P, int t)
     d.n0 = (rem / P.mtiles) * BN;
     d.grp = d.y & 1;
     const long long pos = P.pos0 + (d.y >> 1);  // a position over the records ([a][triple])
-    const long long ai = P.nt > 0 ? pos / P.nt : 0, tpos = pos - ai * P.nt;
+    // records < 2^31 (the host checks): 32-bit division, none for a single a
+    const unsigned ai = (P.nt > 0 && pos >= P.nt) ? (unsigned)pos / (unsigned)P.nt : 0u;
+    const long long tpos = pos - (long long)ai * P.nt;
     const long long tt = (pos < P.ntriples) ? (P.order ? (long long)P.order[tpos] : tpos) : -1;
     const int packed = (tt >= 0 && tt < P.nt) ? P.triples[tt] : -1;
     const int i = packed & 1023, j = (packed >> 10) & 1023, k = (packed >> 20) & 1023;
@@ -556,7 +558,8 @@ __global__ void __launch_bounds__(TNTHREAD) oz_tengy_kernel(const TengyParams P)
     const int nb = (nvir + TW - 1) / TW;
     const long long pos = P.pos0 + blockIdx.y;  // a position over the records ([a][triple])
     if (pos >= S.ntriples || S.nt <= 0) return;
-    const long long ai = pos / S.nt, tpos = pos - ai * S.nt;
+    const unsigned ai = pos >= S.nt ? (unsigned)pos / (unsigned)S.nt : 0u;  // records < 2^31
+    const long long tpos = pos - (long long)ai * S.nt;
     const long long tt = S.order ? (long long)S.order[tpos] : tpos;
     if (tt < 0 || tt >= S.nt) return;
     const int packed = S.triples[tt];
@@ -602,7 +605,7 @@ __global__ void __launch_bounds__(TNTHREAD) oz_tengy_kernel(const TengyParams P)
     tengy_tile_pair_w<TW>(park, b0, c0, diag, v, tid, TNTHREAD, su);
     const TengySums tot = block_sum4(su, red);
     if (tid == 0) {  // block_sum4's result is valid in thread 0
-        double *out = S.partial + ((size_t)(ai * S.nt + tt) * S.npairs * TRPDRV_FUSED_SLOTS + blockIdx.x) * 4;
+        double *out = S.partial + ((size_t)((long long)ai * S.nt + tt) * S.npairs * TRPDRV_FUSED_SLOTS + blockIdx.x) * 4;
         out[0] = tot.e4i;
         out[1] = tot.e5i;
         out[2] = tot.e4k;

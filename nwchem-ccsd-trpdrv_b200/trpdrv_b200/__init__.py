@@ -124,6 +124,9 @@ _proto("trpdrv_synth_fill", C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int, C.c_ui
 _proto("trpdrv_probe_fp64_peak", C.c_int, [C.c_int, C.c_int, _dp])
 _proto("trpdrv_body_device_noalloc", C.c_int, [C.POINTER(BodyDeviceArgs), C.c_void_p])
 _proto("trpdrv_finalize", None, [])
+_proto("trpdrv_register_host", C.c_int, [C.c_void_p, C.c_size_t])
+_proto("trpdrv_refresh_host", C.c_int, [C.c_void_p])
+_proto("trpdrv_unregister_host", C.c_int, [C.c_void_p])
 _body_args = [_dp] * 9 + [_ip] * 3 + [_dp] * 2 + [_ip] * 5 + [_dp] * 20
 for _n in ("ccsd_trpdrv_omp_cbody_", "ccsd_trpdrv_omp_fbody_", "ccsd_trpdrv_cbody_", "ccsd_trpdrv_opencl_"):
     _proto(_n, None, _body_args)
@@ -318,6 +321,30 @@ def body_call(fn, s: System, i: int, j: int, k: int, klo: int, emp4: float = 0.0
 
 def cbody(s: System, i: int, j: int, k: int, klo: int, emp4=0.0, emp5=0.0, f=None, entry="ccsd_trpdrv_omp_cbody_"):
     return body_call(getattr(lib, entry), s, i, j, k, klo, emp4, emp5, f)
+
+
+def register_host(arr: np.ndarray):
+    """trpdrv_register_host: the drop-in entry points read pointers inside `arr` from a device copy."""
+    _check(lib.trpdrv_register_host(C.c_void_p(arr.ctypes.data), arr.nbytes))
+
+
+def refresh_host(arr: np.ndarray):
+    _check(lib.trpdrv_refresh_host(C.c_void_p(arr.ctypes.data)))
+
+
+def unregister_host(arr: np.ndarray):
+    _check(lib.trpdrv_unregister_host(C.c_void_p(arr.ctypes.data)))
+
+
+def register_system(s: "System"):
+    """Registers every array of a host system (its tensors stay unchanged while drop-in calls run)."""
+    for name in TENSOR_NAMES:
+        register_host(s.arrays[name])
+
+
+def unregister_system(s: "System"):
+    for name in TENSOR_NAMES:
+        unregister_host(s.arrays[name])
 
 
 def tengy(f8: np.ndarray, vecs: Sequence[np.ndarray], eorb: np.ndarray, eaijk: float, ncor: int, nocc: int,

@@ -168,3 +168,9 @@ def test_a_sweep_range_is_checked_before_device_use(T):
     with pytest.raises(T.TrpdrvError) as ei:
         T.Plan([s, T.synth_system(2, 8, seed=2)])  # mixed a_count
     assert ei.value.status == 1
+
+
+def test_register_host_checks_arguments_first(T):
+    assert T.lib.trpdrv_register_host(None, 8) == 1
+    assert T.lib.trpdrv_refresh_host(None) == 1
+    assert T.lib.trpdrv_unregister_host(None) == 1

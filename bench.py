@@ -348,7 +348,7 @@ def emulated_ops_per_triple(nocc, nvir, slices):
     return 2 * (2 * nvir) ** 2 * (nvir + nocc) * 2 * slices * (slices + 1) / 2
 
 
-def emulated_sweep(T, R, systems, ref_e4, ref_e5, steps, warmup, slice_list, int8_peak):
+def emulated_sweep(T, R, systems, ref_e4, ref_e5, steps, warmup, slice_list, int8_peak, fp64_peak=None):
     """The emulated form on the same systems for each slice count: triples/s, FP64-equivalent TFLOP/s,
     int8 tensor-pipe rate and its error against the native FP64 fused result."""
     out = {}
@@ -368,6 +368,7 @@ def emulated_sweep(T, R, systems, ref_e4, ref_e5, steps, warmup, slice_list, int
                         "tflops_fp64_equiv": flop / sec / 1e12, "kernel_ms": kms, "gpu_launches": launches,
                         "int8_tops": int8_tops, "int8_frac": (int8_tops / int8_peak) if int8_peak else None,
                         "emp4_rel_err_vs_fp64": r4, "emp5_rel_err_vs_fp64": r5,
+                        "fp64_roofline_frac": (flop / sec / 1e12) / fp64_peak if fp64_peak else None,
                         "batch": tune["candidates"][tune["chosen"]]["batch"]}
     return out
 
@@ -520,7 +521,7 @@ def run_b200_arm(args):
             clocks = ClockSampler(R.local)
             clocks.start()
             time.sleep(0.3)
-        emulated = emulated_sweep(T, R, systems, e4, e5, args.steps, args.warmup, SLICES, int8_peak)
+        emulated = emulated_sweep(T, R, systems, e4, e5, args.steps, args.warmup, SLICES, int8_peak, peak)
         if args.workload == "c3":
             ck = clocks.stop()
     emu_e2e_sec = None

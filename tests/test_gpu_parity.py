@@ -251,6 +251,22 @@ def test_full_size_fused_vs_plain_and_reference_sample(T, O):
             assert_records_close(recf[0][lo:lo + 8], rec)
 
 
+def test_config1_plain_and_fused_match_the_reference_on_every_triple(T, O):
+    """nocc=20, nvir=200, all 4,200 triples of the driver, plain per-triple path and
+    fused kernel against the reference body compiled unmodified (run on every host thread)."""
+    if not O.have_reference():
+        pytest.skip("reference build missing")
+    import os
+    s = T.synth_system(20, 200, seed=2025)
+    ref, tot, mism = O.run_system(s, "reference", nthreads=os.cpu_count() or 1)
+    assert mism == 0 and len(ref) == 4200
+    for mode in (0, 1):
+        e4, e5, rec, _ = _plan_run(T, [s], mode=mode)
+        assert_records_close(rec[0], ref)
+        assert_total_close(e4[0], tot[0], what=f"emp4 mode {mode}")
+        assert_total_close(e5[0], tot[1], what=f"emp5 mode {mode}")
+
+
 def test_tma_staging_is_refused_for_odd_sizes(T):
     s = T.synth_system(5, 33, seed=3)
     with T.Plan([s], mode=1, staging=2) as p:

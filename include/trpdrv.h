@@ -183,7 +183,10 @@ typedef struct trpdrv_options {
                          kvv, dintc, dintx, t1v) then hold a_count consecutive blocks, a-major; the others
                          are shared.  Energies sum over every (a, i, j, k); per-triple records are
                          [a][triple].  0 or 1 = the single `a` of the reference driver (default). */
-    int reserved[3];
+    int target_digits;  /* EMULATED: when > 0, digit slices are chosen for a relative error of 10^-target_digits:
+                           the plan holds 8 slices, runs 8 until trpdrv_plan_autotune has measured on a
+                           sample which fewest slices agree with 8 to 10^-(target_digits+1) */
+    int reserved[2];
 } trpdrv_options;
 
 void trpdrv_options_default(trpdrv_options *opt);
@@ -223,7 +226,8 @@ int trpdrv_plan_destroy(trpdrv_plan *plan);
  * keeps the fastest (FUSED: TMA vs cp.async staging, FP64 MMA shape m16n8k8 vs m16n8k4, CTAs per SM;
  * EMULATED: triples per launch pair, 4 / 8 / 16).  Needs a bound plan (after upload or bind); each
  * system is sampled (about 1/8 of its fused items, 64 triples in the emulated form) and the per-
- * system times are scaled to its full work.  The choice is cached per device and set of shapes for
+ * system times are scaled to its full work.  EMULATED plans with target_digits first pick the fewest
+ * slices (4..8) that meet the accuracy target on the same sample.  The choice is cached per device and set of shapes for
  * the life of the process; a later plan with the same key takes it without timing.  No counterpart
  * in the reference (its BLAS call sites have nothing to tune).  `result` may be NULL. */
 typedef struct trpdrv_tune_candidate {
@@ -236,6 +240,9 @@ typedef struct trpdrv_tune_candidate {
 typedef struct trpdrv_tune_result {
     int ncand, chosen, from_cache;
     trpdrv_tune_candidate cand[8];
+    int slices;           /* EMULATED: digit slices in use after tuning */
+    double est_rel_err;   /* EMULATED with target_digits: sampled per-triple deviation of that slice
+                             count from 8 slices (normwise per energy column), else 0 */
 } trpdrv_tune_result;
 int trpdrv_plan_autotune(trpdrv_plan *plan, trpdrv_tune_result *result);
 

@@ -7,6 +7,7 @@
 #include "launch.h"
 
 #include <cuda_runtime_api.h>
+#include <math.h>
 #include <pthread.h>
 #include <stdarg.h>
 #include <stdio.h>
@@ -420,7 +421,10 @@ int trpdrv_plan_create(trpdrv_plan **plan, const trpdrv_system *shape, int nsys,
         trpdrv_options_default(&o);
     if (o.mode != TRPDRV_MODE_PLAIN && o.mode != TRPDRV_MODE_FUSED && o.mode != TRPDRV_MODE_EMULATED)
         return fail(TRPDRV_ERR_ARG, "unknown mode %d", o.mode);
+    if (o.target_digits < 0 || o.target_digits > 15)
+        return fail(TRPDRV_ERR_ARG, "target_digits %d: must be 0..15", o.target_digits);
     if (o.slices == 0) o.slices = 7;
+    if (o.mode == TRPDRV_MODE_EMULATED && o.target_digits > 0) o.slices = 8; /* room for any choice */
     if (o.batch == 0) o.batch = 8;
     if (!trpdrv_oz_slices_supported(o.slices))
         return fail(TRPDRV_ERR_ARG, "slices %d: must be %d..%d", o.slices, TRPDRV_OZ_MIN_SLICES, TRPDRV_OZ_MAX_SLICES);
@@ -943,6 +947,108 @@ static int tune_time(trpdrv_plan *p, const trpdrv_tune_candidate *c, double *est
     return TRPDRV_OK;
 }
 
+/* emulated plans: switch every system to `slices` digit slices (the buffers hold 8) */
+static int tune_set_slices(trpdrv_plan *p, int slices)
+{
+    for (int q = 0; q < p->nsys; ++q) {
+        p->s[q].oz.slices = slices;
+        const int e = trpdrv_oz_prepare(&p->s[q].oz, p->s[q].oz_maps);
+        if (e) return fail(TRPDRV_ERR_CUDA, "tensor-map encoding failed (%d)", e);
+    }
+    p->opt.slices = slices;
+    if (p->graph_ready) {
+        cudaGraphExecDestroy(p->gexec);
+        cudaGraphDestroy(p->graph);
+        p->gexec = NULL;
+        p->graph = NULL;
+        p->graph_ready = 0;
+    }
+    return TRPDRV_OK;
+}
+
+/* emulated plans: per-triple records of the first 64 positions of every system (the other records keep
+ * what they held), copied to host[q] (ntriples * 4 each) */
+static int tune_sample_records(trpdrv_plan *p, double **host)
+{
+    cudaStream_t st = p->stream;
+    for (int q = 0; q < p->nsys; ++q) {
+        const trpdrv_dev_system *d = &p->h_dev[q];
+        const sysbuf *b = &p->s[q];
+        if (d->ntriples <= 0) continue;
+        const int64_t n = d->ntriples < 64 ? d->ntriples : 64;
+        LAUNCH_TRY(trpdrv_launch_oz_slices(d, &b->oz, st));
+        for (int64_t pos = 0; pos < n; pos += p->opt.batch) {
+            const int m = (int)(n - pos < p->opt.batch ? n - pos : p->opt.batch);
+            LAUNCH_TRY(trpdrv_launch_oz_gemm(d, &b->oz, b->oz_maps, pos, m, p->d_fbuf, p->d_status, p->nsm, st));
+            LAUNCH_TRY(trpdrv_launch_oz_tengy(d, pos, m, p->d_fbuf, st));
+        }
+        LAUNCH_TRY(trpdrv_launch_item_reduce(d, st));
+        CUDA_TRY(cudaMemcpyAsync(host[q], b->rec, sizeof(double) * 4 * (size_t)b->ntriples, cudaMemcpyDeviceToHost, st));
+    }
+    CUDA_TRY(cudaStreamSynchronize(st));
+    return TRPDRV_OK;
+}
+
+/* largest normwise (per energy column) deviation of got from want over every system's records */
+static double tune_record_dev(const trpdrv_plan *p, double **got, double **want)
+{
+    double worst = 0.0;
+    for (int q = 0; q < p->nsys; ++q)
+        for (int c = 0; c < 4; ++c) {
+            double scale = 0.0, dev = 0.0;
+            for (int64_t t = 0; t < p->s[q].ntriples; ++t) {
+                const double w = fabs(want[q][4 * t + c]), e = fabs(got[q][4 * t + c] - want[q][4 * t + c]);
+                if (w > scale) scale = w;
+                if (e > dev) dev = e;
+            }
+            if (scale > 0.0 && dev / scale > worst) worst = dev / scale;
+        }
+    return worst;
+}
+
+/* emulated plans with target_digits: the fewest slices (4..7, else 8) whose sampled records agree with
+ * those of 8 slices to a tenth of the target */
+static int tune_choose_slices(trpdrv_plan *p, double *est)
+{
+    const double target = pow(10.0, -(double)(p->opt.target_digits + 1));
+    double **ref = (double **)calloc((size_t)p->nsys, sizeof(double *));
+    double **got = (double **)calloc((size_t)p->nsys, sizeof(double *));
+    int rc = (ref && got) ? TRPDRV_OK : fail(TRPDRV_ERR_NOMEM, "host allocation failed");
+    for (int q = 0; q < p->nsys && rc == TRPDRV_OK; ++q) {
+        const size_t n = 4 * (size_t)(p->s[q].ntriples > 0 ? p->s[q].ntriples : 1);
+        ref[q] = (double *)calloc(n, sizeof(double));
+        got[q] = (double *)calloc(n, sizeof(double));
+        if (!ref[q] || !got[q]) rc = fail(TRPDRV_ERR_NOMEM, "host allocation failed");
+    }
+    int chosen = 8;
+    double dev = 0.0, prev = 0.0;
+    if (rc == TRPDRV_OK) rc = tune_set_slices(p, 8);
+    if (rc == TRPDRV_OK) rc = tune_sample_records(p, ref);
+    for (int sl = TRPDRV_OZ_MIN_SLICES; sl < 8 && rc == TRPDRV_OK; ++sl) {
+        rc = tune_set_slices(p, sl);
+        if (rc == TRPDRV_OK) rc = tune_sample_records(p, got);
+        if (rc != TRPDRV_OK) break;
+        dev = tune_record_dev(p, got, ref);
+        prev = dev;
+        if (dev <= target) {
+            chosen = sl;
+            break;
+        }
+    }
+    if (rc == TRPDRV_OK) {
+        rc = tune_set_slices(p, chosen);
+        /* 8 slices: its own deviation is about 2^-7 of 7 slices' */
+        *est = chosen == 8 ? prev / 128.0 : dev;
+    }
+    for (int q = 0; q < p->nsys; ++q) {
+        if (ref) free(ref[q]);
+        if (got) free(got[q]);
+    }
+    free(ref);
+    free(got);
+    return rc;
+}
+
 int trpdrv_plan_autotune(trpdrv_plan *p, trpdrv_tune_result *result)
 {
     trpdrv_tune_result local;
@@ -954,9 +1060,17 @@ int trpdrv_plan_autotune(trpdrv_plan *p, trpdrv_tune_result *result)
     CUDA_TRY(cudaSetDevice(p->device));
     p->events_valid = 0; /* the timing below reuses the plan's events */
 
+    double est = 0.0;
+    if (p->opt.mode == TRPDRV_MODE_EMULATED && p->opt.target_digits > 0) {
+        CUDA_TRY(cudaMemsetAsync(p->d_status, 0, sizeof(int), p->stream));
+        TRY(tune_choose_slices(p, &est));
+    }
+    r->slices = p->opt.mode == TRPDRV_MODE_EMULATED ? p->opt.slices : 0;
+    r->est_rel_err = est;
+
     tune_entry key;
     tune_key(p, &key);
-    const int cacheable = p->nsys <= TRPDRV_TMA_MAX_SYSTEMS;
+    const int cacheable = p->nsys <= TRPDRV_TMA_MAX_SYSTEMS && p->opt.target_digits == 0;
     if (cacheable) {
         pthread_mutex_lock(&g_tune_mu);
         int hit = -1;

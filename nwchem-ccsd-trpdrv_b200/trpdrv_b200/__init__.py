@@ -57,7 +57,8 @@ class OptionsStruct(C.Structure):
     _fields_ = [("mode", C.c_int), ("nkpass", C.c_int), ("rank", C.c_int), ("world", C.c_int),
                 ("device", C.c_int), ("tile", C.c_int), ("ctas_per_sm", C.c_int),
                 ("use_graph", C.c_int), ("mma_k", C.c_int), ("staging", C.c_int), ("slices", C.c_int),
-                ("batch", C.c_int), ("a_count", C.c_int), ("reserved", C.c_int * 3)]
+                ("batch", C.c_int), ("a_count", C.c_int), ("target_digits", C.c_int),
+                ("reserved", C.c_int * 2)]
 
 STAGING_AUTO, STAGING_CPASYNC, STAGING_TMA = 0, 1, 2
 
@@ -104,7 +105,8 @@ class TuneCandidate(C.Structure):
 
 
 class TuneResult(C.Structure):
-    _fields_ = [("ncand", C.c_int), ("chosen", C.c_int), ("from_cache", C.c_int), ("cand", TuneCandidate * 8)]
+    _fields_ = [("ncand", C.c_int), ("chosen", C.c_int), ("from_cache", C.c_int), ("cand", TuneCandidate * 8),
+                ("slices", C.c_int), ("est_rel_err", C.c_double)]
 
 
 _proto("trpdrv_plan_autotune", C.c_int, [C.c_void_p, C.POINTER(TuneResult)])
@@ -370,7 +372,7 @@ def tengy(f8: np.ndarray, vecs: Sequence[np.ndarray], eorb: np.ndarray, eaijk: f
 # plans
 # --------------------------------------------------------------------------------------------
 def options(mode=MODE_FUSED, nkpass=1, rank=0, world=1, device=-1, ctas_per_sm=0, use_graph=1,
-            mma_k=0, staging=STAGING_AUTO, slices=0, batch=0, a_count=1) -> OptionsStruct:
+            mma_k=0, staging=STAGING_AUTO, slices=0, batch=0, a_count=1, target_digits=0) -> OptionsStruct:
     o = OptionsStruct()
     lib.trpdrv_options_default(C.byref(o))
     o.mode, o.nkpass, o.rank, o.world, o.device = mode, nkpass, rank, world, device
@@ -382,6 +384,7 @@ def options(mode=MODE_FUSED, nkpass=1, rank=0, world=1, device=-1, ctas_per_sm=0
     if batch:
         o.batch = batch
     o.a_count = a_count
+    o.target_digits = target_digits
     return o
 
 
@@ -444,7 +447,8 @@ class Plan:
         _check(lib.trpdrv_plan_autotune(self.h, C.byref(r)))
         cands = [{"staging": c.staging, "mma_k": c.mma_k, "ctas_per_sm": c.ctas_per_sm, "batch": c.batch,
                   "ms_estimate": c.ms_estimate} for c in r.cand[:r.ncand]]
-        return {"candidates": cands, "chosen": r.chosen, "from_cache": bool(r.from_cache)}
+        return {"candidates": cands, "chosen": r.chosen, "from_cache": bool(r.from_cache), "slices": r.slices,
+                "est_rel_err": r.est_rel_err}
 
     def staging(self) -> int:
         """1 = cp.async, 2 = TMA staging in the fused kernel (0 for plain plans)."""

@@ -87,3 +87,24 @@ def test_emulated_rejects_bad_slice_counts(T):
         with pytest.raises(T.TrpdrvError) as ei:
             T.Plan([s], mode=T.MODE_EMULATED, slices=bad)
         assert ei.value.status == 1
+
+
+@pytest.mark.parametrize("name,digits", [("g_o10_v60", 12), ("g_o4_v30_log", 11), ("g_o4_v30_log", 13)])
+def test_target_digits_picks_the_fewest_slices_that_meet_it(T, name, digits):
+    g = load_golden(name)
+    s = system_from_golden(g)
+    with T.Plan([s], mode=T.MODE_EMULATED, nkpass=g["nkpass"], target_digits=digits) as p:
+        p.upload()
+        r = p.autotune()
+        assert 4 <= r["slices"] <= 8 and r["est_rel_err"] <= 10.0 ** -(digits + 1)
+        p.execute()
+        e4, e5 = p.energies()
+        rec = p.triple_energies(0)
+    assert_records_close(rec, g["records"], rtol=10.0 ** -digits)
+    assert_total_close(e4[0], g["emp4"], rtol=10.0 ** -digits, what="emp4")
+    # fewer slices than chosen would miss the target on the same records
+    if r["slices"] > 4:
+        _, _, recs, _ = _run(T, [s], nkpass=g["nkpass"], slices=r["slices"] - 1)
+        ref = np.asarray(g["records"])
+        dev = np.max(np.abs(recs[0] - ref)) / np.max(np.abs(ref))
+        assert dev > 10.0 ** -(digits + 2)

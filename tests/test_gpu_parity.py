@@ -282,3 +282,25 @@ def test_tma_and_cpasync_stagings_agree(T):
     a = _plan_run(T, [s], mode=1, staging=2)
     b = _plan_run(T, [s], mode=1, staging=1, mma_k=8)
     assert_records_close(a[2][0], b[2][0], rtol=1e-13)
+
+
+@pytest.mark.parametrize("mode,extra", [(1, {}), (0, {}), (2, {"slices": 8})])
+def test_one_call_run_equals_the_plan(T, mode, extra):
+    systems = [T.synth_system(4, 30, seed=91), T.synth_system(5, 22, seed=92, ncor=1)]
+    e4, e5 = T.run(systems, mode=mode, **extra)
+    p4, p5, _, _ = _plan_run(T, systems, mode=mode, **extra)
+    assert np.array_equal(e4, p4) and np.array_equal(e5, p5)
+
+
+def test_more_systems_than_tma_maps_fall_back_to_cpasync(T):
+    # even sizes: each alone could use TMA; nine exceed the 8 tensor-map sets a TMA launch carries
+    systems = [T.synth_system(2 + 2 * (q % 2), 16 + 2 * q, seed=100 + q) for q in range(9)]
+    with T.Plan(systems, mode=1) as p:
+        p.upload()
+        p.execute()
+        e4, e5 = p.energies()
+        recs = [p.triple_energies(q) for q in range(9)]
+        assert p.staging() == 1
+    for q, s in enumerate(systems):
+        a4, a5, arec, _ = _plan_run(T, [s], mode=1, staging=1)
+        assert np.array_equal(recs[q], arec[0]) and e4[q] == a4[0] and e5[q] == a5[0]

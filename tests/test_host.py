@@ -174,3 +174,14 @@ def test_register_host_checks_arguments_first(T):
     assert T.lib.trpdrv_register_host(None, 8) == 1
     assert T.lib.trpdrv_refresh_host(None) == 1
     assert T.lib.trpdrv_unregister_host(None) == 1
+
+
+def test_size_limits_are_checked_before_device_use(T):
+    s = T.synth_system(2, 8, seed=1)
+    for nocc, nvir in ((1024, 8), (2, 16385), (0, 8), (2, 0)):
+        with pytest.raises(T.TrpdrvError) as ei:
+            T.Plan([T.System(0, nocc, nvir, 1, s.arrays)])
+        assert ei.value.status == 1
+    with pytest.raises(T.TrpdrvError) as ei:
+        T.Plan([s], mode=T.MODE_EMULATED, target_digits=16)
+    assert ei.value.status == 1

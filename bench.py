@@ -22,6 +22,8 @@ nocc=40, nvir=300 (32,800 triples, 16.06 TFLOP per step), seeded synthetic input
 --workload c3: the emulated form at nocc=30, nvir=400 with log-uniform integral magnitudes in
   [1e-6, 1]: `value` = triples/s of the emulated form (7 slices), beside the native FP64 fused kernel
   on the same system and the slice sweep with its errors.
+--workload c1: the plain per-triple FP64 path (one grouped 16-GEMM launch and one tengy launch per
+  triple) at nocc=20, nvir=200, every triple per step, beside the reference's CPU body.
 --workload c4: six systems of uneven size, (8,80) (12,150) (16,220) (24,310) (32,380) (40,450), in
   one fused FP64 launch: `value` = aggregate triples/s; per-system energies checked against
   single-system plans; compared with one plain FP64 launch pair per triple, serially per system.
@@ -43,6 +45,7 @@ sys.path.insert(0, os.path.join(ROOT, "nwchem-ccsd-trpdrv_b200"))
 
 METRIC = "(T) triples/s & FP64-equiv TFLOP/s, fused/emulated vs plain FP64 GPU"
 NOCC, NVIR, SEED = 40, 300, 2024
+C1 = (20, 200)
 C3 = (30, 400)
 C4 = [(8, 80), (12, 150), (16, 220), (24, 310), (32, 380), (40, 450)]
 SLICES = (5, 6, 7, 8)
@@ -61,7 +64,7 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--mma-k", type=int, default=8, choices=[4, 8], help="FP64 MMA shape of the fused kernel")
-    ap.add_argument("--workload", default="c2", choices=["c2", "c3", "c4"])
+    ap.add_argument("--workload", default="c2", choices=["c1", "c2", "c3", "c4"])
     ap.add_argument("--no-emulated", action="store_true", help="skip the emulated-FP64 sweep of the default line")
     ap.add_argument("--profile", action="store_true",
                     help="the timed plan only (c2/c4: fused FP64; c3: emulated, 7 slices), no probes, e2e, plain "
@@ -70,7 +73,7 @@ def parse():
     if args.profile:
         args.no_cpu_baseline = args.no_plain = True
         args.no_emulated = args.workload != "c3"
-    dn, dv = C3 if args.workload == "c3" else (NOCC, NVIR)
+    dn, dv = {"c1": C1, "c3": C3}.get(args.workload, (NOCC, NVIR))
     args.nocc = dn if args.nocc is None else args.nocc
     args.nvir = dv if args.nvir is None else args.nvir
     return args
@@ -465,6 +468,49 @@ def fp64_roofline(achieved, peak, traffic, kms):
             "kernel_ms": kms}
 
 
+def run_c1(args, T, R, systems, in_bytes, n_all, flop_all, probe, cublas_dgemm, fp64_probe, peak):
+    """the plain per-triple path on every triple of (20, 200), checked against the fused
+    FP64 kernel on the same inputs (both are checked against the reference by the tests)."""
+    with T.Plan(systems, mode=T.MODE_PLAIN, rank=R.rank, world=R.world, device=R.local) as p:
+        p.upload(stream=R.sp)
+        clocks = ClockSampler(R.local)
+        clocks.start()
+        time.sleep(0.3)
+        sec, kms, launches, e4, e5 = time_plan(T, R, p, args.steps, args.warmup)
+        ck = clocks.stop()
+        rec = p.triple_energies(0)
+        my_flop = p.num_triples(0) * T.triple_flops(args.nocc, args.nvir)
+        e2e_sec = None if args.profile else time_e2e(T, R, p, args.steps, args.warmup)
+    with T.Plan(systems, mode=T.MODE_FUSED, rank=R.rank, world=R.world, device=R.local) as f:
+        f.upload(stream=R.sp)
+        fsec, _, _, f4, f5 = time_plan(T, R, f, 1, 1)
+        frec = f.triple_energies(0)
+    dev = float(np.max(np.abs(rec - frec) / np.maximum(np.max(np.abs(frec), axis=0), 1e-300)))
+    if R.rank != 0:
+        R.close()
+        return
+    cfg = {"workload": f"plain per-triple FP64 path (one grouped 16-GEMM launch + one tengy launch per triple), "
+                       f"nocc={args.nocc} nvir={args.nvir}, all {n_all} (i,j,k) triples of one a per step",
+           "nocc": args.nocc, "nvir": args.nvir, "triples_per_step": n_all,
+           "flop_per_triple": T.triple_flops(args.nocc, args.nvir),
+           "l2": "inputs (0.17 GB) exceed the 126 MB L2; no flush between steps",
+           "parallelism": f"triples sharded over {R.world} rank(s), one 2-double all-reduce per step"}
+    achieved = my_flop / (kms * 1e-3) / 1e12
+    line = base_line(args, R, n_all / sec, sec, cfg)
+    line.update({
+        "dtype": "f64", "tflops_fp64_equiv": flop_all / sec / 1e12,
+        "roofline": fp64_roofline(achieved, peak, None, kms), "fp64_probe_tflops": fp64_probe,
+        "e2e": {"value": (n_all / e2e_sec) if e2e_sec else None, "unit": "triples/s", "h2d_bytes_per_step": in_bytes,
+                "d2h_bytes_per_step": 16,
+                "path": "trpdrv_plan_upload (pinned host) + trpdrv_plan_execute + trpdrv_plan_energies"},
+        "gpu_launches": launches, "clocks": ck, "emp4": e4[0], "emp5": e5[0],
+        "fused_fp64": {"value": n_all / fsec, "unit": "triples/s", "records_max_rel_dev_vs_plain": dev},
+        "cpu_baseline": cpu_leg(args, R, args.nocc, args.nvir),
+    })
+    print(json.dumps(line), flush=True)
+    R.close()
+
+
 def run_b200_arm(args):
     import trpdrv_b200 as T
     R = Ranks()
@@ -490,6 +536,10 @@ def run_b200_arm(args):
     peak = max(max(probe.values()), cublas_dgemm) or 1.0
     fp64_probe = {"dmma_m16n8k4": probe[1], "dmma_m16n8k8": probe[2], "dmma_m16n8k16": probe[3],
                   "dfma": probe[4], "cublas_dgemm_8192": cublas_dgemm}
+
+    if args.workload == "c1":
+        run_c1(args, T, R, systems, in_bytes, n_all, flop_all, probe, cublas_dgemm, fp64_probe, peak)
+        return
 
     if args.profile and args.workload == "c3":
         with T.Plan(systems, mode=T.MODE_EMULATED, slices=DEFAULT_SLICES, rank=R.rank, world=R.world,

@@ -3,8 +3,9 @@
  *
  * Part 1 exports the reference's own entry points with the reference's exact signatures, so the
  * reference driver (omp/test.c) and Fortran/C callers link against this library unchanged.
- * Part 2 is the batched interface: whole systems (every (i,j,k) triple of one `a`) resident on the
- * device, run by one persistent fused kernel, by a plain per-triple path, or sharded over ranks.
+ * Part 2 is the batched interface: whole systems (every (i,j,k) triple of one `a`, or of a range of
+ * `a` with options.a_count) resident on the device, run by one persistent fused FP64 kernel, by the
+ * emulated-FP64 int8 form, or by a plain per-triple path, optionally sharded over ranks.
  *
  * Conventions: all real data is IEEE double; integers are 32-bit unless typed otherwise; orbital
  * indices in the reference entry points are 1-based (Fortran convention, as in the reference).
@@ -208,7 +209,9 @@ int trpdrv_plan_execute(trpdrv_plan *plan, void *stream);
 /* Waits for the job and returns this rank's per-system totals emp4[s], emp5[s] (compensated sums
  * of emp4i + [i!=k] emp4k over the rank's triples).  Either output may be NULL. */
 int trpdrv_plan_energies(trpdrv_plan *plan, double *emp4, double *emp5);
-/* This rank's triples of system `sys`, in processing order: ijk[3*t..] = i, j, k (1-based). */
+/* This rank's records of system `sys`: n_a * (its triples), a-major; trpdrv_plan_triples writes the
+ * triple of record t, ijk[3*t..] = i, j, k (1-based), in the driver order of this rank's share (the
+ * same for every a). */
 int64_t trpdrv_plan_num_triples(const trpdrv_plan *plan, int sys);
 int trpdrv_plan_triples(const trpdrv_plan *plan, int sys, int32_t *ijk);
 /* Per-triple records of system `sys` after a job: rec[4*t..] = emp4i, emp5i, emp4k, emp5k. */

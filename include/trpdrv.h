@@ -227,7 +227,7 @@ int trpdrv_plan_destroy(trpdrv_plan *plan);
 
 /* Autotuner: times every compiled variant of the plan's mode on a sample of the plan's own work and
  * keeps the fastest (FUSED: TMA vs cp.async staging, FP64 MMA shape m16n8k8 vs m16n8k4, CTAs per SM;
- * EMULATED: triples per launch pair, 4 / 8 / 16).  Needs a bound plan (after upload or bind); each
+ * EMULATED: triples per launch pair, 4 / 8 / 16 / 32).  Needs a bound plan (after upload or bind); each
  * system is sampled (about 1/8 of its fused items, 64 triples in the emulated form) and the per-
  * system times are scaled to its full work.  EMULATED plans with target_digits first pick the fewest
  * slices (4..8) that meet the accuracy target on the same sample.  The choice is cached per device and set of shapes for

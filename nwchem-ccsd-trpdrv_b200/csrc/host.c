@@ -165,7 +165,7 @@ static int pack_triple(int i, int j, int k) { return (i - 1) | ((j - 1) << 10) |
 /* plans                                                                                        */
 /* ------------------------------------------------------------------------------------------ */
 
-#define TUNE_MAX_BATCH 16 /* largest emulated batch the autotuner tries */
+#define TUNE_MAX_BATCH 32 /* largest emulated batch the autotuner tries */
 
 typedef struct sysbuf {
     trpdrv_system shape;
@@ -929,7 +929,9 @@ static int tune_time(trpdrv_plan *p, const trpdrv_tune_candidate *c, double *est
             *est += (double)ms * (double)items / (double)sample;
         } else {
             const sysbuf *b = &p->s[q];
-            const int64_t n = d->ntriples < 64 ? d->ntriples : 64;
+            /* four launch pairs of the largest batch, so every candidate is timed over several launches */
+            const int64_t want = 4 * (int64_t)TUNE_MAX_BATCH;
+            const int64_t n = d->ntriples < want ? d->ntriples : want;
             LAUNCH_TRY(trpdrv_launch_oz_slices(d, &b->oz, st));
             for (int rep = 0; rep < 2; ++rep) {
                 CUDA_TRY(cudaEventRecord(p->ev0, st));
@@ -1107,8 +1109,8 @@ int trpdrv_plan_autotune(trpdrv_plan *p, trpdrv_tune_result *result)
             if (occ > 1) c[n++] = (trpdrv_tune_candidate){1, 8, 1, 0, 0.0};
         }
     } else {
-        static const int batches[3] = {4, 8, 16};
-        for (int k = 0; k < 3; ++k)
+        static const int batches[4] = {4, 8, 16, 32};
+        for (int k = 0; k < 4; ++k)
             if (batches[k] <= p->fbuf_batch) c[n++] = (trpdrv_tune_candidate){0, 0, 0, batches[k], 0.0};
     }
     r->ncand = n;

@@ -79,10 +79,21 @@ def parse():
     return args
 
 
-def workload(nocc, nvir):
+def workload_text(name, nocc, nvir):
     n = nocc * nocc * (nocc + 1) // 2
-    return {"workload": f"fused persistent FP64 triples body, nocc={nocc} nvir={nvir}, all {n} (i,j,k) triples of "
-                        f"one a per step", "nocc": nocc, "nvir": nvir, "triples_per_step": n,
+    if name == "c1":
+        return (f"plain per-triple FP64 path (one grouped 16-GEMM launch + one tengy launch per triple), "
+                f"nocc={nocc} nvir={nvir}, all {n} (i,j,k) triples of one a per step")
+    if name == "c3":
+        return (f"emulated-FP64 triples body (Ozaki int8 digit slices on tcgen05, {DEFAULT_SLICES} slices, "
+                f"FP64 energies), nocc={nocc} nvir={nvir}, log-uniform integral magnitudes in [1e-6, 1], "
+                f"all {n} (i,j,k) triples of one a per step")
+    return f"fused persistent FP64 triples body, nocc={nocc} nvir={nvir}, all {n} (i,j,k) triples of one a per step"
+
+
+def workload(nocc, nvir, name="c2"):
+    n = nocc * nocc * (nocc + 1) // 2
+    return {"workload": workload_text(name, nocc, nvir), "nocc": nocc, "nvir": nvir, "triples_per_step": n,
             "flop_per_triple": 16.0 * nvir * nvir * (nvir + nocc),
             "l2": "inputs resident in HBM exceed the 126 MB L2; no flush between steps"}
 
@@ -141,7 +152,7 @@ def run_reference_arm(args):
         if step >= args.warmup:
             vals.append(n_all / sec)
     value = statistics.median(vals)
-    cfg = workload(args.nocc, args.nvir) if args.workload != "c4" else {
+    cfg = workload(args.nocc, args.nvir, args.workload) if args.workload != "c4" else {
         "workload": "six systems of uneven size: " + ", ".join(f"({o},{v})" for o, v in C4),
         "triples_per_step": n_all, "flop_per_step": flop_all}
     line = {
@@ -489,8 +500,7 @@ def run_c1(args, T, R, systems, in_bytes, n_all, flop_all, probe, cublas_dgemm, 
     if R.rank != 0:
         R.close()
         return
-    cfg = {"workload": f"plain per-triple FP64 path (one grouped 16-GEMM launch + one tengy launch per triple), "
-                       f"nocc={args.nocc} nvir={args.nvir}, all {n_all} (i,j,k) triples of one a per step",
+    cfg = {"workload": workload_text("c1", args.nocc, args.nvir),
            "nocc": args.nocc, "nvir": args.nvir, "triples_per_step": n_all,
            "flop_per_triple": T.triple_flops(args.nocc, args.nvir),
            "l2": "inputs (0.17 GB) exceed the 126 MB L2; no flush between steps",
@@ -618,9 +628,7 @@ def run_b200_arm(args):
         emu = emulated[str(DEFAULT_SLICES)] if emulated else None
         value = emu["value"] if emu else n_all / sec
         wsec = (emu["ms_per_step"] * 1e-3) if emu else sec
-        cfg = {"workload": f"emulated-FP64 triples body (Ozaki int8 digit slices on tcgen05, {DEFAULT_SLICES} slices, "
-                           f"FP64 energies), nocc={args.nocc} nvir={args.nvir}, log-uniform integral magnitudes "
-                           f"in [1e-6, 1], all {n_all} (i,j,k) triples of one a per step",
+        cfg = {"workload": workload_text("c3", args.nocc, args.nvir),
                "nocc": args.nocc, "nvir": args.nvir, "triples_per_step": n_all, "slices": DEFAULT_SLICES,
                "flop_per_triple": T.triple_flops(args.nocc, args.nvir),
                "l2": "inputs resident in HBM exceed the 126 MB L2; no flush between steps",

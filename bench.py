@@ -27,8 +27,10 @@ nocc=40, nvir=300 (32,800 triples, 16.06 TFLOP per step), seeded synthetic input
 --workload c4: six systems of uneven size, (8,80) (12,150) (16,220) (24,310) (32,380) (40,450), in
   one fused FP64 launch: `value` = aggregate triples/s; per-system energies checked against
   single-system plans; compared with one plain FP64 launch pair per triple, serially per system.
-With torchrun (N > 1) the triples are split over ranks (strong scaling) and the two energies are summed
-with one NCCL all-reduce per step.
+With torchrun (N > 1) every rank runs the whole workload for its own virtual index a (weak scaling: the
+a loop of the full (T) is what partitions into independent units; `value` counts the triples of all
+ranks), and one NCCL all-reduce of the energies per step sums the ranks' (T) contributions.  With
+--scaling strong the triples of one a are split over the ranks instead.
 """
 import argparse
 import json
@@ -65,6 +67,9 @@ def parse():
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--mma-k", type=int, default=8, choices=[4, 8], help="FP64 MMA shape of the fused kernel")
     ap.add_argument("--workload", default="c2", choices=["c1", "c2", "c3", "c4"])
+    ap.add_argument("--scaling", default="weak", choices=["weak", "strong"],
+                    help="N > 1: weak = every rank runs the whole workload for its own virtual index a (the "
+                         "outer loop of the full (T)); strong = the triples of one a are split over the ranks")
     ap.add_argument("--no-emulated", action="store_true", help="skip the emulated-FP64 sweep of the default line")
     ap.add_argument("--profile", action="store_true",
                     help="the timed plan only (c2/c4: fused FP64; c3: emulated, 7 slices), no probes, e2e, plain "
@@ -248,6 +253,13 @@ class Ranks:
         self.stream = torch.cuda.Stream(device=self.dev)
         self.sp = self.stream.cuda_stream
         assert self.sp != 0
+        self.set_scaling("strong")
+
+    def set_scaling(self, scaling):
+        """weak: each rank's plans take the whole workload (for its own a); strong: plans split it."""
+        self.weak = scaling == "weak"
+        self.shard = dict(rank=0, world=1) if self.weak else dict(rank=self.rank, world=self.world)
+        self.mult = self.world if self.weak else 1  # workloads per step, summed over ranks
 
     def barrier(self):
         if self.world > 1:
@@ -367,10 +379,10 @@ def emulated_sweep(T, R, systems, ref_e4, ref_e5, steps, warmup, slice_list, int
     """The emulated form on the same systems for each slice count: triples/s, FP64-equivalent TFLOP/s,
     int8 tensor-pipe rate and its error against the native FP64 fused result."""
     out = {}
-    n_all = sum(T.count_triples(s.nocc) for s in systems)
-    flop = sum(T.count_triples(s.nocc) * T.triple_flops(s.nocc, s.nvir) for s in systems)
+    n_all = R.mult * sum(T.count_triples(s.nocc) for s in systems)  # every rank's triples
+    flop = R.mult * sum(T.count_triples(s.nocc) * T.triple_flops(s.nocc, s.nvir) for s in systems)
     for sl in slice_list:
-        with T.Plan(systems, mode=T.MODE_EMULATED, slices=sl, rank=R.rank, world=R.world, device=R.local) as p:
+        with T.Plan(systems, mode=T.MODE_EMULATED, slices=sl, **R.shard, device=R.local) as p:
             p.upload(stream=R.sp)
             tune = p.autotune()
             sec, kms, launches, e4, e5 = time_plan(T, R, p, steps, warmup)
@@ -386,7 +398,7 @@ def emulated_sweep(T, R, systems, ref_e4, ref_e5, steps, warmup, slice_list, int
                         "fp64_roofline_frac": (flop / sec / 1e12) / fp64_peak if fp64_peak else None,
                         "batch": tune["candidates"][tune["chosen"]]["batch"]}
     # the accuracy target of the north star (1e-11 relative): the autotuner picks the slice count
-    with T.Plan(systems, mode=T.MODE_EMULATED, target_digits=TARGET_DIGITS, rank=R.rank, world=R.world,
+    with T.Plan(systems, mode=T.MODE_EMULATED, target_digits=TARGET_DIGITS, **R.shard,
                 device=R.local) as p:
         p.upload(stream=R.sp)
         tune = p.autotune()
@@ -463,9 +475,17 @@ def cpu_leg(args, R, nocc, nvir):
                 "sample": f"unavailable: {ex}"}
 
 
+def parallelism(R, nsys=1):
+    if R.weak:
+        return (f"{R.world} rank(s), each running the whole workload for its own virtual index a (weak scaling); "
+                f"one all-reduce of {2 * nsys} doubles per step sums the (T) contributions")
+    return f"triples sharded over {R.world} rank(s), one all-reduce of {2 * nsys} doubles per step"
+
+
 def base_line(args, R, value, sec, config):
     return {"metric": METRIC, "value": value, "unit": "triples/s", "n_gpus": R.world, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": 1e3 * sec, "higher_is_better": True, "scaling": "strong",
+            "warmup": args.warmup, "ms_per_step": 1e3 * sec, "higher_is_better": True,
+            "scaling": "weak" if R.weak else "strong",
             "vs_baseline": None, "data": "synthetic (seeded counter-based generator, reference config distributions)",
             "config": config}
 
@@ -482,7 +502,7 @@ def fp64_roofline(achieved, peak, traffic, kms):
 def run_c1(args, T, R, systems, in_bytes, n_all, flop_all, probe, cublas_dgemm, fp64_probe, peak):
     """the plain per-triple path on every triple of (20, 200), checked against the fused
     FP64 kernel on the same inputs (both are checked against the reference by the tests)."""
-    with T.Plan(systems, mode=T.MODE_PLAIN, rank=R.rank, world=R.world, device=R.local) as p:
+    with T.Plan(systems, mode=T.MODE_PLAIN, **R.shard, device=R.local) as p:
         p.upload(stream=R.sp)
         clocks = ClockSampler(R.local)
         clocks.start()
@@ -492,7 +512,7 @@ def run_c1(args, T, R, systems, in_bytes, n_all, flop_all, probe, cublas_dgemm, 
         rec = p.triple_energies(0)
         my_flop = p.num_triples(0) * T.triple_flops(args.nocc, args.nvir)
         e2e_sec = None if args.profile else time_e2e(T, R, p, args.steps, args.warmup)
-    with T.Plan(systems, mode=T.MODE_FUSED, rank=R.rank, world=R.world, device=R.local) as f:
+    with T.Plan(systems, mode=T.MODE_FUSED, **R.shard, device=R.local) as f:
         f.upload(stream=R.sp)
         fsec, _, _, f4, f5 = time_plan(T, R, f, 1, 1)
         frec = f.triple_energies(0)
@@ -504,7 +524,7 @@ def run_c1(args, T, R, systems, in_bytes, n_all, flop_all, probe, cublas_dgemm, 
            "nocc": args.nocc, "nvir": args.nvir, "triples_per_step": n_all,
            "flop_per_triple": T.triple_flops(args.nocc, args.nvir),
            "l2": "inputs (0.17 GB) exceed the 126 MB L2; no flush between steps",
-           "parallelism": f"triples sharded over {R.world} rank(s), one 2-double all-reduce per step"}
+           "parallelism": parallelism(R)}
     achieved = my_flop / (kms * 1e-3) / 1e12
     line = base_line(args, R, n_all / sec, sec, cfg)
     line.update({
@@ -524,6 +544,10 @@ def run_c1(args, T, R, systems, in_bytes, n_all, flop_all, probe, cublas_dgemm, 
 def run_b200_arm(args):
     import trpdrv_b200 as T
     R = Ranks()
+    R.set_scaling(args.scaling)
+    # weak scaling: rank r runs the workload for its own virtual index (a = first virtual + r), whose
+    # a-dependent integrals come from its own seed; rank 0 is the N = 1 workload
+    off = R.rank if R.weak else 0
 
     # inputs in pinned host memory (the e2e leg copies them every step)
     pinned = []
@@ -534,13 +558,16 @@ def run_b200_arm(args):
         return t.numpy()
 
     if args.workload == "c4":
-        systems = [T.synth_system(o, v, seed=SEED + q, alloc=alloc) for q, (o, v) in enumerate(C4)]
+        systems = [T.synth_system(o, v, seed=SEED + q + 97 * off, a=o + 1 + off, alloc=alloc)
+                   for q, (o, v) in enumerate(C4)]
     else:
         dist = T.DIST_LOGUNIFORM if args.workload == "c3" else T.DIST_UNIFORM
-        systems = [T.synth_system(args.nocc, args.nvir, seed=SEED, dist=dist, alloc=alloc)]
+        systems = [T.synth_system(args.nocc, args.nvir, seed=SEED + 97 * off, a=args.nocc + 1 + off, dist=dist,
+                                  alloc=alloc)]
     in_bytes = sum(s.nbytes() for s in systems)
-    n_all = sum(T.count_triples(s.nocc) for s in systems)
-    flop_all = sum(T.count_triples(s.nocc) * T.triple_flops(s.nocc, s.nvir) for s in systems)
+    # triples and FLOPs of one step over all ranks
+    n_all = R.mult * sum(T.count_triples(s.nocc) for s in systems)
+    flop_all = R.mult * sum(T.count_triples(s.nocc) * T.triple_flops(s.nocc, s.nvir) for s in systems)
 
     probe, cublas_dgemm, int8_peak = measure_peaks(T, R, args.profile)
     peak = max(max(probe.values()), cublas_dgemm) or 1.0
@@ -552,7 +579,7 @@ def run_b200_arm(args):
         return
 
     if args.profile and args.workload == "c3":
-        with T.Plan(systems, mode=T.MODE_EMULATED, slices=DEFAULT_SLICES, rank=R.rank, world=R.world,
+        with T.Plan(systems, mode=T.MODE_EMULATED, slices=DEFAULT_SLICES, **R.shard,
                     device=R.local) as p:
             p.upload(stream=R.sp)
             sec, kms, launches, e4, e5 = time_plan(T, R, p, args.steps, args.warmup)
@@ -563,7 +590,7 @@ def run_b200_arm(args):
         return
 
     # the native FP64 fused kernel (the headline of c2 and c4, the comparison of c3)
-    plan = T.Plan(systems, mode=T.MODE_FUSED, rank=R.rank, world=R.world, device=R.local, mma_k=args.mma_k)
+    plan = T.Plan(systems, mode=T.MODE_FUSED, **R.shard, device=R.local, mma_k=args.mma_k)
     plan.upload(stream=R.sp)
     tune = None if args.profile else plan.autotune()  # outside the timed region
     my_flop = sum(plan.num_triples(q) * T.triple_flops(s.nocc, s.nvir) for q, s in enumerate(systems))
@@ -582,7 +609,7 @@ def run_b200_arm(args):
     if args.workload == "c4":
         singles = []
         for q, s in enumerate(systems):
-            with T.Plan([s], mode=T.MODE_FUSED, rank=R.rank, world=R.world, device=R.local) as p1:
+            with T.Plan([s], mode=T.MODE_FUSED, **R.shard, device=R.local) as p1:
                 p1.upload(stream=R.sp)
                 _, _, _, a4, a5 = time_plan(T, R, p1, 1, 0)
             singles.append(bool(a4[0] == e4[q] and a5[0] == e5[q]))
@@ -601,7 +628,7 @@ def run_b200_arm(args):
             ck = clocks.stop()
     emu_e2e_sec = None
     if args.workload == "c3" and not args.no_emulated:
-        with T.Plan(systems, mode=T.MODE_EMULATED, slices=DEFAULT_SLICES, rank=R.rank, world=R.world,
+        with T.Plan(systems, mode=T.MODE_EMULATED, slices=DEFAULT_SLICES, **R.shard,
                     device=R.local) as p:
             p.upload(stream=R.sp)
             emu_e2e_sec = time_e2e(T, R, p, args.steps, args.warmup)
@@ -612,10 +639,10 @@ def run_b200_arm(args):
         if args.workload == "c4":
             per = [plain_sample(T, R, s, T.triple_flops(s.nocc, s.nvir), frac=32) for s in systems]
             serial_sec = sum(T.count_triples(s.nocc) / pl["value"] for s, pl in zip(systems, per))
-            plain = {"value": n_all / serial_sec, "unit": "triples/s",
+            plain = {"value": (n_all / R.mult) / serial_sec, "unit": "triples/s",  # one GPU
                      "sample": "1/32 of each system's triples, one grouped 16-GEMM launch + one tengy launch per "
                                "triple, systems one after another; serial time extrapolated by triple counts",
-                     "tflops_fp64_equiv": flop_all / serial_sec / 1e12, "per_system": per}
+                     "tflops_fp64_equiv": (flop_all / R.mult) / serial_sec / 1e12, "per_system": per}
         else:
             s = systems[0]
             plain = plain_sample(T, R, s, T.triple_flops(s.nocc, s.nvir))
@@ -632,7 +659,7 @@ def run_b200_arm(args):
                "nocc": args.nocc, "nvir": args.nvir, "triples_per_step": n_all, "slices": DEFAULT_SLICES,
                "flop_per_triple": T.triple_flops(args.nocc, args.nvir),
                "l2": "inputs resident in HBM exceed the 126 MB L2; no flush between steps",
-               "parallelism": f"triples sharded over {R.world} rank(s), one 2-double all-reduce per step"}
+               "parallelism": parallelism(R)}
         line = base_line(args, R, value, wsec, cfg)
         line.update({
             "dtype": "int8 (emulated f64)",
@@ -654,7 +681,7 @@ def run_b200_arm(args):
                     "path": "trpdrv_plan_upload (pinned host) + trpdrv_plan_execute + trpdrv_plan_energies"},
             "gpu_launches": emu["gpu_launches"] if emu else launches,
             "clocks": ck, "plain_gpu": plain,
-            "speedup_vs_plain": (value / plain["value"]) if plain else None,
+            "speedup_vs_plain": (value / R.world / plain["value"]) if plain else None,  # per GPU
             "cpu_baseline": cpu_leg(args, R, args.nocc, args.nvir),
         })
     else:
@@ -665,10 +692,10 @@ def run_b200_arm(args):
                    "systems": [{"nocc": s.nocc, "nvir": s.nvir, "triples": T.count_triples(s.nocc)} for s in systems],
                    "triples_per_step": n_all, "flop_per_step": flop_all,
                    "l2": "inputs resident in HBM exceed the 126 MB L2; no flush between steps",
-                   "parallelism": f"triples sharded over {R.world} rank(s), one all-reduce of 12 doubles per step"}
+                   "parallelism": parallelism(R, len(systems))}
         else:
             cfg = dict(workload(args.nocc, args.nvir),
-                       parallelism=f"triples sharded over {R.world} rank(s), one 2-double all-reduce per step")
+                       parallelism=parallelism(R))
         cfg["mma"] = f"m16n8k{args.mma_k} f64"
         line = base_line(args, R, value, sec, cfg)
         line.update({
@@ -682,7 +709,7 @@ def run_b200_arm(args):
             "gpu_launches": launches,
             "clocks": ck,
             "plain_gpu": plain,
-            "speedup_vs_plain": (value / plain["value"]) if plain else None,
+            "speedup_vs_plain": (value / R.world / plain["value"]) if plain else None,  # per GPU
             "autotune": tune,
         })
         if args.workload == "c4":
@@ -701,10 +728,10 @@ def run_b200_arm(args):
                 tgt = emulated["target"]
                 line["emulated"] = {"default_slices": DEFAULT_SLICES, "value": emu["value"], "unit": "triples/s",
                                     "speedup_vs_fp64_fused": emu["value"] / value,
-                                    "speedup_vs_plain": (emu["value"] / plain["value"]) if plain else None,
+                                    "speedup_vs_plain": (emu["value"] / R.world / plain["value"]) if plain else None,
                                     "at_target_1e-11": {"slices": tgt["slices"], "value": tgt["value"],
                                                         "speedup_vs_fp64_fused": tgt["value"] / value,
-                                                        "speedup_vs_plain": (tgt["value"] / plain["value"])
+                                                        "speedup_vs_plain": (tgt["value"] / R.world / plain["value"])
                                                         if plain else None},
                                     "int8_peak_tops": int8_peak, "slices": emulated}
     print(json.dumps(line), flush=True)

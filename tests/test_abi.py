@@ -78,3 +78,18 @@ def test_header_compiles_as_c_and_cxx(tmp_path):
 def test_status_strings(T):
     for code in range(8):
         assert T.lib.trpdrv_status_string(code).decode()
+
+
+def _build_c_caller(out_dir):
+    lib_dir = os.path.join(ROOT, "nwchem-ccsd-trpdrv_b200", "lib")
+    exe = os.path.join(str(out_dir), "c_plan_caller")
+    subprocess.run(["gcc", "-std=c99", "-Wall", "-Wextra", "-Werror", "-I", os.path.join(ROOT, "include"),
+                    os.path.join(ROOT, "tests", "c_plan_caller.c"), "-o", exe, "-L", lib_dir, "-ltrpdrv_b200",
+                    "-Wl,-rpath," + lib_dir], check=True)
+    return exe
+
+
+def test_c_caller_of_the_plan_interface_compiles_and_links(tmp_path):
+    """A C99 program using the plan interface (tests/c_plan_caller.c) builds against the header and links
+    against libtrpdrv_b200.so; running it needs a GPU (tests/test_gpu_parity.py)."""
+    assert os.access(_build_c_caller(tmp_path), os.X_OK)

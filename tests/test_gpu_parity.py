@@ -304,3 +304,20 @@ def test_more_systems_than_tma_maps_fall_back_to_cpasync(T):
     for q, s in enumerate(systems):
         a4, a5, arec, _ = _plan_run(T, [s], mode=1, staging=1)
         assert np.array_equal(recs[q], arec[0]) and e4[q] == a4[0] and e5[q] == a5[0]
+
+
+def test_c_caller_of_the_plan_interface_gives_the_python_plan_energies(T, tmp_path):
+    """tests/c_plan_caller.c (synthetic inputs, fused plan, autotune, execute) prints the energies the
+    Python binding's plan gives on the same seeded system."""
+    from test_abi import _build_c_caller
+    exe = _build_c_caller(tmp_path)
+    out = subprocess.run([exe, "6", "50", "77"], check=True, capture_output=True, text=True).stdout.split()
+    s = T.synth_system(6, 50, seed=77)
+    with T.Plan([s], mode=1) as p:
+        p.upload()
+        p.autotune()
+        p.execute()
+        e4, e5 = p.energies()
+    # each process autotunes for itself and may keep another variant: compare at the parity bar
+    assert_total_close(float(out[0]), e4[0], what="emp4")
+    assert_total_close(float(out[1]), e5[0], what="emp5")

@@ -8,7 +8,9 @@ nocc=40, nvir=300 (32,800 triples, 16.06 TFLOP per step), seeded synthetic input
 
 --impl b200 (default): `value` = triples/s of the fused kernel on device-resident inputs (CUDA events,
   max over ranks); `e2e` = the same metric through the C ABI with host buffers (pinned host -> device
-  copy of every input tensor, execute, device -> host read of the energies inside the timed region);
+  copy of every input tensor, execute, device -> host read of the energies inside the timed region;
+  one trpdrv_plan_upload_execute call, which copies T2/JOV/KOV span by span under the fused kernel,
+  with the upload-then-execute figure beside it);
   `roofline` = FP64 tensor-pipe fraction of the fused kernel against the FP64 DMMA peak measured live
   by the library's probe; `plain_gpu` = the plain per-triple GPU path (16 GEMMs + tengy per triple) on a
   bounded sample; `cpu_baseline` = the reference's own CPU body (oracle/_ref, OpenBLAS) on a bounded
@@ -347,9 +349,11 @@ def time_plan(T, R, plan, steps, warmup):
     return elapsed / steps, statistics.mean(kernel_ms), launches, tot[:n], tot[n:]
 
 
-def time_e2e(T, R, plan, steps, warmup):
-    """Through the C ABI with host buffers: pinned host -> device copy of every input (trpdrv_plan_upload),
-    execute, device -> host read of the energies; seconds per step, max over ranks."""
+def time_e2e(T, R, plan, steps, warmup, streamed=False):
+    """Through the C ABI with host buffers: pinned host -> device copy of every input, execute, device ->
+    host read of the energies; seconds per step, max over ranks.  streamed: one
+    trpdrv_plan_upload_execute call (T2/JOV/KOV copied span by span under the fused kernel), else
+    trpdrv_plan_upload then trpdrv_plan_execute."""
     torch = R.torch
     times = []
     for it in range(warmup + steps):
@@ -357,8 +361,11 @@ def time_e2e(T, R, plan, steps, warmup):
         R.barrier()
         t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         t0.record(R.stream)
-        plan.upload(stream=R.sp)
-        plan.execute(stream=R.sp)
+        if streamed:
+            plan.upload_execute(stream=R.sp)
+        else:
+            plan.upload(stream=R.sp)
+            plan.execute(stream=R.sp)
         e4, e5 = plan.energies()
         t1.record(R.stream)
         torch.cuda.synchronize()
@@ -601,9 +608,10 @@ def run_b200_arm(args):
         time.sleep(0.3)
     sec, kms, launches, e4, e5 = time_plan(T, R, plan, args.steps, args.warmup)
     ck = clocks.stop() if clocks else None
-    e2e_sec = None
+    e2e_sec = e2e_serial_sec = None
     if not args.profile and args.workload != "c3":
-        e2e_sec = time_e2e(T, R, plan, args.steps, args.warmup)
+        e2e_sec = time_e2e(T, R, plan, args.steps, args.warmup, streamed=True)
+        e2e_serial_sec = time_e2e(T, R, plan, args.steps, args.warmup)
     # per-system energies of the batch against single-system plans (c4)
     singles = None
     if args.workload == "c4":
@@ -705,7 +713,9 @@ def run_b200_arm(args):
             "fp64_probe_tflops": fp64_probe,
             "e2e": {"value": (n_all / e2e_sec) if e2e_sec else None, "unit": "triples/s",
                     "h2d_bytes_per_step": in_bytes, "d2h_bytes_per_step": 16 * len(systems),
-                    "path": "trpdrv_plan_upload (pinned host) + trpdrv_plan_execute + trpdrv_plan_energies"},
+                    "path": "trpdrv_plan_upload_execute (pinned host; T2/JOV/KOV copied span by span under "
+                            "the fused kernel) + trpdrv_plan_energies",
+                    "upload_then_execute": (n_all / e2e_serial_sec) if e2e_serial_sec else None},
             "gpu_launches": launches,
             "clocks": ck,
             "plain_gpu": plain,

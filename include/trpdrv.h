@@ -201,6 +201,15 @@ int trpdrv_plan_create(trpdrv_plan **plan, const trpdrv_system *shape, int nsys,
 /* Copies every host tensor of `host` (nsys entries, same shapes) into the plan's device storage
  * (host->device inside this call; pinned host memory makes it faster).  stream may be NULL. */
 int trpdrv_plan_upload(trpdrv_plan *plan, const trpdrv_system *host, void *stream);
+/* trpdrv_plan_upload followed by trpdrv_plan_execute, with the copies overlapped with the kernels
+ * (fused form).  The tensors every j reads (eorb, J, K, TOV, XOV, dintc, dintx, t1v) are copied
+ * first; T2, JOV and KOV, which a triple (i, j, k) reads only at block j, are copied on a second
+ * stream in `chunks` spans of the processing order (0 = 16), each span's kernel launch waiting only
+ * for its own j blocks.  Energies and records are bit-identical to upload + execute.  Other modes
+ * run upload + execute (the emulated form slices all of T2 before its first product).  The host
+ * tensors must stay unchanged until trpdrv_plan_energies returns; pinned host memory makes the
+ * copies asynchronous.  No counterpart in the reference (its driver has no device copies). */
+int trpdrv_plan_upload_execute(trpdrv_plan *plan, const trpdrv_system *host, int chunks, void *stream);
 /* Uses caller-owned DEVICE tensors instead (no copy).  They must stay valid until the next
  * upload/bind or destroy. */
 int trpdrv_plan_bind_device(trpdrv_plan *plan, const trpdrv_system *dev);
@@ -273,6 +282,13 @@ int64_t trpdrv_shard_triples(int nocc, int nkpass, int rank, int world, int32_t 
  * stretch of work touches fit in L2.  Writes the permutation order[position] = list index; returns
  * 0, or -1 on bad arguments.  block <= 0 selects the default (8). */
 int trpdrv_processing_order(const int32_t *ijk, int64_t n, int block, int32_t *order);
+/* The spans of a processing order (order[position] = list index, NULL = list order) that
+ * trpdrv_plan_upload_execute launches one by one: positions [bounds[s], bounds[s+1]) for
+ * s < the returned count (at most `chunks`; bounds needs chunks + 1 entries, bounds[0] = 0 and the
+ * last bound = n).  Span s ends at the first change of j at or after position (s+1)*n/chunks, so
+ * that a run of equal j is never split.  Returns -1 on bad arguments.  No counterpart in the
+ * reference. */
+int64_t trpdrv_upload_spans(const int32_t *ijk, const int32_t *order, int64_t n, int chunks, int64_t *bounds);
 /* Cost (FLOPs) of one triple of a system: 16*nvir*nvir*(nvir+nocc). */
 double trpdrv_triple_flops(int nocc, int nvir);
 

@@ -174,6 +174,7 @@ typedef struct sysbuf {
     double *ntov, *nxov;             /* -tov, -xov */
     int32_t *d_triples, *h_triples;
     int32_t *d_order;                /* fused/emulated processing order (trpdrv_processing_order) */
+    int32_t *h_order;                /* its host copy (chunks of trpdrv_plan_upload_execute) */
     trpdrv_oz_system oz;             /* emulated form: digit slices and scales (device) */
     void *oz_maps;                   /* emulated form: tensor maps of oz.sa / oz.sb (host blob) */
     int64_t ntriples;                /* records: n_a * nt */
@@ -207,6 +208,12 @@ struct trpdrv_plan {
     int fbuf_batch;     /* triples d_fbuf holds (>= opt.batch, and room for the autotuner's batches) */
     int tuned_staging;  /* FUSED staging chosen by the autotuner (1 cp.async, 2 TMA), 0 = none */
     void *tma_maps;     /* tensor maps of every system, passed by value to each launch */
+    /* trpdrv_plan_upload_execute: copy stream, one event per chunk, the chunks' first work items */
+    cudaStream_t copy_stream;
+    cudaEvent_t *chunk_ev, ev_in, ev_out;
+    int nchunk_ev;
+    unsigned long long *d_chunk_first, *h_chunk_first;
+    int nchunk_first;
 };
 
 void trpdrv_options_default(trpdrv_options *opt)
@@ -240,6 +247,7 @@ static void plan_free(trpdrv_plan *p)
             if (b->nxov) cudaFree(b->nxov);
             if (b->d_triples) cudaFree(b->d_triples);
             if (b->d_order) cudaFree(b->d_order);
+            free(b->h_order);
             if (b->oz.sa) cudaFree(b->oz.sa);
             if (b->oz.sb) cudaFree(b->oz.sb);
             if (b->oz.ea) cudaFree(b->oz.ea);
@@ -263,6 +271,13 @@ static void plan_free(trpdrv_plan *p)
     if (p->d_tcount) cudaFree(p->d_tcount);
     if (p->ev0) cudaEventDestroy(p->ev0);
     if (p->ev1) cudaEventDestroy(p->ev1);
+    for (int c = 0; c < p->nchunk_ev; ++c) cudaEventDestroy(p->chunk_ev[c]);
+    free(p->chunk_ev);
+    if (p->ev_in) cudaEventDestroy(p->ev_in);
+    if (p->ev_out) cudaEventDestroy(p->ev_out);
+    if (p->d_chunk_first) cudaFree(p->d_chunk_first);
+    free(p->h_chunk_first);
+    if (p->copy_stream) cudaStreamDestroy(p->copy_stream);
     if (p->stream) cudaStreamDestroy(p->stream);
     free(p);
 }
@@ -320,7 +335,7 @@ static int plan_build(trpdrv_plan *p, const trpdrv_system *shape)
             const cudaError_t e2 = e1 == cudaSuccess ? cudaMemcpy(b->d_order, order, sizeof(int32_t) * (size_t)n,
                                                                   cudaMemcpyHostToDevice)
                                                      : e1;
-            free(order);
+            b->h_order = order;
             CUDA_TRY(e2);
         }
 
@@ -524,26 +539,40 @@ static int plan_publish(trpdrv_plan *p)
     return TRPDRV_OK;
 }
 
-int trpdrv_plan_upload(trpdrv_plan *p, const trpdrv_system *host, void *stream)
+/* Elements of tensor w in the plan's device copy (a-dependent tensors hold n_a blocks). */
+static size_t upload_elems(const sysbuf *b, int w)
 {
-    if (!p || !host) return fail(TRPDRV_ERR_ARG, "NULL plan or systems");
-    CUDA_TRY(cudaSetDevice(p->device));
-    cudaStream_t st = stream ? (cudaStream_t)stream : p->stream;
+    return trpdrv_tensor_elems(w, b->shape.ncor, b->shape.nocc, b->shape.nvir) *
+           (trpdrv_tensor_a_dependent(w) ? (size_t)b->n_a : 1);
+}
+
+/* Checks `host` against the plan's shapes and allocates the owned device copies it will fill. */
+static int upload_prepare(trpdrv_plan *p, const trpdrv_system *host)
+{
     for (int q = 0; q < p->nsys; ++q) {
         sysbuf *b = &p->s[q];
         const trpdrv_system *h = &host[q];
         if (h->ncor != b->shape.ncor || h->nocc != b->shape.nocc || h->nvir != b->shape.nvir || h->a != b->shape.a)
             return fail(TRPDRV_ERR_ARG, "system %d: shape differs from the plan's", q);
         for (int w = 0; w < TRPDRV_T_COUNT; ++w) {
-            const double *src = sys_tensor(h, w);
-            if (!src) return fail(TRPDRV_ERR_ARG, "system %d: tensor %d is NULL", q, w);
-            const size_t n = trpdrv_tensor_elems(w, b->shape.ncor, b->shape.nocc, b->shape.nvir) *
-                             (trpdrv_tensor_a_dependent(w) ? (size_t)b->n_a : 1);
-            if (!b->own[w]) CUDA_TRY(cudaMalloc((void **)&b->own[w], sizeof(double) * n));
-            CUDA_TRY(cudaMemcpyAsync(b->own[w], src, sizeof(double) * n, cudaMemcpyHostToDevice, st));
+            if (!sys_tensor(h, w)) return fail(TRPDRV_ERR_ARG, "system %d: tensor %d is NULL", q, w);
+            if (!b->own[w]) CUDA_TRY(cudaMalloc((void **)&b->own[w], sizeof(double) * upload_elems(b, w)));
             b->t[w] = b->own[w];
         }
     }
+    return TRPDRV_OK;
+}
+
+int trpdrv_plan_upload(trpdrv_plan *p, const trpdrv_system *host, void *stream)
+{
+    if (!p || !host) return fail(TRPDRV_ERR_ARG, "NULL plan or systems");
+    CUDA_TRY(cudaSetDevice(p->device));
+    cudaStream_t st = stream ? (cudaStream_t)stream : p->stream;
+    TRY(upload_prepare(p, host));
+    for (int q = 0; q < p->nsys; ++q)
+        for (int w = 0; w < TRPDRV_T_COUNT; ++w)
+            CUDA_TRY(cudaMemcpyAsync(p->s[q].own[w], sys_tensor(&host[q], w), sizeof(double) * upload_elems(&p->s[q], w),
+                                     cudaMemcpyHostToDevice, st));
     if (st != p->stream) CUDA_TRY(cudaStreamSynchronize(st));
     return plan_publish(p);
 }
@@ -745,6 +774,249 @@ int trpdrv_plan_execute(trpdrv_plan *p, void *stream)
     } else {
         TRY(enqueue_device(p, st, 0));
     }
+    p->events_valid = 1;
+    return TRPDRV_OK;
+}
+
+/* ------------------------------------------------------------------------------------------ */
+/* upload overlapped with execution (fused form)                                                 */
+/* ------------------------------------------------------------------------------------------ */
+
+/* T2, JOV and KOV hold one block per j (T2[j][i], JOV[j][i], KOV[j][i]); a triple (i, j, k) reads
+ * only block j of each.  Every other tensor is read by every j. */
+static int tensor_j_blocked(int w) { return w == TRPDRV_T_T2 || w == TRPDRV_T_JOV || w == TRPDRV_T_KOV; }
+
+/* j (0-based) of the triple at processing position t of system b. */
+static int position_j(const sysbuf *b, int64_t t)
+{
+    const int32_t idx = b->h_order ? b->h_order[t] : (int32_t)t;
+    return (b->h_triples[idx] >> 10) & 1023;
+}
+
+/* One launch of the fused kernel over work items [first, end) of system q, preceded (for the
+ * positions [p0, p1) of the first a) by the copies of the j blocks they read first. */
+typedef struct chunk_span {
+    int q;
+    int64_t p0, p1;
+    int64_t first, end;
+} chunk_span;
+
+static int chunk_spans(const trpdrv_plan *p, int chunks, chunk_span **out, int *nout)
+{
+    int64_t cap = 0, maxnt = 1;
+    for (int q = 0; q < p->nsys; ++q) {
+        cap += chunks + 1;
+        if (p->s[q].nt > maxnt) maxnt = p->s[q].nt;
+    }
+    chunk_span *sp = (chunk_span *)malloc(sizeof(chunk_span) * (size_t)cap);
+    int32_t *ijk = (int32_t *)malloc(sizeof(int32_t) * 3 * (size_t)maxnt);
+    int64_t *bounds = (int64_t *)malloc(sizeof(int64_t) * ((size_t)chunks + 1));
+    if (!sp || !ijk || !bounds) {
+        free(sp);
+        free(ijk);
+        free(bounds);
+        return fail(TRPDRV_ERR_NOMEM, "host allocation failed");
+    }
+    int n = 0;
+    for (int q = 0; q < p->nsys; ++q) {
+        const sysbuf *b = &p->s[q];
+        const trpdrv_dev_system *d = &p->h_dev[q];
+        const int64_t nt = b->nt, np = b->npairs;
+        for (int64_t t = 0; t < nt; ++t) {
+            const int pk = b->h_triples[t];
+            ijk[3 * t] = (pk & 1023) + 1;
+            ijk[3 * t + 1] = ((pk >> 10) & 1023) + 1;
+            ijk[3 * t + 2] = ((pk >> 20) & 1023) + 1;
+        }
+        /* the first a's positions; the other a values read blocks that are all resident by then */
+        const int64_t ns = trpdrv_upload_spans(ijk, b->h_order, nt, chunks, bounds);
+        if (ns < 0) {
+            free(sp);
+            free(ijk);
+            free(bounds);
+            return fail(TRPDRV_ERR_ARG, "system %d: cannot split the processing order", q);
+        }
+        for (int64_t c = 0; c < ns; ++c)
+            sp[n++] = (chunk_span){q, bounds[c], bounds[c + 1], d->item_begin + bounds[c] * np,
+                                   d->item_begin + bounds[c + 1] * np};
+        if (b->n_a > 1 && nt > 0)
+            sp[n++] = (chunk_span){q, -1, -1, d->item_begin + nt * np, d->item_begin + b->ntriples * np};
+    }
+    free(ijk);
+    free(bounds);
+    *out = sp;
+    *nout = n;
+    return TRPDRV_OK;
+}
+
+static int span_resources(trpdrv_plan *p, int n)
+{
+    if (!p->copy_stream) CUDA_TRY(cudaStreamCreateWithFlags(&p->copy_stream, cudaStreamNonBlocking));
+    if (!p->ev_in) CUDA_TRY(cudaEventCreateWithFlags(&p->ev_in, cudaEventDisableTiming));
+    if (!p->ev_out) CUDA_TRY(cudaEventCreateWithFlags(&p->ev_out, cudaEventDisableTiming));
+    if (n > p->nchunk_ev) {
+        cudaEvent_t *ev = (cudaEvent_t *)realloc(p->chunk_ev, sizeof(cudaEvent_t) * (size_t)n);
+        if (!ev) return fail(TRPDRV_ERR_NOMEM, "host allocation failed");
+        p->chunk_ev = ev;
+        while (p->nchunk_ev < n) {
+            CUDA_TRY(cudaEventCreateWithFlags(&p->chunk_ev[p->nchunk_ev], cudaEventDisableTiming));
+            ++p->nchunk_ev;
+        }
+    }
+    if (n > p->nchunk_first) {
+        if (p->d_chunk_first) cudaFree(p->d_chunk_first);
+        free(p->h_chunk_first);
+        p->d_chunk_first = NULL;
+        p->nchunk_first = 0;
+        p->h_chunk_first = (unsigned long long *)malloc(sizeof(unsigned long long) * (size_t)n);
+        if (!p->h_chunk_first) return fail(TRPDRV_ERR_NOMEM, "host allocation failed");
+        CUDA_TRY(cudaMalloc((void **)&p->d_chunk_first, sizeof(unsigned long long) * (size_t)n));
+        p->nchunk_first = n;
+    }
+    return TRPDRV_OK;
+}
+
+/* Copies blocks j = lo .. hi-1 of T2, JOV and KOV of system q on the copy stream. */
+static int copy_j_blocks(trpdrv_plan *p, const trpdrv_system *host, int q, int lo, int hi)
+{
+    const sysbuf *b = &p->s[q];
+    for (int w = 0; w < TRPDRV_T_COUNT; ++w) {
+        if (!tensor_j_blocked(w)) continue;
+        const size_t blk = upload_elems(b, w) / (size_t)b->shape.nocc;
+        CUDA_TRY(cudaMemcpyAsync(b->own[w] + (size_t)lo * blk, sys_tensor(&host[q], w) + (size_t)lo * blk,
+                                 sizeof(double) * blk * (size_t)(hi - lo), cudaMemcpyHostToDevice, p->copy_stream));
+    }
+    return TRPDRV_OK;
+}
+
+/* Copies the j blocks that positions [p0, p1) of the span's system read and no earlier span of it
+ * copied (have[j] marks the copied ones), one copy per run of consecutive j. */
+static int span_copies(trpdrv_plan *p, const trpdrv_system *host, const chunk_span *c, unsigned char *have)
+{
+    const sysbuf *b = &p->s[c->q];
+    int lo = -1, hi = -1;
+    for (int64_t t = c->p0; t < c->p1; ++t) {
+        const int j = position_j(b, t);
+        if (have[j]) continue;
+        have[j] = 1;
+        if (j == hi) {
+            ++hi;
+            continue;
+        }
+        if (lo >= 0) TRY(copy_j_blocks(p, host, c->q, lo, hi));
+        lo = j;
+        hi = j + 1;
+    }
+    if (lo >= 0) TRY(copy_j_blocks(p, host, c->q, lo, hi));
+    return TRPDRV_OK;
+}
+
+int trpdrv_plan_upload_execute(trpdrv_plan *p, const trpdrv_system *host, int chunks, void *stream)
+{
+    if (!p || !host) return fail(TRPDRV_ERR_ARG, "NULL plan or systems");
+    if (chunks < 0 || chunks > 4096) return fail(TRPDRV_ERR_ARG, "chunks %d: must be 0..4096", chunks);
+    if (p->opt.mode != TRPDRV_MODE_FUSED) { /* every digit slice needs all of T2 first */
+        TRY(trpdrv_plan_upload(p, host, stream));
+        return trpdrv_plan_execute(p, stream);
+    }
+    if (chunks == 0) chunks = 16;
+    CUDA_TRY(cudaSetDevice(p->device));
+    cudaStream_t user = stream ? (cudaStream_t)stream : NULL;
+    TRY(upload_prepare(p, host));
+    chunk_span *sp = NULL;
+    int nsp = 0;
+    TRY(chunk_spans(p, chunks, &sp, &nsp));
+    int rc = span_resources(p, nsp > 0 ? nsp : 1);
+    unsigned char *have = NULL;
+    int maxo = 1;
+    for (int q = 0; q < p->nsys; ++q)
+        if (p->s[q].shape.nocc > maxo) maxo = p->s[q].shape.nocc;
+    if (rc == TRPDRV_OK && !(have = (unsigned char *)malloc((size_t)maxo)))
+        rc = fail(TRPDRV_ERR_NOMEM, "host allocation failed");
+#define STEP(call)                          \
+    do {                                    \
+        if (rc == TRPDRV_OK) rc = (call);   \
+    } while (0)
+#define STEP_CUDA(call)                                                                             \
+    do {                                                                                            \
+        if (rc == TRPDRV_OK) {                                                                      \
+            cudaError_t e_ = (call);                                                                \
+            if (e_ != cudaSuccess)                                                                  \
+                rc = fail(TRPDRV_ERR_CUDA, "%s: %s (%s:%d)", #call, cudaGetErrorString(e_), __FILE__, __LINE__); \
+        }                                                                                           \
+    } while (0)
+    /* both streams after the caller's stream and after the previous execution */
+    if (user) {
+        STEP_CUDA(cudaEventRecord(p->ev_in, user));
+        STEP_CUDA(cudaStreamWaitEvent(p->stream, p->ev_in, 0));
+    }
+    if (p->last_stream && p->last_stream != p->stream && p->last_stream != user) {
+        STEP_CUDA(cudaEventRecord(p->ev_in, p->last_stream));
+        STEP_CUDA(cudaStreamWaitEvent(p->stream, p->ev_in, 0));
+    }
+    STEP_CUDA(cudaEventRecord(p->ev_in, p->stream));
+    STEP_CUDA(cudaStreamWaitEvent(p->copy_stream, p->ev_in, 0));
+    /* the tensors every j reads, then the plan's derived arrays and tensor maps */
+    for (int q = 0; q < p->nsys && rc == TRPDRV_OK; ++q)
+        for (int w = 0; w < TRPDRV_T_COUNT; ++w)
+            if (!tensor_j_blocked(w))
+                STEP_CUDA(cudaMemcpyAsync(p->s[q].own[w], sys_tensor(&host[q], w),
+                                          sizeof(double) * upload_elems(&p->s[q], w), cudaMemcpyHostToDevice,
+                                          p->stream));
+    STEP(plan_publish(p));
+    /* per span: its j blocks on the copy stream, then the kernel over its items once they are in */
+    if (rc == TRPDRV_OK)
+        for (int c = 0; c < nsp; ++c) p->h_chunk_first[c] = (unsigned long long)sp[c].first;
+    STEP_CUDA(cudaMemsetAsync(p->d_status, 0, sizeof(int), p->stream));
+    STEP_CUDA(cudaMemsetAsync(p->d_tot, 0, sizeof(double) * 4 * (size_t)p->nsys, p->stream));
+    if (nsp > 0)
+        STEP_CUDA(cudaMemcpyAsync(p->d_chunk_first, p->h_chunk_first, sizeof(unsigned long long) * (size_t)nsp,
+                                  cudaMemcpyHostToDevice, p->stream));
+    STEP_CUDA(cudaEventRecord(p->ev0, p->stream));
+    int64_t launches = 0;
+    int prev_q = -1;
+    for (int c = 0; c < nsp && rc == TRPDRV_OK; ++c) {
+        if (sp[c].q != prev_q) {
+            memset(have, 0, (size_t)maxo);
+            prev_q = sp[c].q;
+        }
+        if (sp[c].p0 >= 0) {
+            STEP(span_copies(p, host, &sp[c], have));
+            STEP_CUDA(cudaEventRecord(p->chunk_ev[c], p->copy_stream));
+            STEP_CUDA(cudaStreamWaitEvent(p->stream, p->chunk_ev[c], 0));
+        }
+        const int64_t n = sp[c].end - sp[c].first;
+        const int cap = p->use_tma ? p->grid_tma : p->grid;
+        const int grid = (int64_t)cap < n ? cap : (int)n;
+        if (n <= 0 || rc != TRPDRV_OK) continue;
+        int e = p->use_tma ? trpdrv_launch_fused_tma(p->d_dev, p->nsys, sp[c].end, p->d_chunk_first + c, p->d_status,
+                                                     grid, p->tma_maps, p->stream)
+                           : trpdrv_launch_fused(p->d_dev, p->nsys, sp[c].end, p->d_chunk_first + c, p->d_status,
+                                                 grid, p->vec2, p->opt.mma_k, p->stream);
+        if (e) rc = fail(TRPDRV_ERR_CUDA, "fused launch of span %d: %s", c, cudaGetErrorString((cudaError_t)e));
+        ++launches;
+    }
+    STEP_CUDA(cudaEventRecord(p->ev1, p->stream));
+    for (int q = 0; q < p->nsys && rc == TRPDRV_OK; ++q) {
+        if (p->h_dev[q].ntriples <= 0) continue;
+        int e = trpdrv_launch_item_reduce(&p->h_dev[q], p->stream);
+        if (!e)
+            e = trpdrv_launch_system_reduce(p->s[q].rec, p->s[q].d_triples, p->s[q].ntriples, p->s[q].nt,
+                                            p->d_tot + 4 * q, p->stream);
+        if (e) rc = fail(TRPDRV_ERR_CUDA, "reduction launch: %s", cudaGetErrorString((cudaError_t)e));
+        launches += 2;
+    }
+    if (user) {
+        STEP_CUDA(cudaEventRecord(p->ev_out, p->stream));
+        STEP_CUDA(cudaStreamWaitEvent(user, p->ev_out, 0));
+    }
+#undef STEP
+#undef STEP_CUDA
+    free(have);
+    free(sp);
+    if (rc != TRPDRV_OK) return rc;
+    p->last_launches = launches;
+    p->last_stream = user ? user : p->stream;
     p->events_valid = 1;
     return TRPDRV_OK;
 }
@@ -1154,8 +1426,7 @@ int trpdrv_run(const trpdrv_system *host, int nsys, const trpdrv_options *opt, d
 {
     trpdrv_plan *p = NULL;
     TRY(trpdrv_plan_create(&p, host, nsys, opt));
-    int rc = trpdrv_plan_upload(p, host, NULL);
-    if (rc == TRPDRV_OK) rc = trpdrv_plan_execute(p, NULL);
+    int rc = trpdrv_plan_upload_execute(p, host, 0, NULL);
     if (rc == TRPDRV_OK) rc = trpdrv_plan_energies(p, emp4, emp5);
     trpdrv_plan_destroy(p);
     return rc;

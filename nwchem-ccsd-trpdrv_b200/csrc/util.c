@@ -143,6 +143,26 @@ int trpdrv_processing_order(const int32_t *ijk, int64_t n, int block, int32_t *o
     return 0;
 }
 
+int64_t trpdrv_upload_spans(const int32_t *ijk, const int32_t *order, int64_t n, int chunks, int64_t *bounds)
+{
+    if (n < 0 || n > INT32_MAX || chunks < 1 || !bounds || (n > 0 && !ijk)) return -1;
+    if (order)
+        for (int64_t t = 0; t < n; ++t)
+            if (order[t] < 0 || order[t] >= n) return -1;
+    int64_t ns = 0, start = 0;
+    bounds[0] = 0;
+    for (int c = 0; c < chunks && start < n; ++c) {
+        int64_t end = c + 1 == chunks ? n : (int64_t)(c + 1) * n / chunks;
+        if (end <= start) end = start + 1;
+        while (end < n && ijk[3 * (int64_t)(order ? order[end] : end) + 1] ==
+                              ijk[3 * (int64_t)(order ? order[end - 1] : end - 1) + 1])
+            ++end;
+        bounds[++ns] = end;
+        start = end;
+    }
+    return ns;
+}
+
 double trpdrv_triple_flops(int nocc, int nvir)
 {
     return 16.0 * (double)nvir * (double)nvir * ((double)nvir + (double)nocc);

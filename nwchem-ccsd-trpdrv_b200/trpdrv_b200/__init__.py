@@ -89,6 +89,7 @@ _proto("trpdrv_options_default", None, [C.POINTER(OptionsStruct)])
 _proto("trpdrv_plan_create", C.c_int, [C.POINTER(C.c_void_p), C.POINTER(SystemStruct), C.c_int,
                                        C.POINTER(OptionsStruct)])
 _proto("trpdrv_plan_upload", C.c_int, [C.c_void_p, C.POINTER(SystemStruct), C.c_void_p])
+_proto("trpdrv_plan_upload_execute", C.c_int, [C.c_void_p, C.POINTER(SystemStruct), C.c_int, C.c_void_p])
 _proto("trpdrv_plan_bind_device", C.c_int, [C.c_void_p, C.POINTER(SystemStruct)])
 _proto("trpdrv_plan_execute", C.c_int, [C.c_void_p, C.c_void_p])
 _proto("trpdrv_plan_energies", C.c_int, [C.c_void_p, _dp, _dp])
@@ -119,6 +120,8 @@ _proto("trpdrv_partition", C.c_int, [_dp, C.c_int64, C.c_int, C.POINTER(C.c_int6
 _proto("trpdrv_shard_triples", C.c_int64, [C.c_int, C.c_int, C.c_int, C.c_int, C.POINTER(C.c_int32)])
 _proto("trpdrv_tensor_a_dependent", C.c_int, [C.c_int])
 _proto("trpdrv_processing_order", C.c_int, [C.POINTER(C.c_int32), C.c_int64, C.c_int, C.POINTER(C.c_int32)])
+_proto("trpdrv_upload_spans", C.c_int64,
+       [C.POINTER(C.c_int32), C.POINTER(C.c_int32), C.c_int64, C.c_int, C.POINTER(C.c_int64)])
 _proto("trpdrv_triple_flops", C.c_double, [C.c_int, C.c_int])
 _proto("trpdrv_tensor_elems", C.c_size_t, [C.c_int, C.c_int, C.c_int, C.c_int])
 _proto("trpdrv_synth_fill", C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int, C.c_uint64, C.c_int, _dp,
@@ -202,6 +205,20 @@ def processing_order(ijk: np.ndarray, block: int = 0) -> np.ndarray:
     if rc != 0:
         raise TrpdrvError(1, "processing_order: bad arguments")
     return out[:len(a)]
+
+
+def upload_spans(ijk: np.ndarray, order: Optional[np.ndarray], chunks: int) -> np.ndarray:
+    """Span bounds (positions of the processing order) that trpdrv_plan_upload_execute launches one by
+    one: spans are [b[s], b[s+1])."""
+    a = np.ascontiguousarray(ijk, dtype=np.int32).reshape(-1, 3)
+    o = None if order is None else np.ascontiguousarray(order, dtype=np.int32)
+    out = np.zeros(max(chunks, 0) + 1, dtype=np.int64)
+    ns = lib.trpdrv_upload_spans(a.ctypes.data_as(C.POINTER(C.c_int32)),
+                                 None if o is None else o.ctypes.data_as(C.POINTER(C.c_int32)), len(a), chunks,
+                                 out.ctypes.data_as(C.POINTER(C.c_int64)))
+    if ns < 0:
+        raise TrpdrvError(1, "upload_spans: bad arguments")
+    return out[:ns + 1]
 
 
 def triple_flops(nocc: int, nvir: int) -> float:
@@ -410,6 +427,13 @@ class Plan:
         systems = self.systems if systems is None else systems
         arr = (SystemStruct * len(systems))(*[s.struct() for s in systems])
         _check(lib.trpdrv_plan_upload(self.h, arr, C.c_void_p(stream) if stream else None))
+
+    def upload_execute(self, systems: Optional[Sequence[System]] = None, chunks: int = 0, stream: int = 0):
+        """trpdrv_plan_upload_execute: upload and execute with the T2/JOV/KOV copies overlapped with the
+        fused kernel, j range by j range."""
+        systems = self.systems if systems is None else systems
+        arr = (SystemStruct * len(systems))(*[s.struct() for s in systems])
+        _check(lib.trpdrv_plan_upload_execute(self.h, arr, chunks, C.c_void_p(stream) if stream else None))
 
     def bind_device(self, ptrs: Sequence[dict]):
         arr = (SystemStruct * len(self.systems))(*[s.struct(p) for s, p in zip(self.systems, ptrs)])

@@ -136,6 +136,42 @@ def test_processing_order_rejects_bad_arguments(T):
     assert len(T.processing_order(np.zeros((0, 3), np.int32))) == 0
 
 
+@pytest.mark.parametrize("nocc,nkpass,world,chunks", [(40, 1, 1, 16), (40, 1, 1, 1), (40, 1, 1, 100),
+                                                       (13, 3, 1, 5), (17, 1, 3, 4), (2, 1, 1, 16)])
+def test_upload_spans_cover_the_order_and_never_split_a_j_run(T, nocc, nkpass, world, chunks):
+    """The spans trpdrv_plan_upload_execute launches one by one: contiguous, covering every position,
+    at most `chunks`, each ending where j changes, and (one k pass) each reading a j range of its own."""
+    for rank in range(world):
+        ijk = T.shard_triples(nocc, nkpass, rank, world)
+        order = T.processing_order(ijk)
+        b = T.upload_spans(ijk, order, chunks)
+        n = len(ijk)
+        assert b[0] == 0 and b[-1] == n and np.all(np.diff(b) > 0) and len(b) - 1 <= chunks
+        js = ijk[order, 1]
+        for e in b[1:-1]:
+            assert js[e] != js[e - 1]
+        if nkpass == 1:  # j rises along the order: the spans' j ranges are disjoint and ascending
+            ranges = [(js[lo], js[hi - 1]) for lo, hi in zip(b[:-1], b[1:])]
+            assert all(r0[1] < r1[0] for r0, r1 in zip(ranges[:-1], ranges[1:]))
+        if chunks >= len(np.unique(js)) and nkpass == 1:
+            assert len(b) - 1 == len(np.unique(js))  # one span per j when chunks allow
+    # list order (no permutation) and the empty list
+    ijk = T.shard_triples(6, 1, 0, 1)
+    assert np.array_equal(T.upload_spans(ijk, None, 6), np.concatenate([[0], np.cumsum(np.arange(1, 7) * 0 + 21)]))
+    assert list(T.upload_spans(np.zeros((0, 3), np.int32), None, 4)) == [0]
+
+
+def test_upload_spans_reject_bad_arguments(T):
+    ijk = T.shard_triples(5, 1, 0, 1)
+    with pytest.raises(T.TrpdrvError):
+        T.upload_spans(ijk, None, 0)
+    bad = T.processing_order(ijk)
+    bad[3] = len(ijk)  # not a position of the list
+    with pytest.raises(T.TrpdrvError):
+        T.upload_spans(ijk, bad, 4)
+    assert T.lib.trpdrv_plan_upload_execute(None, None, 0, None) == 1
+
+
 def test_autotune_rejects_a_null_plan(T):
     import ctypes as C
     r = T.TuneResult()

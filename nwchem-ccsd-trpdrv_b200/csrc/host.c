@@ -1025,6 +1025,7 @@ static int plan_wait(trpdrv_plan *p)
 {
     CUDA_TRY(cudaSetDevice(p->device));
     CUDA_TRY(cudaStreamSynchronize(p->last_stream ? p->last_stream : p->stream));
+    p->last_stream = NULL; /* the job is done: the caller may now destroy its stream */
     int status = 0;
     CUDA_TRY(cudaMemcpy(&status, p->d_status, sizeof(int), cudaMemcpyDeviceToHost));
     if (status & 2) return fail(TRPDRV_ERR_DEVICE, "a fused-kernel pipeline wait ran out of time");

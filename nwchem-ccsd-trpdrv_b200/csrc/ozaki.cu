@@ -576,16 +576,19 @@ __global__ void __launch_bounds__(TNTHREAD) oz_tengy_kernel(const TengyParams P)
     const size_t lnvv = (size_t)nvir * nvir;
     const double *f = P.fbuf + (size_t)blockIdx.y * 8 * lnvv;
 
-    // park f(B,C) (o = 0) and f(C,B) (o = 1) tiles of all eight f; column q of a tile is contiguous in f
+    // park f(B,C) (o = 0) and f(C,B) (o = 1) tiles of all eight f; column q of a tile is contiguous in f.
+    // Every copy of a thread is issued before any is waited for (cp.async, zero fill outside nvir), so
+    // that a CTA keeps its whole 32 KB in flight instead of one load per thread.
     const int ntiles = diag ? 8 : 16;
     for (int idx = tid; idx < ntiles * TW * TW; idx += TNTHREAD) {
         const int tile = idx / (TW * TW), q = (idx / TW) % TW, r = idx % TW;
         const int o = tile >> 3, xf = tile & 7;
         const int row = (o ? c0 : b0) + r, col = (o ? b0 : c0) + q;
-        double v = 0.0;
-        if (row < nvir && col < nvir) v = f[(size_t)xf * lnvv + row + (size_t)col * nvir];
-        park[tile * TILE + r * TP + q] = v;
+        const bool ok = row < nvir && col < nvir;
+        cp_async_8(park + tile * TILE + r * TP + q, ok ? f + (size_t)xf * lnvv + row + (size_t)col * nvir : f, ok);
     }
+    cp_async_commit();
+    cp_async_wait<0>();
     __syncthreads();
 
     TengyVecs v;

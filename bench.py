@@ -404,7 +404,7 @@ def emulated_sweep(T, R, systems, ref_e4, ref_e5, steps, warmup, slice_list, int
                         "emp4_rel_err_vs_fp64": r4, "emp5_rel_err_vs_fp64": r5,
                         "fp64_roofline_frac": (flop / sec / 1e12) / fp64_peak if fp64_peak else None,
                         "batch": tune["candidates"][tune["chosen"]]["batch"]}
-    # the accuracy target of the north star (1e-11 relative): the autotuner picks the slice count
+    # the 1e-11 relative accuracy target on emp4 and emp5: the autotuner picks the slice count
     with T.Plan(systems, mode=T.MODE_EMULATED, target_digits=TARGET_DIGITS, **R.shard,
                 device=R.local) as p:
         p.upload(stream=R.sp)

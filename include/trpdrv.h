@@ -342,8 +342,8 @@ int trpdrv_probe_fp64_peak(int device, int kind, double *tflops);
 
 /* ---- inputs that do not change between drop-in calls ----
  * The drop-in entry points copy every input slice host -> device on each call, because the
- * reference's callers may refill their buffers between calls (SURVEY of the NWChem driver: the same
- * host buffers are refilled per (i, a) and (k, j) block).  A caller whose arrays stay fixed while
+ * reference's callers may refill their buffers between calls (the NWChem driver refills the same
+ * host buffers per (i, a) and (k, j) block).  A caller whose arrays stay fixed while
  * it loops over triples (omp/test.c:160-195 passes slices of arrays allocated once) registers them:
  * the library keeps a device copy of [ptr, ptr + bytes), and every drop-in pointer that lies inside
  * a registered array is read from that copy, with no per-call transfer.  After changing a registered

@@ -552,8 +552,9 @@ def run_b200_arm(args):
     import trpdrv_b200 as T
     R = Ranks()
     R.set_scaling(args.scaling)
-    # weak scaling: rank r runs the workload for its own virtual index (a = first virtual + r), whose
-    # a-dependent integrals come from its own seed; rank 0 is the N = 1 workload
+    # weak scaling: rank r runs the workload for its own virtual index a = first virtual + r of the same
+    # molecule (block r of the a sweep: its own J, K, dintc, dintx, t1v; T2, TOV, XOV, JOV, KOV and the
+    # orbital energies shared); rank 0 is the N = 1 workload
     off = R.rank if R.weak else 0
 
     # inputs in pinned host memory (the e2e leg copies them every step)
@@ -565,12 +566,12 @@ def run_b200_arm(args):
         return t.numpy()
 
     if args.workload == "c4":
-        systems = [T.synth_system(o, v, seed=SEED + q + 97 * off, a=o + 1 + off, alloc=alloc)
+        systems = [T.synth_system(o, v, seed=SEED + q, a=o + 1, alloc=alloc, a_block=off)
                    for q, (o, v) in enumerate(C4)]
     else:
         dist = T.DIST_LOGUNIFORM if args.workload == "c3" else T.DIST_UNIFORM
-        systems = [T.synth_system(args.nocc, args.nvir, seed=SEED + 97 * off, a=args.nocc + 1 + off, dist=dist,
-                                  alloc=alloc)]
+        systems = [T.synth_system(args.nocc, args.nvir, seed=SEED, a=args.nocc + 1, dist=dist, alloc=alloc,
+                                  a_block=off)]
     in_bytes = sum(s.nbytes() for s in systems)
     # triples and FLOPs of one step over all ranks
     n_all = R.mult * sum(T.count_triples(s.nocc) for s in systems)

@@ -275,21 +275,26 @@ class System:
 
 
 def synth_system(nocc: int, nvir: int, seed: int = 1, ncor: int = 0, dist: int = DIST_UNIFORM,
-                 a: Optional[int] = None, alloc=None, a_count: int = 1) -> System:
+                 a: Optional[int] = None, alloc=None, a_count: int = 1, a_block: int = 0) -> System:
     """Seeded synthetic system.  `a` defaults to the first virtual orbital (ncor+nocc+1), which keeps
     every denominator e_b + e_c + eaijk >= 2.1 under these distributions.  `alloc(n)` may return a
     preallocated (e.g. pinned) float64 buffer of n elements.  With a_count > 1 the a-dependent
     tensors get a_count blocks; block 0 is the a_count = 1 system's, block m is generated from seed
-    + 7919 m."""
+    + 7919 m.  a_block = m starts the sweep at its block m instead (virtual index a + m): with
+    a_count = 1 that is one a of the molecule, equal to synth_system(..., a_count=m+1).a_view(m)."""
     if a is None:
         a = ncor + nocc + 1
-    sysm = System(ncor, nocc, nvir, a, a_count=a_count)
+    if a_block < 0:
+        raise TrpdrvError(1, f"a_block {a_block}: must be >= 0")
+    sysm = System(ncor, nocc, nvir, a + a_block, a_count=a_count)
     for t, name in enumerate(TENSOR_NAMES):
         n = tensor_elems(t, ncor, nocc, nvir)
-        blocks = a_count if tensor_a_dependent(t) else 1
+        dep = tensor_a_dependent(t)
+        blocks = a_count if dep else 1
         buf = alloc(n * blocks) if alloc is not None else np.empty(n * blocks, dtype=np.float64)
         for m in range(blocks):
-            _check(lib.trpdrv_synth_fill(t, ncor, nocc, nvir, seed + 7919 * m, dist, _ptr(buf[m * n:]), n))
+            mm = m + a_block if dep else m
+            _check(lib.trpdrv_synth_fill(t, ncor, nocc, nvir, seed + 7919 * mm, dist, _ptr(buf[m * n:]), n))
         sysm.arrays[name] = buf
     return sysm
 

@@ -179,6 +179,20 @@ def test_autotune_rejects_a_null_plan(T):
     assert r.ncand == 0
 
 
+def test_a_block_generates_one_block_of_the_sweep(T):
+    sweep = T.synth_system(4, 20, seed=9, a_count=3)
+    for m in range(3):
+        one = T.synth_system(4, 20, seed=9, a_block=m)
+        v = sweep.a_view(m)
+        assert one.a == v.a == sweep.a + m and one.a_count == 1
+        for name in T.TENSOR_NAMES:
+            assert np.array_equal(one.arrays[name], v.arrays[name])
+    tail = T.synth_system(4, 20, seed=9, a_count=2, a_block=1)  # blocks 1 and 2 of the same sweep
+    assert np.array_equal(tail.a_view(1).arrays["jvv"], sweep.a_view(2).arrays["jvv"])
+    with pytest.raises(T.TrpdrvError):
+        T.synth_system(4, 20, seed=9, a_block=-1)
+
+
 def test_a_sweep_synthetic_blocks_and_views(T):
     one = T.synth_system(4, 20, seed=9)
     three = T.synth_system(4, 20, seed=9, a_count=3)

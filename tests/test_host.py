@@ -1,5 +1,7 @@
 """Host-side logic of the library (no GPU): triple enumeration, partitioning, shards, the synthetic
 generator, argument validation of the drop-in entry points and plan creation without a device."""
+import os
+
 import numpy as np
 import pytest
 
@@ -235,3 +237,26 @@ def test_size_limits_are_checked_before_device_use(T):
     with pytest.raises(T.TrpdrvError) as ei:
         T.Plan([s], mode=T.MODE_EMULATED, target_digits=16)
     assert ei.value.status == 1
+
+
+@pytest.mark.skipif(not os.path.exists(os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))),
+                                                    "oracle", "_ref", "libtrpdrv_ref.so")),
+                    reason="reference not built")
+def test_bench_reference_arm_prints_one_contract_line():
+    """`bench.py --impl reference` (the reference's CPU body on this host, no GPU needed) prints one JSON
+    line with the keys the benchmark contract asks of the reference arm."""
+    import json
+    import subprocess
+    import sys
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    out = subprocess.run([sys.executable, os.path.join(root, "bench.py"), "--impl", "reference", "--steps", "1",
+                          "--warmup", "0"], check=True, capture_output=True, text=True, timeout=600).stdout
+    lines = [l for l in out.splitlines() if l.startswith("{")]
+    assert len(lines) == 1
+    d = json.loads(lines[0])
+    assert d["impl"] == "reference" and d["unit"] == "triples/s" and d["higher_is_better"] is True
+    assert d["value"] > 0 and d["steps"] == 1 and d["n_gpus"] == 1
+    assert d["config"]["triples_per_step"] == 32800 and d["config"]["nocc"] == 40 and d["config"]["nvir"] == 300
+    assert d["cpu_baseline"]["kind"] == "reference" and d["cpu_baseline"]["value"] == d["value"]
+    assert d["cpu_baseline"]["cores"] >= 1
+    assert d["e2e"] == {"value": d["value"], "unit": "triples/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}

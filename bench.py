@@ -34,15 +34,20 @@ a loop of the full (T) is what partitions into independent units; `value` counts
 ranks), and one NCCL all-reduce of the energies per step sums the ranks' (T) contributions.  With
 --scaling strong the triples of one a are split over the ranks instead.
 """
-import argparse
-import json
 import os
-import statistics
-import subprocess
-import sys
-import time
 
-import numpy as np
+# The reference's CPU path (OpenMP tengy + OpenBLAS, serial body calls) is timed with a passive OpenMP
+# wait policy: libgomp reads its environment when it is first loaded, so this precedes every import.
+os.environ.setdefault("OMP_WAIT_POLICY", "passive")
+
+import argparse  # noqa: E402
+import json  # noqa: E402
+import statistics  # noqa: E402
+import subprocess  # noqa: E402
+import sys  # noqa: E402
+import time  # noqa: E402
+
+import numpy as np  # noqa: E402
 
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, os.path.join(ROOT, "nwchem-ccsd-trpdrv_b200"))
@@ -67,7 +72,7 @@ def parse():
     ap.add_argument("--nvir", type=int, default=None, help="default 300 (c2) / 400 (c3)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-plain", action="store_true")
-    ap.add_argument("--mma-k", type=int, default=8, choices=[4, 8], help="FP64 MMA shape of the fused kernel")
+    ap.add_argument("--mma-k", type=int, default=8, choices=[4, 8, 16], help="FP64 MMA shape of the fused kernel (before autotuning)")
     ap.add_argument("--workload", default="c2", choices=["c1", "c2", "c3", "c4"])
     ap.add_argument("--scaling", default="weak", choices=["weak", "strong"],
                     help="N > 1: weak = every rank runs the whole workload for its own virtual index a (the "
@@ -108,70 +113,110 @@ def workload(nocc, nvir, name="c2"):
 # ------------------------------------------------------------------------------------------------
 # CPU reference path (test infrastructure: oracle/_ref is the reference compiled unmodified)
 # ------------------------------------------------------------------------------------------------
-def time_reference_cpu(nocc, nvir, budget_s=12.0, max_triples=None):
+def time_reference_cpu(nocc, nvir, budget_s=12.0, seed=None, dist=0, min_triples=16):
     """Times the reference body (omp/ccsd_trpdrv_omp_cbody.c + omp/ccsd_tengy_c99.c, unmodified, OpenBLAS)
-    over consecutive triples of the synthetic system, serially as omp/test.c calls it, each call using
-    every host thread (OpenMP + OpenBLAS).  Returns (triples/s, triples timed, seconds, threads)."""
+    over consecutive triples of the synthetic system, serially as omp/test.c:160-195 calls it (the body
+    accumulates emp4/emp5 itself; nothing else runs), each call using every host thread (OpenMP +
+    OpenBLAS).  Inputs come from the oracle's restatement of the generator, so nothing of the product
+    is loaded.  Returns (triples/s, triples timed, seconds, threads)."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import ctypes as C
     import glob
     import oracle as O
-    import trpdrv_b200 as T
     ncpu = os.cpu_count() or 1
-    os.environ.setdefault("OMP_WAIT_POLICY", "passive")
-    R = O.ref()
+    O.ref()
     for so in glob.glob(os.path.join(O._scipy_libs(), "libscipy_openblas-*.so")):
         ob = C.CDLL(so)
         ob.scipy_openblas_set_num_threads.argtypes = [C.c_int]
         ob.scipy_openblas_set_num_threads(ncpu)
-    s = T.synth_system(nocc, nvir, seed=SEED)
-    O.run_system(s, "reference", t_begin=0, t_end=2, nthreads=1)  # warm-up (thread pools, pages)
+    s = O.synth_system(nocc, nvir, seed=SEED if seed is None else seed, dist=dist, a=nocc + 1)
+    O.time_body(s, "reference", t_begin=0, t_end=2)  # warm-up (thread pools, pages)
     n_all = nocc * nocc * (nocc + 1) // 2
-    done, t0, chunk = 0, time.perf_counter(), 8
+    done, t0, chunk = 0, time.perf_counter(), 4
+    e4 = e5 = 0.0
     while True:
         hi = min(n_all, done + chunk)
-        O.run_system(s, "reference", t_begin=done, t_end=hi, nthreads=1)
+        e4, e5 = O.time_body(s, "reference", t_begin=done, t_end=hi, emp4=e4, emp5=e5)
         done = hi
         el = time.perf_counter() - t0
-        if done >= n_all or el >= budget_s or (max_triples and done >= max_triples):
+        if done >= n_all or (el >= budget_s and done >= min_triples):
             break
-    del R
     return done / el, done, el, ncpu
+
+
+def workload_shapes(name, nocc, nvir):
+    """(nocc, nvir, seed, dist) of every system of a workload."""
+    if name == "c4":
+        return [(o, v, SEED + q, 0) for q, (o, v) in enumerate(C4)]
+    return [(nocc, nvir, SEED, 1 if name == "c3" else 0)]
+
+
+def parallelism_text(gpus, scaling, nsys=1):
+    if scaling == "weak":
+        return (f"{gpus} rank(s), each running the whole workload for its own virtual index a (weak scaling); "
+                f"one all-reduce of {2 * nsys} doubles per step sums the (T) contributions")
+    return f"triples sharded over {gpus} rank(s), one all-reduce of {2 * nsys} doubles per step"
+
+
+def config_for(args):
+    """The `config` object of the line, identical in both arms for the same arguments."""
+    shapes = workload_shapes(args.workload, args.nocc, args.nvir)
+    mult = args.gpus if args.scaling == "weak" else 1  # weak scaling: every rank runs the whole workload
+    counts = [mult * o * o * (o + 1) // 2 for o, _, _, _ in shapes]
+    l2 = "inputs resident in HBM exceed the 126 MB L2; no flush between steps"
+    if args.workload == "c4":
+        return {"workload": "fused persistent FP64 triples body over six systems of uneven size in one launch: "
+                            + ", ".join(f"({o},{v})" for o, v, _, _ in shapes) + f"; all {sum(counts)} triples of "
+                            f"one a each",
+                "systems": [{"nocc": o, "nvir": v, "triples": c} for (o, v, _, _), c in zip(shapes, counts)],
+                "triples_per_step": sum(counts),
+                "flop_per_step": sum(c * 16.0 * v * v * (v + o) for c, (o, v, _, _) in zip(counts, shapes)),
+                "l2": l2, "parallelism": parallelism_text(args.gpus, args.scaling, len(shapes))}
+    cfg = workload(args.nocc, args.nvir, args.workload)
+    cfg["triples_per_step"] = counts[0]
+    if args.workload == "c3":
+        cfg["slices"] = DEFAULT_SLICES
+    if args.workload == "c1":
+        cfg["l2"] = "inputs (0.17 GB) exceed the 126 MB L2; no flush between steps"
+    cfg["parallelism"] = parallelism_text(args.gpus, args.scaling)
+    return cfg
 
 
 def run_reference_arm(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    shapes = C4 if args.workload == "c4" else [(args.nocc, args.nvir)]
-    counts = [o * o * (o + 1) // 2 for o, _ in shapes]
-    n_all = sum(counts)
-    flop_all = sum(c * 16.0 * v * v * (v + o) for c, (o, v) in zip(counts, shapes))
-    budget = 8.0 / len(shapes)
-    vals, per_step = [], None
+    shapes = workload_shapes(args.workload, args.nocc, args.nvir)
+    counts = [o * o * (o + 1) // 2 for o, _, _, _ in shapes]
+    weights = [c * 16.0 * v * v * (v + o) for c, (o, v, _, _) in zip(counts, shapes)]
+    n_all, flop_all = sum(counts), sum(weights)
+    budget = 4.0 / len(shapes)
+    vals, secs, per_step = [], [], None
     for step in range(args.warmup + args.steps):
-        sec, timed, ncpu = 0.0, 0, os.cpu_count()
-        for c, (o, v) in zip(counts, shapes):
-            rate, n, el, ncpu = time_reference_cpu(o, v, budget_s=budget)
-            sec += c / rate  # the system's full triple count at the sampled rate
+        sec, sec_full, timed, ncpu = 0.0, 0.0, 0, os.cpu_count()
+        for c, (o, v, sd, dist) in zip(counts, shapes):
+            rate, n, el, ncpu = time_reference_cpu(o, v, budget_s=budget, seed=sd, dist=dist,
+                                                   min_triples=4 if len(shapes) > 1 else 16)
+            sec += el
+            sec_full += c / rate  # the system's full triple count at its sampled rate
             timed += n
         per_step = (timed, ncpu)
         if step >= args.warmup:
-            vals.append(n_all / sec)
+            vals.append(n_all / sec_full)
+            secs.append(sec)
     value = statistics.median(vals)
-    cfg = workload(args.nocc, args.nvir, args.workload) if args.workload != "c4" else {
-        "workload": "six systems of uneven size: " + ", ".join(f"({o},{v})" for o, v in C4),
-        "triples_per_step": n_all, "flop_per_step": flop_all}
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": "triples/s", "n_gpus": args.gpus,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * n_all / value,
-        "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "f64",
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * statistics.mean(secs),
+        "higher_is_better": True, "scaling": args.scaling, "vs_baseline": None, "dtype": "f64",
         "data": "synthetic (seeded counter-based generator, reference config distributions)",
-        "config": cfg,
+        "config": config_for(args),
         "cpu_baseline": {"value": value, "unit": "triples/s", "cores": per_step[1], "kind": "reference",
-                         "sample": f"{per_step[0]} consecutive triples per step (of {n_all}, every system sampled), "
-                                   f"serial calls of the reference body with {per_step[1]} OpenMP + OpenBLAS "
-                                   f"threads, ~8 s per step; ms_per_step extrapolates to the full workload"},
+                         "sample": f"each step: {per_step[0]} consecutive triples of the driver order (every "
+                                   f"system sampled, about {budget:.0f} s each), serial calls of the reference "
+                                   f"body with {per_step[1]} OpenMP (passive wait) + OpenBLAS threads; "
+                                   f"ms_per_step is the sampled step, value the full workload's triples over "
+                                   f"the time the sampled rate(s) give it"},
         "e2e": {"value": value, "unit": "triples/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
         "tflops_fp64_equiv": value * flop_all / n_all / 1e12,
     }
@@ -286,6 +331,20 @@ class Ranks:
             self.dist.destroy_process_group()
 
 
+def probe_fp64_peak(kind, device):
+    """TFLOP/s of the FP64 issue-rate probe (lib/libtrpdrv_probe.so, a measurement tool built beside the
+    library): kind 1..3 = DMMA m16n8k4/k8/k16 with register operands, 4 = scalar DFMA."""
+    import ctypes as C
+    lib = C.CDLL(os.path.join(ROOT, "nwchem-ccsd-trpdrv_b200", "lib", "libtrpdrv_probe.so"))
+    lib.trpdrv_probe_fp64_peak.argtypes = [C.c_int, C.c_int, C.POINTER(C.c_double)]
+    lib.trpdrv_probe_fp64_peak.restype = C.c_int
+    out = C.c_double()
+    rc = lib.trpdrv_probe_fp64_peak(device, kind, C.byref(out))
+    if rc:
+        raise RuntimeError(f"FP64 probe kind {kind} failed with CUDA error {rc}")
+    return out.value
+
+
 def measure_peaks(T, R, skip):
     """FP64: the library's probes (DMMA m16n8k4/k8/k16, DFMA) and cuBLAS DGEMM 8192^3; int8: cuBLASLt
     int8 GEMM 8192^3 (torch._int_mm), the denominator of the emulated form's tensor-pipe fraction."""
@@ -293,7 +352,7 @@ def measure_peaks(T, R, skip):
     probe, cublas_dgemm, int8 = {1: 0.0, 2: 0.0, 3: 0.0, 4: 0.0}, 0.0, None
     if skip:
         return probe, cublas_dgemm, int8
-    probe = {k: T.probe_fp64_peak(k, R.local) for k in (1, 2, 3, 4)}
+    probe = {k: probe_fp64_peak(k, R.local) for k in (1, 2, 3, 4)}
 
     def best_of(fn, flop, reps=3):
         fn()
@@ -482,13 +541,6 @@ def cpu_leg(args, R, nocc, nvir):
                 "sample": f"unavailable: {ex}"}
 
 
-def parallelism(R, nsys=1):
-    if R.weak:
-        return (f"{R.world} rank(s), each running the whole workload for its own virtual index a (weak scaling); "
-                f"one all-reduce of {2 * nsys} doubles per step sums the (T) contributions")
-    return f"triples sharded over {R.world} rank(s), one all-reduce of {2 * nsys} doubles per step"
-
-
 def base_line(args, R, value, sec, config):
     return {"metric": METRIC, "value": value, "unit": "triples/s", "n_gpus": R.world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": 1e3 * sec, "higher_is_better": True,
@@ -500,7 +552,7 @@ def base_line(args, R, value, sec, config):
 def fp64_roofline(achieved, peak, traffic, kms):
     return {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
             "traffic": traffic,
-            "peak_source": "measured live on this device: max of the library's FP64 probes (DMMA m16n8k4/k8/k16 "
+            "peak_source": "measured live on this device: max of the FP64 probes (lib/libtrpdrv_probe.so) (DMMA m16n8k4/k8/k16 "
                            "and DFMA, register operands, 50 ms bursts) and cuBLAS DGEMM 8192^3; "
                            "MEASURED_PEAKS.json has no FP64 entry",
             "kernel_ms": kms}
@@ -527,11 +579,7 @@ def run_c1(args, T, R, systems, in_bytes, n_all, flop_all, probe, cublas_dgemm, 
     if R.rank != 0:
         R.close()
         return
-    cfg = {"workload": workload_text("c1", args.nocc, args.nvir),
-           "nocc": args.nocc, "nvir": args.nvir, "triples_per_step": n_all,
-           "flop_per_triple": T.triple_flops(args.nocc, args.nvir),
-           "l2": "inputs (0.17 GB) exceed the 126 MB L2; no flush between steps",
-           "parallelism": parallelism(R)}
+    cfg = config_for(args)
     achieved = my_flop / (kms * 1e-3) / 1e12
     line = base_line(args, R, n_all / sec, sec, cfg)
     line.update({
@@ -664,11 +712,7 @@ def run_b200_arm(args):
         emu = emulated[str(DEFAULT_SLICES)] if emulated else None
         value = emu["value"] if emu else n_all / sec
         wsec = (emu["ms_per_step"] * 1e-3) if emu else sec
-        cfg = {"workload": workload_text("c3", args.nocc, args.nvir),
-               "nocc": args.nocc, "nvir": args.nvir, "triples_per_step": n_all, "slices": DEFAULT_SLICES,
-               "flop_per_triple": T.triple_flops(args.nocc, args.nvir),
-               "l2": "inputs resident in HBM exceed the 126 MB L2; no flush between steps",
-               "parallelism": parallelism(R)}
+        cfg = config_for(args)
         line = base_line(args, R, value, wsec, cfg)
         line.update({
             "dtype": "int8 (emulated f64)",
@@ -695,20 +739,10 @@ def run_b200_arm(args):
         })
     else:
         value = n_all / sec
-        if args.workload == "c4":
-            cfg = {"workload": "fused persistent FP64 triples body over six systems of uneven size in one launch: "
-                               + ", ".join(f"({o},{v})" for o, v in C4) + f"; all {n_all} triples of one a each",
-                   "systems": [{"nocc": s.nocc, "nvir": s.nvir, "triples": T.count_triples(s.nocc)} for s in systems],
-                   "triples_per_step": n_all, "flop_per_step": flop_all,
-                   "l2": "inputs resident in HBM exceed the 126 MB L2; no flush between steps",
-                   "parallelism": parallelism(R, len(systems))}
-        else:
-            cfg = dict(workload(args.nocc, args.nvir),
-                       parallelism=parallelism(R))
-        cfg["mma"] = f"m16n8k{args.mma_k} f64"
-        line = base_line(args, R, value, sec, cfg)
+        line = base_line(args, R, value, sec, config_for(args))
         line.update({
             "dtype": "f64",
+            "fused_mma": f"m16n8k{args.mma_k} f64",
             "tflops_fp64_equiv": flop_all / sec / 1e12,
             "roofline": fp64_roofline(achieved, peak, traffic, kms),
             "fp64_probe_tflops": fp64_probe,

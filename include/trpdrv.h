@@ -173,7 +173,9 @@ typedef struct trpdrv_options {
     int tile;         /* fused tile width (32 is the only compiled width); 0 = default */
     int ctas_per_sm;  /* fused persistent grid = ctas_per_sm * SM count; 0 = default */
     int use_graph;    /* capture trpdrv_plan_execute's launch sequence in a CUDA graph; default 1 */
-    int mma_k;        /* FP64 MMA shape of the cp.async fused kernel: 8 = m16n8k8 (default), 4 = m16n8k4 */
+    int mma_k;        /* FP64 MMA shape of the fused kernel: 8 = m16n8k8 (default); 16 = m16n8k16 (TMA
+                         staging only; cp.async staging then uses 8); 4 = m16n8k4 (cp.async staging only;
+                         TMA staging then uses 8) */
     int staging;      /* fused-kernel operand staging: 0 = TMA where supported (even nvir and nocc,
                          16-byte aligned tensors, <= 8 systems), else cp.async; 1 = cp.async; 2 = TMA
                          or fail with TRPDRV_ERR_UNSUPPORTED */
@@ -244,7 +246,7 @@ int trpdrv_plan_destroy(trpdrv_plan *plan);
  * in the reference (its BLAS call sites have nothing to tune).  `result` may be NULL. */
 typedef struct trpdrv_tune_candidate {
     int staging;          /* FUSED: 1 cp.async, 2 TMA; 0 otherwise */
-    int mma_k;            /* FUSED cp.async MMA shape */
+    int mma_k;            /* FUSED: FP64 MMA shape k (TMA: 8 or 16; cp.async: 4 or 8) */
     int ctas_per_sm;      /* FUSED cp.async grid */
     int batch;            /* EMULATED: triples per launch pair */
     double ms_estimate;   /* estimated device time of one execution with this candidate */
@@ -309,9 +311,10 @@ int trpdrv_synth_fill(int tensor, int ncor, int nocc, int nvir, uint64_t seed, i
                       double *out, size_t n);
 
 /* ---- one triple without device allocation ----
- * No counterpart in the reference.  For callers that cannot allocate device memory when they need
- * the work done: code inside a CUDA stream capture (cudaMalloc is not allowed there), code under a
- * device-memory budget fixed by its host application, or callers that own every device buffer.
+ * No counterpart in the reference.  For callers that cannot call cudaMalloc when they need the work
+ * done: a host application that reserves device memory up front in its own pool and gives libraries
+ * a fixed budget, a plug-in inside a framework that owns every device buffer, or a loop that cannot
+ * pay for an allocation (which may synchronise the device) on every call.
  * Runs the body of one triple (a,i,j,k) on DEVICE pointers that are already sliced for the triple
  * (tkj is the (k,j) block itself, not the k-chunk base; likewise jka, kka, tka, xka, jkj, kkj;
  * dintc2/dintx2/t1v2 are the k vectors) and writes out4[0..3] = emp4i, emp5i, emp4k, emp5k on the
@@ -320,7 +323,10 @@ int trpdrv_synth_fill(int tensor, int ncor, int nocc, int nvir, uint64_t seed, i
  * to nvir <= TRPDRV_NOALLOC_MAX_NVIR and nocc <= TRPDRV_NOALLOC_MAX_NOCC (larger sizes are
  * rejected with TRPDRV_ERR_ARG).  All calls on a device share that array: calls that overlap on
  * the GPU race and must be serialised by the caller.  The first call on each device looks up the
- * array and sets kernel attributes; make it before any stream capture. */
+ * array and sets kernel attributes; make it before any stream capture.  `a` may be any orbital
+ * 1..ncor+nocc+nvir, as in the reference body, whose own driver passes a = 1 (omp/test.c:162); a
+ * virtual a (> ncor+nocc) is the physical case.  A CUDA error already pending on the calling thread
+ * makes the call return TRPDRV_ERR_STATE without enqueuing anything (the error is left in place). */
 #define TRPDRV_NOALLOC_MAX_NVIR 256
 #define TRPDRV_NOALLOC_MAX_NOCC 64
 typedef struct trpdrv_body_device_args {
@@ -333,12 +339,6 @@ typedef struct trpdrv_body_device_args {
     double *out4;
 } trpdrv_body_device_args;
 int trpdrv_body_device_noalloc(const trpdrv_body_device_args *args, void *stream);
-
-/* ---- device probes ---- */
-
-/* FP64 issue-rate microbenchmark on `device`: kind 0 = DMMA m8n8k4, 1 = m16n8k4, 2 = m16n8k8,
- * 3 = m16n8k16, 4 = scalar DFMA.  Writes the achieved TFLOP/s. */
-int trpdrv_probe_fp64_peak(int device, int kind, double *tflops);
 
 /* ---- inputs that do not change between drop-in calls ----
  * The drop-in entry points copy every input slice host -> device on each call, because the

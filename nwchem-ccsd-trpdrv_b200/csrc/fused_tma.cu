@@ -19,6 +19,15 @@
 //    128-byte swizzled, read with 128-bit loads.
 // Every box row is a full 128-byte line: with 64-byte rows (DK = 8) the TMA request rate, not L2
 // bandwidth, bounded the staging at about half of this rate.
+// Fragment row/column labels are permuted, lane group g owning row (and column) PERM[g] of its 8,
+// PERM = {0,6,1,7,2,4,3,5}: the two rows a quarter-warp reads with one 128-bit load of an X-major
+// panel then differ in bit 2 (disjoint bank sets under the 128-byte swizzle) and the rows of one
+// 64-bit load of a K-major panel differ in bit 1 where they share bit 0, so no fragment read has a
+// bank conflict.  The permutation only relabels which (b, c) a register holds; the epilogue and the
+// diagonal exchange use the permuted coordinates.
+// The MMA shape is a template parameter: m16n8k8 (two k-steps per 16-index chunk) or m16n8k16,
+// whose fragments are exactly the two k8 fragments of the chunk side by side (lane t holds logical
+// k = t + 4q at physical index 2t + (q & 1) + 8 (q >> 1)).
 // The 3-D tensor maps ([system block][contraction][row]) give every dimension its own bound, so the
 // ragged tails in nvir and nocc are zero-filled by the TMA unit.
 //
@@ -138,6 +147,9 @@ __device__ __forceinline__ void tma_load_3d(void *dst, const CUtensorMap *map, u
 // Byte offsets of one thread's fragment elements inside a staged panel.  They depend only on the
 // thread's sub-block and lane, so they are computed once and every fragment read in the main loop is
 // a single shared load at (panel base + constant offset).
+// Row/column of its 8 that lane group g (0..7) owns (see the header): conflict-free fragment reads.
+__device__ __forceinline__ int perm8(int g) { return (0x53427160 >> (4 * g)) & 7; }
+
 __device__ __forceinline__ int kmajor_off(int kk, int x)
 {
     const int h = x >> 4, xi = x & 15;
@@ -151,15 +163,16 @@ struct FragOffsets {
     int xB;                  // X-major B fragment: column c at contraction 2t (128-bit)
     __device__ __forceinline__ FragOffsets(int rx0, int cx0, int g, int t)
     {
-        kA0 = kmajor_off(2 * t, rx0 + g);
-        kA1 = kmajor_off(2 * t, rx0 + g + 8);
-        kA2 = kmajor_off(2 * t + 1, rx0 + g);
-        kA3 = kmajor_off(2 * t + 1, rx0 + g + 8);
-        kB0 = kmajor_off(2 * t, cx0 + g);
-        kB1 = kmajor_off(2 * t + 1, cx0 + g);
-        xA0 = (rx0 + g) * 128 + ((t ^ ((rx0 + g) & 7)) << 4);
-        xA1 = (rx0 + g + 8) * 128 + ((t ^ ((rx0 + g + 8) & 7)) << 4);
-        xB = (cx0 + g) * 128 + ((t ^ ((cx0 + g) & 7)) << 4);
+        const int r = rx0 + perm8(g), c = cx0 + perm8(g);
+        kA0 = kmajor_off(2 * t, r);
+        kA1 = kmajor_off(2 * t, r + 8);
+        kA2 = kmajor_off(2 * t + 1, r);
+        kA3 = kmajor_off(2 * t + 1, r + 8);
+        kB0 = kmajor_off(2 * t, c);
+        kB1 = kmajor_off(2 * t + 1, c);
+        xA0 = r * 128 + ((t ^ (r & 7)) << 4);
+        xA1 = (r + 8) * 128 + ((t ^ ((r + 8) & 7)) << 4);
+        xB = c * 128 + ((t ^ (c & 7)) << 4);
     }
     __device__ __forceinline__ static double ld(const char *p, int off) { return *reinterpret_cast<const double *>(p + off); }
     __device__ __forceinline__ static double2 ld2(const char *p, int off) { return *reinterpret_cast<const double2 *>(p + off); }
@@ -190,6 +203,29 @@ struct FragOffsets {
         b[1] = v.y;
     }
 };
+
+// m16n8k16 fragments: the k8 fragments of the chunk's two k-steps (K-major panels: the second
+// k-step starts 8 rows = 1024 bytes further; X-major panels: 64 bytes further in each row).
+__device__ __forceinline__ void ld_a16_K(const FragOffsets &fo, double (&a)[8], const char *P)
+{
+    fo.ldA_K(*reinterpret_cast<double(*)[4]>(&a[0]), P);
+    fo.ldA_K(*reinterpret_cast<double(*)[4]>(&a[4]), P + 1024);
+}
+__device__ __forceinline__ void ld_b16_K(const FragOffsets &fo, double (&b)[4], const char *P)
+{
+    fo.ldB_K(*reinterpret_cast<double(*)[2]>(&b[0]), P);
+    fo.ldB_K(*reinterpret_cast<double(*)[2]>(&b[2]), P + 1024);
+}
+__device__ __forceinline__ void ld_a16_X(const FragOffsets &fo, double (&a)[8], const char *P)
+{
+    fo.ldA_X(*reinterpret_cast<double(*)[4]>(&a[0]), P, 0);
+    fo.ldA_X(*reinterpret_cast<double(*)[4]>(&a[4]), P, 64);
+}
+__device__ __forceinline__ void ld_b16_X(const FragOffsets &fo, double (&b)[4], const char *P)
+{
+    fo.ldB_X(*reinterpret_cast<double(*)[2]>(&b[0]), P, 0);
+    fo.ldB_X(*reinterpret_cast<double(*)[2]>(&b[2]), P, 64);
+}
 
 // Brings the 128-byte lines of the energy vectors the item's epilogue will read into L1 (lanes 0..27:
 // 7 vectors x {B, C} block x 2 lines), so the register epilogue does not wait on L2.
@@ -222,8 +258,8 @@ __device__ __forceinline__ void warp_epilogue(const ItemCtx &cx, const double (&
     const double eaijk = cx.eaijk;
 #pragma unroll
     for (int e = 0; e < 4; ++e) {
-        const int b = rb0 + g + ((e & 2) ? 8 : 0);
-        const int c = cb0 + 2 * t + (e & 1);
+        const int b = rb0 + perm8(g) + ((e & 2) ? 8 : 0);
+        const int c = cb0 + perm8(2 * t + (e & 1));
         if (b < V && c < V) {
             double fbc[8], fcb[8];
 #pragma unroll
@@ -387,6 +423,7 @@ __device__ __forceinline__ void producer(const trpdrv_dev_system *__restrict__ s
 }
 
 // ------------------------------------------------------------------------------------------------
+template <int KS>
 __global__ void __launch_bounds__(NTHREAD, 1)
 fused_tma_kernel(const trpdrv_dev_system *__restrict__ sys, int nsys, long long total, unsigned long long *counter,
                  int *status, const __grid_constant__ Maps maps)
@@ -458,7 +495,41 @@ fused_tma_kernel(const trpdrv_dev_system *__restrict__ sys, int nsys, long long 
             // the second k-step of a chunk is skipped when it lies entirely in the zero padding
             const int kval = ph1 ? cx.nocc - (ch - nV) * DK : cx.nvir - ch * DK;
             if (ch == pf) prefetch_epilogue(cx, lane);
-            if (active) {
+            if (KS == 16 && active && kval > 8) {
+                // one m16n8k16 per product: the fragments of both k-steps of the chunk side by side
+#pragma unroll
+                for (int fam = 0; fam < 2; ++fam) {
+                    const char *P = st + fam * 8 * PANEL_BYTES;   // o = 0 panels
+                    const char *Q = P + PANEL_BYTES;             // o = 1 panels
+                    const int x0 = fam * 4;
+                    double aJ[8], aK[8], b1[4], b3[4];
+                    ld_a16_K(fo, aJ, P + 0 * PANEL_BYTES);
+                    ld_a16_K(fo, aK, P + 2 * PANEL_BYTES);
+                    ld_b16_X(fo, b3, P + 6 * PANEL_BYTES);
+                    if (!ph1)
+                        ld_b16_K(fo, b1, P + 4 * PANEL_BYTES);
+                    else
+                        ld_b16_X(fo, b1, P + 4 * PANEL_BYTES);
+                    dmma_16x8x16(f[x0 + 0], aJ, b1);
+                    dmma_16x8x16(f[x0 + 1], aK, b1);
+                    dmma_16x8x16(f[x0 + 2], aJ, b3);
+                    dmma_16x8x16(f[x0 + 3], aK, b3);
+                    if (!diag) {
+                        double a1[8], a3[8], bJ[4], bK[4];
+                        ld_b16_K(fo, bJ, Q + 0 * PANEL_BYTES);
+                        ld_b16_K(fo, bK, Q + 2 * PANEL_BYTES);
+                        ld_a16_X(fo, a3, Q + 6 * PANEL_BYTES);
+                        if (!ph1)
+                            ld_a16_K(fo, a1, Q + 4 * PANEL_BYTES);
+                        else
+                            ld_a16_X(fo, a1, Q + 4 * PANEL_BYTES);
+                        dmma_16x8x16(gT[x0 + 0], a1, bJ);
+                        dmma_16x8x16(gT[x0 + 1], a1, bK);
+                        dmma_16x8x16(gT[x0 + 2], a3, bJ);
+                        dmma_16x8x16(gT[x0 + 3], a3, bK);
+                    }
+                }
+            } else if (active) {
 #pragma unroll
                 for (int ks = 0; ks < 2; ++ks)
 #pragma unroll
@@ -516,14 +587,14 @@ fused_tma_kernel(const trpdrv_dev_system *__restrict__ sys, int nsys, long long 
                 double *xb = xbuf + (x & 1) * XBUF;
 #pragma unroll
                 for (int e = 0; e < 4; ++e)
-                    xb[(rx0 + g + ((e & 2) ? 8 : 0)) * (T + 1) + cx0 + 2 * t + (e & 1)] = f[x][e];
+                    xb[(rx0 + perm8(g) + ((e & 2) ? 8 : 0)) * (T + 1) + cx0 + perm8(2 * t + (e & 1))] = f[x][e];
                 __syncwarp();
                 if (lane == 0) mbar_arrive(xbar);
                 if (!mbar_wait(xbar, xphase, status)) return;
                 xphase ^= 1;
 #pragma unroll
                 for (int e = 0; e < 4; ++e)
-                    gT[x][e] = xb[(cx0 + 2 * t + (e & 1)) * (T + 1) + rx0 + g + ((e & 2) ? 8 : 0)];
+                    gT[x][e] = xb[(cx0 + perm8(2 * t + (e & 1))) * (T + 1) + rx0 + perm8(g) + ((e & 2) ? 8 : 0)];
             }
         }
         warp_epilogue(cx, f, gT, cx.b0 + rx0, cx.c0 + cx0, g, t, lane, cx.out + warp * 4);
@@ -613,21 +684,35 @@ extern "C" int trpdrv_tma_prepare(const trpdrv_dev_system *h_sys, int nsys, void
 
 extern "C" int trpdrv_launch_fused_tma(const trpdrv_dev_system *d_sys, int nsys, int64_t total_items,
                                        unsigned long long *counter, int *status, int grid, const void *maps,
-                                       void *stream)
+                                       int mma_k, void *stream)
 {
     if (grid <= 0 || total_items <= 0) return 0;
     if (g_launch_regs != tma::REG_LAUNCH) return (int)cudaErrorInvalidConfiguration;
-    tma::fused_tma_kernel<<<grid, tma::NTHREAD, tma::SMEM_BYTES, (cudaStream_t)stream>>>(
-        d_sys, nsys, total_items, counter, status, *static_cast<const tma::Maps *>(maps));
+    const tma::Maps &m = *static_cast<const tma::Maps *>(maps);
+    if (mma_k == 16)
+        tma::fused_tma_kernel<16><<<grid, tma::NTHREAD, tma::SMEM_BYTES, (cudaStream_t)stream>>>(
+            d_sys, nsys, total_items, counter, status, m);
+    else if (mma_k == 8)
+        tma::fused_tma_kernel<8><<<grid, tma::NTHREAD, tma::SMEM_BYTES, (cudaStream_t)stream>>>(
+            d_sys, nsys, total_items, counter, status, m);
+    else
+        return (int)cudaErrorInvalidValue;
     return (int)cudaGetLastError();
 }
 
+// Both instantiations must be launched with REG_LAUNCH registers per thread (the setmaxnreg split
+// assumes it); g_launch_regs holds the common value, or 0 when they differ.
 extern "C" int trpdrv_fused_tma_init(void)
 {
-    cudaFuncAttributes fa;
-    cudaError_t e = cudaFuncGetAttributes(&fa, tma::fused_tma_kernel);
+    cudaFuncAttributes f8, f16;
+    cudaError_t e = cudaFuncGetAttributes(&f8, tma::fused_tma_kernel<8>);
+    if (e == cudaSuccess) e = cudaFuncGetAttributes(&f16, tma::fused_tma_kernel<16>);
     if (e != cudaSuccess) return (int)e;
-    g_launch_regs = fa.numRegs;
-    return (int)cudaFuncSetAttribute(tma::fused_tma_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     (int)tma::SMEM_BYTES);
+    g_launch_regs = f8.numRegs == f16.numRegs ? f8.numRegs : 0;
+    e = cudaFuncSetAttribute(tma::fused_tma_kernel<8>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)tma::SMEM_BYTES);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(tma::fused_tma_kernel<16>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)tma::SMEM_BYTES);
+    return (int)e;
 }

@@ -204,6 +204,7 @@ struct trpdrv_plan {
     int64_t last_launches;
     cudaStream_t last_stream;
     int use_tma;        /* the fused launch stages panels with TMA (fused_tma.cu) */
+    int tma_mma_k;      /* FP64 MMA shape of the TMA kernel: 8 (m16n8k8) or 16 (m16n8k16) */
     double *d_fbuf;     /* emulated form: f of one batch of triples [fbuf_batch][8][nvir][nvir] */
     int fbuf_batch;     /* triples d_fbuf holds (>= opt.batch, and room for the autotuner's batches) */
     int tuned_staging;  /* FUSED staging chosen by the autotuner (1 cp.async, 2 TMA), 0 = none */
@@ -452,7 +453,8 @@ int trpdrv_plan_create(trpdrv_plan **plan, const trpdrv_system *shape, int nsys,
         return fail(TRPDRV_ERR_UNSUPPORTED, "tile %d: only %d is compiled", o.tile, TRPDRV_TILE);
     if (o.nkpass < 1) o.nkpass = 1;
     if (o.mma_k == 0) o.mma_k = 8;
-    if (o.mma_k != 4 && o.mma_k != 8) return fail(TRPDRV_ERR_ARG, "mma_k %d: must be 4 or 8", o.mma_k);
+    if (o.mma_k != 4 && o.mma_k != 8 && o.mma_k != 16)
+        return fail(TRPDRV_ERR_ARG, "mma_k %d: must be 4, 8 or 16", o.mma_k);
     if (o.staging < 0 || o.staging > 2) return fail(TRPDRV_ERR_ARG, "staging %d: must be 0, 1 or 2", o.staging);
     for (int q = 0; q < nsys; ++q) {
         TRY(check_shape(&shape[q], q));
@@ -468,6 +470,10 @@ int trpdrv_plan_create(trpdrv_plan **plan, const trpdrv_system *shape, int nsys,
     if (!p) return fail(TRPDRV_ERR_NOMEM, "host allocation failed");
     p->nsys = nsys;
     p->opt = o;
+    /* mma_k names the shape of whichever fused kernel runs: 16 exists only with TMA staging, 4 only
+     * with cp.async staging; each kernel takes its nearest shape */
+    p->tma_mma_k = o.mma_k == 16 ? 16 : 8;
+    if (p->opt.mma_k == 16) p->opt.mma_k = 8;
     p->device = dev;
     p->nsm = nsm;
     int rc = plan_build(p, shape);
@@ -615,7 +621,7 @@ static int enqueue_fused(trpdrv_plan *p, cudaStream_t st, int capturing)
     if (p->total_items > 0) {
         if (p->use_tma)
             LAUNCH_TRY(trpdrv_launch_fused_tma(p->d_dev, p->nsys, p->total_items, p->d_counter, p->d_status,
-                                               p->grid_tma, p->tma_maps, st));
+                                               p->grid_tma, p->tma_maps, p->tma_mma_k, st));
         else
             LAUNCH_TRY(trpdrv_launch_fused(p->d_dev, p->nsys, p->total_items, p->d_counter, p->d_status, p->grid,
                                            p->vec2, p->opt.mma_k, st));
@@ -990,7 +996,7 @@ int trpdrv_plan_upload_execute(trpdrv_plan *p, const trpdrv_system *host, int ch
         const int grid = (int64_t)cap < n ? cap : (int)n;
         if (n <= 0 || rc != TRPDRV_OK) continue;
         int e = p->use_tma ? trpdrv_launch_fused_tma(p->d_dev, p->nsys, sp[c].end, p->d_chunk_first + c, p->d_status,
-                                                     grid, p->tma_maps, p->stream)
+                                                     grid, p->tma_maps, p->tma_mma_k, p->stream)
                            : trpdrv_launch_fused(p->d_dev, p->nsys, sp[c].end, p->d_chunk_first + c, p->d_status,
                                                  grid, p->vec2, p->opt.mma_k, p->stream);
         if (e) rc = fail(TRPDRV_ERR_CUDA, "fused launch of span %d: %s", c, cudaGetErrorString((cudaError_t)e));
@@ -1142,6 +1148,7 @@ static void tune_apply(trpdrv_plan *p, const trpdrv_tune_candidate *c)
     if (p->opt.mode == TRPDRV_MODE_FUSED) {
         p->use_tma = c->staging == 2;
         p->tuned_staging = c->staging; /* a later upload/bind keeps it where TMA remains possible */
+        if (c->staging == 2) p->tma_mma_k = c->mma_k;
         if (c->staging == 1) {
             p->opt.mma_k = c->mma_k;
             p->opt.ctas_per_sm = c->ctas_per_sm;
@@ -1192,7 +1199,7 @@ static int tune_time(trpdrv_plan *p, const trpdrv_tune_candidate *c, double *est
                 CUDA_TRY(cudaEventRecord(p->ev0, st));
                 if (c->staging == 2)
                     LAUNCH_TRY(trpdrv_launch_fused_tma(p->d_dev, p->nsys, d->item_begin + sample, p->d_counter,
-                                                       p->d_status, grid, p->tma_maps, st));
+                                                       p->d_status, grid, p->tma_maps, c->mma_k, st));
                 else
                     LAUNCH_TRY(trpdrv_launch_fused(p->d_dev, p->nsys, d->item_begin + sample, p->d_counter,
                                                    p->d_status, grid, p->vec2, c->mma_k, st));
@@ -1374,7 +1381,8 @@ int trpdrv_plan_autotune(trpdrv_plan *p, trpdrv_tune_result *result)
         int occ = 1;
         if (trpdrv_fused_max_ctas_per_sm(&occ) != 0 || occ < 1) occ = 1;
         if (p->opt.staging != 1 && trpdrv_tma_supported(p->h_dev, p->nsys) && p->tma_maps) {
-            c[n++] = (trpdrv_tune_candidate){2, 0, 1, 0, 0.0};
+            c[n++] = (trpdrv_tune_candidate){2, 8, 1, 0, 0.0};
+            c[n++] = (trpdrv_tune_candidate){2, 16, 1, 0, 0.0};
         }
         if (p->opt.staging != 2) {
             c[n++] = (trpdrv_tune_candidate){1, 8, occ, 0, 0.0};
@@ -1431,53 +1439,6 @@ int trpdrv_run(const trpdrv_system *host, int nsys, const trpdrv_options *opt, d
     if (rc == TRPDRV_OK) rc = trpdrv_plan_energies(p, emp4, emp5);
     trpdrv_plan_destroy(p);
     return rc;
-}
-
-/* ------------------------------------------------------------------------------------------ */
-/* FP64 probe                                                                                   */
-/* ------------------------------------------------------------------------------------------ */
-
-int trpdrv_probe_fp64_peak(int device, int kind, double *tflops)
-{
-    if (!tflops || kind < 0 || kind > 4) return fail(TRPDRV_ERR_ARG, "bad probe arguments");
-    int dev = 0, nsm = 0;
-    TRY(ensure_device(device, &dev, &nsm));
-    const int grid = nsm * 4;
-    double *sink = NULL;
-    CUDA_TRY(cudaMalloc((void **)&sink, sizeof(double) * (size_t)grid * 256));
-    cudaEvent_t e0, e1;
-    CUDA_TRY(cudaEventCreate(&e0));
-    CUDA_TRY(cudaEventCreate(&e1));
-    double flops = 0.0;
-    int iters = 256;
-    float ms = 0.0f;
-    int rc = TRPDRV_OK;
-    /* warm up, then grow the loop until one launch takes >= 50 ms */
-    for (int attempt = 0; attempt < 12; ++attempt) {
-        if (trpdrv_launch_probe(kind, grid, iters, sink, &flops, NULL) != 0) {
-            rc = fail(TRPDRV_ERR_CUDA, "probe launch failed");
-            break;
-        }
-        cudaEventRecord(e0, NULL);
-        if (trpdrv_launch_probe(kind, grid, iters, sink, &flops, NULL) != 0) {
-            rc = fail(TRPDRV_ERR_CUDA, "probe launch failed");
-            break;
-        }
-        cudaEventRecord(e1, NULL);
-        if (cudaEventSynchronize(e1) != cudaSuccess) {
-            rc = fail(TRPDRV_ERR_CUDA, "probe sync failed");
-            break;
-        }
-        cudaEventElapsedTime(&ms, e0, e1);
-        if (ms >= 50.0f) break;
-        iters *= 2;
-    }
-    cudaEventDestroy(e0);
-    cudaEventDestroy(e1);
-    cudaFree(sink);
-    if (rc != TRPDRV_OK) return rc;
-    *tflops = flops / (ms * 1e-3) / 1e12;
-    return TRPDRV_OK;
 }
 
 /* ------------------------------------------------------------------------------------------ */

@@ -61,7 +61,7 @@ size_t trpdrv_tma_maps_bytes(void);
 int trpdrv_tma_prepare(const trpdrv_dev_system *h_sys, int nsys, void *maps_out);
 int trpdrv_launch_fused_tma(const trpdrv_dev_system *d_sys, int nsys, int64_t total_items,
                             unsigned long long *counter, int *status, int grid, const void *maps,
-                            void *stream);
+                            int mma_k, void *stream);
 int trpdrv_fused_tma_init(void);
 
 /* Emulated-FP64 (Ozaki int8) form, ozaki.cu.  Per system: digit slices of the A operands
@@ -131,8 +131,6 @@ typedef struct trpdrv_tengy_args {
 int trpdrv_launch_tengy(const trpdrv_tengy_args *args, void *stream);
 size_t trpdrv_tengy_smem_bytes(void);
 
-/* FP64 issue-rate probe: kind as trpdrv_probe_fp64_peak; returns FLOPs executed. */
-int trpdrv_launch_probe(int kind, int grid, int iters, double *sink, double *flops, void *stream);
 
 /* Sets the dynamic shared memory limits of every kernel (call once per device). */
 int trpdrv_kernels_init(void);

@@ -1,9 +1,10 @@
 // The triples body on caller-owned device buffers without any device allocation.
 //
-// Some callers cannot allocate device memory at the moment they need this work: code running while
-// a CUDA stream is being captured into a graph (cudaMalloc is not allowed inside a capture), code
-// that runs under a fixed device-memory budget handed out by its host application, or a caller
-// that owns every device buffer and forbids libraries from allocating behind its back.  For them,
+// Some callers cannot call cudaMalloc when they need this work: a host application (a quantum-
+// chemistry code, for one) that reserves the device memory up front in its own pool and hands
+// libraries a fixed budget, so an allocation behind its back could fail or break that budget; a
+// plug-in running inside a framework that owns every device buffer; or a loop that cannot pay for
+// cudaMalloc/cudaFree, which may synchronise the device, on every call.  For them,
 // trpdrv_body_device_noalloc runs the plain per-triple path (the grouped FP64 GEMM that forms the
 // eight f and the tengy reduction, the same kernels as the plain plans) with all of its scratch in
 // one statically sized device array that the CUDA module reserves when it loads:
@@ -16,7 +17,9 @@
 //     and sets the kernels' shared-memory limits; make that first call before any stream capture.
 //
 // The caller passes device pointers for the inputs (already sliced for the triple) and for the
-// four outputs; this function enqueues on the caller's stream and returns without waiting.
+// four outputs; this function enqueues on the caller's stream and returns without waiting.  It
+// refuses to start while an earlier CUDA error is pending on the thread (it would otherwise read
+// and clear that error as its own), and reports it without clearing it.
 
 #include <cuda_runtime.h>
 #include <pthread.h>
@@ -97,6 +100,14 @@ extern "C" int trpdrv_body_device_noalloc(const trpdrv_body_device_args *a, void
         if (!p) return fail(TRPDRV_ERR_ARG, "trpdrv_body_device_noalloc: NULL input pointer");
     if (!a->out4) return fail(TRPDRV_ERR_ARG, "trpdrv_body_device_noalloc: NULL output pointer");
 
+    // an error left by the caller's earlier work stays the caller's: report it, do not clear it
+    const cudaError_t pending = cudaPeekAtLastError();
+    if (pending != cudaSuccess) {
+        char msg[256];
+        snprintf(msg, sizeof msg, "trpdrv_body_device_noalloc: an earlier CUDA error is pending (%s); nothing enqueued",
+                 cudaGetErrorString(pending));
+        return fail(TRPDRV_ERR_STATE, msg);
+    }
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= MAX_DEVICES)
         return fail(TRPDRV_ERR_NODEV, "trpdrv_body_device_noalloc: no current CUDA device");

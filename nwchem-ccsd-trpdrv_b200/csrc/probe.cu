@@ -1,12 +1,15 @@
 // FP64 issue-rate probe: the roofline denominator for the FP64 contraction kernels.
 //
+// A measurement tool, not part of the product: it is built into its own library,
+// lib/libtrpdrv_probe.so, which only the benchmark loads.
+//
 // Every warp keeps NACC independent accumulator chains in registers and issues NACC MMAs (or DFMAs)
 // per iteration with register operands only, so the measured rate is the FP64 tensor (or FMA) pipe
 // throughput of the device, not a memory rate.  The accumulators are written out at the end so the
 // work cannot be eliminated.
 
 #include "device_common.cuh"
-#include "launch.h"
+#include <cuda_runtime.h>
 
 namespace trpdrv {
 namespace probe {
@@ -65,9 +68,8 @@ probe_kernel(int iters, double *sink)
 
 using namespace trpdrv;
 
-extern "C" int trpdrv_launch_probe(int kind, int grid, int iters, double *sink, double *flops, void *stream)
+static int launch_probe(int kind, int grid, int iters, double *sink, double *flops, cudaStream_t st)
 {
-    cudaStream_t st = (cudaStream_t)stream;
     const double warps = (double)grid * (probe::NTHREAD / 32);
     const double per_iter = probe::NACC;
     double mma_flops = 0.0;
@@ -97,4 +99,47 @@ extern "C" int trpdrv_launch_probe(int kind, int grid, int iters, double *sink, 
     }
     if (flops) *flops = warps * iters * per_iter * mma_flops;
     return (int)cudaGetLastError();
+}
+
+// FP64 issue rate of `device` (-1 = current): kind 0 = DMMA m8n8k4, 1 = m16n8k4, 2 = m16n8k8,
+// 3 = m16n8k16, 4 = scalar DFMA.  The loop grows until one launch takes >= 50 ms; writes TFLOP/s.
+// Returns 0, or a CUDA error code.
+extern "C" int trpdrv_probe_fp64_peak(int device, int kind, double *tflops)
+{
+    if (!tflops || kind < 0 || kind > 4) return (int)cudaErrorInvalidValue;
+    cudaError_t e = cudaSuccess;
+    if (device >= 0 && (e = cudaSetDevice(device)) != cudaSuccess) return (int)e;
+    int dev = 0, nsm = 0;
+    if ((e = cudaGetDevice(&dev)) != cudaSuccess) return (int)e;
+    if ((e = cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess) return (int)e;
+    const int grid = nsm * 4;
+    double *sink = nullptr;
+    if ((e = cudaMalloc((void **)&sink, sizeof(double) * (size_t)grid * probe::NTHREAD)) != cudaSuccess) return (int)e;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    double flops = 0.0;
+    int iters = 256, rc = 0;
+    float ms = 0.0f;
+    for (int attempt = 0; attempt < 12 && rc == 0; ++attempt) {
+        rc = launch_probe(kind, grid, iters, sink, &flops, nullptr);  // warm-up
+        if (rc) break;
+        cudaEventRecord(e0, nullptr);
+        rc = launch_probe(kind, grid, iters, sink, &flops, nullptr);
+        if (rc) break;
+        cudaEventRecord(e1, nullptr);
+        if ((e = cudaEventSynchronize(e1)) != cudaSuccess) {
+            rc = (int)e;
+            break;
+        }
+        cudaEventElapsedTime(&ms, e0, e1);
+        if (ms >= 50.0f) break;
+        iters *= 2;
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    cudaFree(sink);
+    if (rc) return rc;
+    *tflops = flops / (ms * 1e-3) / 1e12;
+    return 0;
 }

@@ -126,7 +126,6 @@ _proto("trpdrv_triple_flops", C.c_double, [C.c_int, C.c_int])
 _proto("trpdrv_tensor_elems", C.c_size_t, [C.c_int, C.c_int, C.c_int, C.c_int])
 _proto("trpdrv_synth_fill", C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int, C.c_uint64, C.c_int, _dp,
                                       C.c_size_t])
-_proto("trpdrv_probe_fp64_peak", C.c_int, [C.c_int, C.c_int, _dp])
 _proto("trpdrv_body_device_noalloc", C.c_int, [C.POINTER(BodyDeviceArgs), C.c_void_p])
 _proto("trpdrv_finalize", None, [])
 _proto("trpdrv_register_host", C.c_int, [C.c_void_p, C.c_size_t])
@@ -528,12 +527,6 @@ def body_device_noalloc(ncor: int, nocc: int, nvir: int, a: int, i: int, j: int,
     for n in BODY_DEVICE_FIELDS:
         setattr(args, n, C.c_void_p(int(ptrs[n])) if ptrs.get(n) else None)
     _check(lib.trpdrv_body_device_noalloc(C.byref(args), C.c_void_p(stream) if stream else None))
-
-
-def probe_fp64_peak(kind: int, device: int = -1) -> float:
-    out = C.c_double(0.0)
-    _check(lib.trpdrv_probe_fp64_peak(device, kind, C.byref(out)))
-    return out.value
 
 
 def finalize():

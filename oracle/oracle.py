@@ -57,6 +57,13 @@ def lib():
                                       _dp, C.c_int, C.c_double, _dp, C.c_int]
         _lib.oracle_tengy.restype = None
         _lib.oracle_tengy.argtypes = [_dp] * 15 + [C.c_double] + [_dp] * 4 + [C.c_int] * 3
+        _lib.oracle_tensor_elems.restype = C.c_int64
+        _lib.oracle_tensor_elems.argtypes = [C.c_int] * 4
+        _lib.oracle_synth_fill.restype = C.c_int64
+        _lib.oracle_synth_fill.argtypes = [C.c_int] * 4 + [C.c_uint64, C.c_int, _dp, C.c_int64]
+        _lib.oracle_time_body.restype = None
+        _lib.oracle_time_body.argtypes = [C.POINTER(OracleSystem), C.c_int, C.c_int64, C.c_int64, C.c_void_p,
+                                          _dp, _dp]
     return _lib
 
 
@@ -91,6 +98,53 @@ def _struct(s) -> OracleSystem:
         assert arr.dtype == np.float64 and arr.flags.c_contiguous
         setattr(o, n, C.c_void_p(arr.ctypes.data))
     return o
+
+
+class SynthSystem:
+    """One seeded system in the slice layout of trpdrv_oracle.h (arrays: name -> float64 ndarray)."""
+
+    def __init__(self, ncor, nocc, nvir, a):
+        self.ncor, self.nocc, self.nvir, self.a = ncor, nocc, nvir, a
+        self.arrays = {}
+
+    def nbytes(self) -> int:
+        return sum(int(v.nbytes) for v in self.arrays.values())
+
+
+A_DEPENDENT = ("jvv", "kvv", "dintc", "dintx", "t1v")
+
+
+def synth_system(nocc: int, nvir: int, seed: int = 1, ncor: int = 0, dist: int = 0, a: int | None = None,
+                 a_block: int = 0) -> SynthSystem:
+    """The seeded synthetic system of the product's generator, restated (oracle_synth_fill): `a`
+    defaults to the first virtual orbital ncor+nocc+1; a_block = m takes virtual index a + m of the
+    sweep, whose a-dependent tensors (jvv, kvv, dintc, dintx, t1v) come from seed + 7919 m."""
+    if a is None:
+        a = ncor + nocc + 1
+    s = SynthSystem(ncor, nocc, nvir, a + a_block)
+    L = lib()
+    for t, name in enumerate(TENSOR_NAMES):
+        n = int(L.oracle_tensor_elems(t, ncor, nocc, nvir))
+        buf = np.empty(n, dtype=np.float64)
+        sd = seed + 7919 * a_block if name in A_DEPENDENT else seed
+        if L.oracle_synth_fill(t, ncor, nocc, nvir, sd, dist, buf.ctypes.data_as(_dp), n) != n:
+            raise ValueError(f"oracle_synth_fill({name}) refused its arguments")
+        s.arrays[name] = buf
+    return s
+
+
+def time_body(s, which: str = "reference", nkpass: int = 1, t_begin: int = 0, t_end: int | None = None,
+              emp4: float = 0.0, emp5: float = 0.0):
+    """Serial body calls over triples [t_begin, t_end) of the driver order, as omp/test.c:160-195 makes
+    them (the body accumulates emp4/emp5 itself; nothing else runs).  Returns (emp4, emp5)."""
+    L = lib()
+    if t_end is None:
+        t_end = count_triples(s.nocc)
+    fn = C.cast(ref().ccsd_trpdrv_omp_cbody_ if which == "reference" else L.oracle_cbody, C.c_void_p)
+    e4, e5 = C.c_double(emp4), C.c_double(emp5)
+    st = _struct(s)
+    L.oracle_time_body(C.byref(st), nkpass, t_begin, t_end, fn, C.byref(e4), C.byref(e5))
+    return e4.value, e5.value
 
 
 def count_triples(nocc: int) -> int:

@@ -283,3 +283,105 @@ int64_t oracle_run_system(const oracle_system *s, int nkpass, int64_t t_begin, i
     free(ijkl);
     return mismatches;
 }
+
+/* ---- seeded synthetic inputs (SplitMix64 counter stream; Steele, Lea & Flood, OOPSLA 2014) ---- */
+
+static uint64_t sm64(uint64_t x)
+{
+    x += 0x9E3779B97F4A7C15ull;
+    x = (x ^ (x >> 30)) * 0xBF58476D1CE4E5B9ull;
+    x = (x ^ (x >> 27)) * 0x94D049BB133111EBull;
+    return x ^ (x >> 31);
+}
+
+static int cmp_dbl(const void *p, const void *q)
+{
+    const double x = *(const double *)p, y = *(const double *)q;
+    return (x > y) - (x < y);
+}
+
+int64_t oracle_tensor_elems(int tensor, int ncor, int nocc, int nvir)
+{
+    const int64_t o = nocc > 0 ? nocc : 0, v = nvir > 0 ? nvir : 0;
+    switch (tensor) {
+    case 0: return (int64_t)(ncor > 0 ? ncor : 0) + o + v; /* eorb */
+    case 1: return o * o * v * v;                          /* t2 [j][x][v][v] */
+    case 2: case 3: return o * v * v;                      /* jvv, kvv */
+    case 4: case 5: return o * v * o;                      /* tov, xov */
+    case 6: case 7: return o * o * o * v;                  /* jov, kov */
+    case 8: case 9: case 10: return o * v;                 /* dintc, dintx, t1v */
+    default: return -1;
+    }
+}
+
+int64_t oracle_synth_fill(int tensor, int ncor, int nocc, int nvir, uint64_t seed, int dist,
+                          double *out, int64_t n)
+{
+    if (tensor < 0 || tensor > 10 || !out || ncor < 0 || nocc < 1 || nvir < 1 || (dist != 0 && dist != 1))
+        return -1;
+    if (n != oracle_tensor_elems(tensor, ncor, nocc, nvir)) return -1;
+    const uint64_t key = sm64(seed ^ ((uint64_t)(tensor + 1) * 0xD1B54A32D192ED03ull));
+    if (tensor == 0) {
+        for (int64_t e = 0; e < n; ++e) {
+            const double u = (double)(sm64(key + (uint64_t)e) >> 11) * 0x1.0p-53;
+            out[e] = e < ncor ? -20.0 + 15.0 * u : (e < ncor + nocc ? -2.0 + 1.5 * u : 0.2 + 2.8 * u);
+        }
+        qsort(out, (size_t)ncor, sizeof(double), cmp_dbl);
+        qsort(out + ncor, (size_t)nocc, sizeof(double), cmp_dbl);
+        qsort(out + ncor + nocc, (size_t)nvir, sizeof(double), cmp_dbl);
+        return n;
+    }
+    const double half = tensor == 1 ? 0.05 : ((tensor == 4 || tensor == 5 || tensor == 10) ? 0.02 : 0.1);
+    const int integral = !(tensor == 1 || tensor == 4 || tensor == 5 || tensor == 10);
+    const int logmag = integral && dist == 1;
+#pragma omp parallel for schedule(static)
+    for (int64_t e = 0; e < n; ++e) {
+        const uint64_t h = sm64(key + (uint64_t)e);
+        const double u = (double)(h >> 11) * 0x1.0p-53;
+        if (logmag) {
+            const double m = pow(10.0, -6.0 * u);
+            out[e] = (h & 1u) ? -m : m;
+        } else {
+            out[e] = -half + 2.0 * half * u;
+        }
+    }
+    return n;
+}
+
+/* ---- the reference driver's timed loop (omp/test.c:160-195), body calls only ---- */
+
+void oracle_time_body(const oracle_system *s, int nkpass, int64_t t_begin, int64_t t_end,
+                      oracle_body_fn body, double *emp4, double *emp5)
+{
+    const int nocc = s->nocc, nvir = s->nvir;
+    const int64_t ntot = oracle_count_triples(nocc);
+    if (t_begin < 0) t_begin = 0;
+    if (t_end > ntot) t_end = ntot;
+    if (t_end <= t_begin || !body) return;
+    int32_t *ijkl = (int32_t *)malloc(sizeof(int32_t) * 4 * (size_t)ntot);
+    oracle_enumerate(nocc, nkpass, ijkl);
+    const size_t lnvv = (size_t)nvir * nvir, lnov = (size_t)nocc * nvir;
+    double *f = (double *)malloc(sizeof(double) * 8 * lnvv);
+    double e4 = *emp4, e5 = *emp5;
+    for (int64_t t = t_begin; t < t_end; ++t) {
+        int i = ijkl[4 * t], j = ijkl[4 * t + 1], k = ijkl[4 * t + 2], klo = ijkl[4 * t + 3];
+        int ncor = s->ncor, no = nocc, nv = nvir, a = s->a;
+        const size_t jb = (size_t)(j - 1) * nocc;
+        body(f, f + lnvv, f + 2 * lnvv, f + 3 * lnvv, f + 4 * lnvv, f + 5 * lnvv, f + 6 * lnvv, f + 7 * lnvv,
+             (double *)s->eorb, &ncor, &no, &nv, &e4, &e5, &a, &i, &j, &k, &klo,
+             (double *)s->t2 + (jb + (i - 1)) * lnvv, (double *)s->t2 + (jb + (klo - 1)) * lnvv,
+             (double *)s->tov + (size_t)(i - 1) * lnov, (double *)s->tov + (size_t)(klo - 1) * lnov,
+             (double *)s->xov + (size_t)(i - 1) * lnov, (double *)s->xov + (size_t)(klo - 1) * lnov,
+             (double *)s->jvv + (size_t)(i - 1) * lnvv, (double *)s->jvv + (size_t)(klo - 1) * lnvv,
+             (double *)s->kvv + (size_t)(i - 1) * lnvv, (double *)s->kvv + (size_t)(klo - 1) * lnvv,
+             (double *)s->jov + (jb + (i - 1)) * lnov, (double *)s->jov + (jb + (klo - 1)) * lnov,
+             (double *)s->kov + (jb + (i - 1)) * lnov, (double *)s->kov + (jb + (klo - 1)) * lnov,
+             (double *)s->dintc + (size_t)(i - 1) * nvir, (double *)s->dintx + (size_t)(i - 1) * nvir,
+             (double *)s->t1v + (size_t)(i - 1) * nvir, (double *)s->dintc + (size_t)(k - 1) * nvir,
+             (double *)s->dintx + (size_t)(k - 1) * nvir, (double *)s->t1v + (size_t)(k - 1) * nvir);
+    }
+    *emp4 = e4;
+    *emp5 = e5;
+    free(f);
+    free(ijkl);
+}

@@ -92,6 +92,27 @@ int64_t oracle_run_system(const oracle_system *s, int nkpass, int64_t t_begin, i
  * tot[0] = sum emp4i + [i!=k] emp4k, tot[1] likewise for emp5. */
 void oracle_sum_records(const double *rec, const int32_t *ijkl, int64_t n, double *tot);
 
+/* Seeded synthetic inputs, restated from the product generator's published recipe so that the
+ * oracle and the reference arm of the benchmark need nothing from the product library.  Tensor ids
+ * 0..10 are eorb, t2, jvv, kvv, tov, xov, jov, kov, dintc, dintx, t1v (the slice layout above);
+ * dist 0 = uniform, 1 = log-uniform integral magnitudes.  Element e of tensor w under seed s is
+ * splitmix64(key(s, w) + e), key(s, w) = splitmix64(s ^ (w + 1) * 0xD1B54A32D192ED03), mapped to
+ * [0, 1) by its top 53 bits:
+ *   eorb: core -20 + 15u, occupied -2 + 1.5u, virtual 0.2 + 2.8u, each group sorted ascending;
+ *   t2 -0.05 + 0.1u; tov, xov, t1v -0.02 + 0.04u; integrals -0.1 + 0.2u, or with dist 1 a magnitude
+ *   10^(-6u) with the sign of the hash's lowest bit (set = negative).
+ * Returns the element count written, or -1 on bad arguments (n must equal oracle_tensor_elems). */
+int64_t oracle_tensor_elems(int tensor, int ncor, int nocc, int nvir);
+int64_t oracle_synth_fill(int tensor, int ncor, int nocc, int nvir, uint64_t seed, int dist,
+                          double *out, int64_t n);
+
+/* The reference driver's timed loop (omp/test.c:160-195) without any extra work: triples
+ * [t_begin, t_end) of the driver order, one serial call of `body` each, emp4/emp5 accumulated by the
+ * body itself through its pointers (starting from *emp4, *emp5).  The f scratch is allocated once.
+ * This is what the CPU baseline times. */
+void oracle_time_body(const oracle_system *s, int nkpass, int64_t t_begin, int64_t t_end,
+                      oracle_body_fn body, double *emp4, double *emp5);
+
 #ifdef __cplusplus
 }
 #endif

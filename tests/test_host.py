@@ -260,3 +260,49 @@ def test_bench_reference_arm_prints_one_contract_line():
     assert d["cpu_baseline"]["kind"] == "reference" and d["cpu_baseline"]["value"] == d["value"]
     assert d["cpu_baseline"]["cores"] >= 1
     assert d["e2e"] == {"value": d["value"], "unit": "triples/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}
+
+
+@pytest.mark.skipif(not os.path.exists(os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))),
+                                                    "oracle", "_ref", "libtrpdrv_ref.so")),
+                    reason="reference not built")
+def test_bench_reference_arm_maps_no_product_library():
+    """The reference arm runs the reference's CPU body on inputs from the oracle's generator: the
+    product library is never mapped into that process, and libgomp sees the passive wait policy."""
+    import subprocess
+    import sys
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    code = (
+        "import os, sys\n"
+        f"sys.path.insert(0, {root!r})\n"
+        "os.environ.pop('OMP_WAIT_POLICY', None)\n"
+        "sys.argv = ['bench.py', '--impl', 'reference', '--steps', '1', '--warmup', '0', '--workload', 'c1']\n"
+        "import bench\n"
+        "bench.main()\n"
+        "maps = open('/proc/self/maps').read()\n"
+        "print('MAPS', 'libtrpdrv_b200' in maps, 'libtrpdrv_ref' in maps, os.environ.get('OMP_WAIT_POLICY'))\n")
+    env = dict(os.environ)
+    env.pop("OMP_WAIT_POLICY", None)
+    out = subprocess.run([sys.executable, "-c", code], check=True, capture_output=True, text=True, timeout=600,
+                         env=env).stdout
+    tail = [ln for ln in out.splitlines() if ln.startswith("MAPS")][0]
+    assert tail == "MAPS False True passive", tail
+
+
+def test_bench_config_is_shared_by_both_arms():
+    """Both arms print the same `config` object for the same arguments (the lines then compare)."""
+    import importlib
+    import sys
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    sys.path.insert(0, root)
+    bench = importlib.import_module("bench")
+    for wl in ("c1", "c2", "c3", "c4"):
+        sys_argv = sys.argv
+        sys.argv = ["bench.py", "--workload", wl]
+        try:
+            args = bench.parse()
+        finally:
+            sys.argv = sys_argv
+        cfg = bench.config_for(args)
+        assert cfg["triples_per_step"] == sum(o * o * (o + 1) // 2 for o, _, _, _ in
+                                              bench.workload_shapes(wl, args.nocc, args.nvir))
+        assert "parallelism" in cfg and "workload" in cfg

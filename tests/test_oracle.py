@@ -76,3 +76,43 @@ def test_oracle_tengy_matches_reference_tengy(O):
     got = O.tengy(f8, vecs, eorb, 2.5, ncor, nocc, nvir, which="port")
     want = O.tengy(f8, vecs, eorb, 2.5, ncor, nocc, nvir, which="reference")
     np.testing.assert_allclose(got, want, rtol=1e-13)
+
+
+@pytest.mark.parametrize("shape", [(5, 33, 13, 2, 0, 0), (4, 30, 14, 0, 1, 0), (6, 40, 3, 0, 0, 2), (7, 21, 99, 1, 1, 3)])
+def test_oracle_generator_restatement_equals_the_product_generator(O, T, shape):
+    """oracle.synth_system (used by the benchmark's reference arm and the full-size fixtures) gives
+    bit-identical tensors to the product's trpdrv_synth_fill, for every tensor and distribution."""
+    nocc, nvir, seed, ncor, dist, a_block = shape
+    so = O.synth_system(nocc, nvir, seed=seed, ncor=ncor, dist=dist, a_block=a_block)
+    sp = T.synth_system(nocc, nvir, seed=seed, ncor=ncor, dist=dist, a_block=a_block)
+    assert so.a == sp.a
+    for name in O.TENSOR_NAMES:
+        assert np.array_equal(so.arrays[name], sp.arrays[name]), name
+
+
+def test_oracle_generator_matches_the_full_size_fixture_checksums(O):
+    """The full-size fixtures record input checksums; the restated generator reproduces them (C2 is
+    checked tensor by tensor on its 1.5 GB of inputs)."""
+    path = os.path.join(GOLDEN, "big_c2_o40_v300.json")
+    if not os.path.exists(path):
+        pytest.skip("full-size fixture not generated")
+    with open(path) as f:
+        g = json.load(f)["systems"][0]
+    s = O.synth_system(g["nocc"], g["nvir"], seed=g["seed"], dist=g["dist"], a=g["a"])
+    for n, (s1, s2) in g["checksums"].items():
+        a = s.arrays[n]
+        assert float(np.sum(a)) == s1 and float(np.sum(a * a)) == s2, n
+
+
+@pytest.mark.parametrize("which", ["port", "reference"])
+def test_oracle_timed_loop_accumulates_like_the_driver(O, which):
+    """oracle.time_body (the CPU baseline's loop: body calls only, the body accumulating emp4/emp5)
+    gives the totals of the recorded run, split over two calls."""
+    if which == "reference" and not O.have_reference():
+        pytest.skip("reference not built")
+    s = O.synth_system(5, 26, seed=21)
+    n = O.count_triples(5)
+    _, tot, _ = O.run_system(s, "port", nthreads=2)
+    e4, e5 = O.time_body(s, which, t_begin=0, t_end=n // 3)
+    e4, e5 = O.time_body(s, which, t_begin=n // 3, t_end=n, emp4=e4, emp5=e5)
+    assert abs(e4 - tot[0]) <= 1e-12 * abs(tot[0]) and abs(e5 - tot[1]) <= 1e-12 * abs(tot[1])

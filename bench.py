@@ -36,15 +36,18 @@ ranks), and one NCCL all-reduce of the energies per step sums the ranks' (T) con
 """
 import os
 
-# The reference's CPU path (OpenMP tengy + OpenBLAS, serial body calls) is timed with a passive OpenMP
-# wait policy: libgomp reads its environment when it is first loaded, so this precedes every import.
-os.environ.setdefault("OMP_WAIT_POLICY", "passive")
+# The reference arm times the reference's CPU path (OpenMP tengy + OpenBLAS, serial body calls) with a
+# passive OpenMP wait policy: libgomp reads its environment when it is first loaded, so this precedes
+# every import.  The B200 arm runs its CPU baseline as a separate reference-arm process.
+import sys  # noqa: E402
+
+if "--impl" in sys.argv and sys.argv[sys.argv.index("--impl") + 1:][:1] == ["reference"]:
+    os.environ.setdefault("OMP_WAIT_POLICY", "passive")
 
 import argparse  # noqa: E402
 import json  # noqa: E402
 import statistics  # noqa: E402
 import subprocess  # noqa: E402
-import sys  # noqa: E402
 import time  # noqa: E402
 
 import numpy as np  # noqa: E402
@@ -78,6 +81,8 @@ def parse():
                     help="N > 1: weak = every rank runs the whole workload for its own virtual index a (the "
                          "outer loop of the full (T)); strong = the triples of one a are split over the ranks")
     ap.add_argument("--no-emulated", action="store_true", help="skip the emulated-FP64 sweep of the default line")
+    ap.add_argument("--no-sub-legs", action="store_true",
+                    help="skip the default line's c3 / c4 sub-legs (N = 1) and strong split (N > 1)")
     ap.add_argument("--profile", action="store_true",
                     help="the timed plan only (c2/c4: fused FP64; c3: emulated, 7 slices), no probes, e2e, plain "
                          "or CPU legs: the command profiled with ncu")
@@ -500,42 +505,65 @@ def plain_sample(T, R, s, flop_triple, frac=16):
             "tflops_fp64_equiv": nplain * flop_triple / (pms * 1e-3) / 1e12}
 
 
-def dropin_leg(T, s, ntrip=256):
+def dropin_leg(T, s, ntrip=512):
     """The reference-facing entry point ccsd_trpdrv_omp_cbody_ called once per triple from host buffers,
-    as omp/test.c:160-195 calls it (wall clock: every call returns its energies to the host).  Timed with
-    per-call copies of the slices (the default) and with the system's arrays registered as unchanging
-    (trpdrv_register_host: no per-call transfer)."""
+    as omp/test.c:160-195 calls it (wall clock: every call returns its energies to the host).  The
+    39 arguments of every call are prepared before the timed loop (raw addresses), so the loop is one
+    foreign call per triple.  Timed with per-call copies of the slices (the default) and with the
+    system's arrays registered as unchanging (trpdrv_register_host: no per-call transfer)."""
+    import ctypes as C
     ijkl = T.enumerate_triples(s.nocc, 1)[:ntrip]
     # pageable host memory, like the reference driver's own arrays (omp/test.c:112-146)
     s = T.System(s.ncor, s.nocc, s.nvir, s.a, {k: np.array(v, copy=True) for k, v in s.arrays.items()})
+    fn = C.CFUNCTYPE(None, *([C.c_void_p] * 39))(C.cast(T.lib.ccsd_trpdrv_omp_cbody_, C.c_void_p).value)
+    f = np.zeros((8, s.nvir * s.nvir))
+    emp = np.zeros(2)
+    fp = [f[q].ctypes.data for q in (0, 1, 2, 3, 4, 5, 6, 7)]  # f1n f1t f2n f2t f3n f3t f4n f4t
+    keep, calls = [], []
+    for i, j, k, klo in ijkl:
+        ints = np.array([s.ncor, s.nocc, s.nvir, s.a, i, j, k, klo], dtype=np.int32)
+        keep.append(ints)
+        sl = T.triple_slices(s, int(i), int(j), int(k), int(klo))
+        calls.append(tuple(fp + [sl["eorb"].ctypes.data] + [ints.ctypes.data + 4 * q for q in range(3)] +
+                           [emp.ctypes.data, emp.ctypes.data + 8] + [ints.ctypes.data + 4 * q for q in range(3, 8)] +
+                           [sl[n].ctypes.data for n in T.BODY_ORDER]))
     out = {}
     for label in ("per_call_copies", "registered_inputs"):
         if label == "registered_inputs":
             T.register_system(s)
-        for i, j, k, klo in ijkl[:8]:  # warm-up
-            T.cbody(s, int(i), int(j), int(k), int(klo))
+        for args in calls[:8]:  # warm-up
+            fn(*args)
+        emp[:] = 0.0
         t0 = time.perf_counter()
-        e4 = e5 = 0.0
-        for i, j, k, klo in ijkl:
-            e4, e5 = T.cbody(s, int(i), int(j), int(k), int(klo), e4, e5)
+        for args in calls:
+            fn(*args)
         el = time.perf_counter() - t0
         if label == "registered_inputs":
             T.unregister_system(s)
-        out[label] = {"value": len(ijkl) / el, "unit": "triples/s", "emp4": e4, "emp5": e5}
-    out["sample"] = (f"the first {len(ijkl)} triples of the driver order at nocc={s.nocc} nvir={s.nvir}, one "
-                     f"ccsd_trpdrv_omp_cbody_ call each from pageable host buffers (wall clock, Python caller)")
+        out[label] = {"value": len(calls) / el, "unit": "triples/s", "emp4": float(emp[0]), "emp5": float(emp[1])}
+    out["sample"] = (f"the first {len(calls)} triples of the driver order at nocc={s.nocc} nvir={s.nvir}, one "
+                     f"ccsd_trpdrv_omp_cbody_ call each from pageable host buffers (wall clock; arguments prepared "
+                     f"before the timed loop)")
     return out
 
 
-def cpu_leg(args, R, nocc, nvir):
+def cpu_leg(args, R, workload_name=None):
+    """The reference's CPU body on this host's cores: the reference arm of this script run as its own
+    process (only the oracle's libraries loaded, passive OpenMP wait), three steps of about 4 s."""
     if R.rank != 0 or R.world != 1 or args.no_cpu_baseline:
         return None
+    wl = workload_name or args.workload
+    cmd = [sys.executable, os.path.abspath(__file__), "--impl", "reference", "--steps", "3", "--warmup", "1",
+           "--workload", wl]
+    if wl in ("c1", "c2", "c3"):
+        cmd += ["--nocc", str(args.nocc), "--nvir", str(args.nvir)]
+    env = {k: v for k, v in os.environ.items() if k not in ("RANK", "WORLD_SIZE", "LOCAL_RANK")}
     try:
-        v, n, el, ncpu = time_reference_cpu(nocc, nvir, budget_s=15.0)
-        return {"value": v, "unit": "triples/s", "cores": ncpu, "kind": "reference",
-                "sample": f"{n} consecutive triples of nocc={nocc} nvir={nvir}, serial calls of the reference body "
-                          f"(oracle/_ref: omp/ccsd_trpdrv_omp_cbody.c + omp/ccsd_tengy_c99.c, OpenBLAS 0.3.30), "
-                          f"{ncpu} OpenMP + OpenBLAS threads, {el:.1f} s"}
+        out = subprocess.run(cmd, capture_output=True, text=True, timeout=900, env=env, check=True).stdout
+        line = json.loads([ln for ln in out.splitlines() if ln.startswith("{")][-1])
+        cb = dict(line["cpu_baseline"])
+        cb["sample"] = "a reference-arm process of this script (" + " ".join(cmd[2:]) + "): " + cb["sample"]
+        return cb
     except Exception as ex:  # the reference build is missing
         return {"value": None, "unit": "triples/s", "cores": os.cpu_count(), "kind": "reference",
                 "sample": f"unavailable: {ex}"}
@@ -556,6 +584,76 @@ def fp64_roofline(achieved, peak, traffic, kms):
                            "and DFMA, register operands, 50 ms bursts) and cuBLAS DGEMM 8192^3; "
                            "MEASURED_PEAKS.json has no FP64 entry",
             "kernel_ms": kms}
+
+
+def reference_fixture(name):
+    """Totals the reference itself computed for a full-size workload (tests/golden/make_golden_large.py):
+    a list of {"nocc", "nvir", "emp4", "emp5"} per system, or None when the fixture is absent."""
+    path = os.path.join(ROOT, "tests", "golden", name + ".json")
+    if not os.path.exists(path):
+        return None
+    with open(path) as f:
+        return [{k: g[k] for k in ("nocc", "nvir", "emp4", "emp5")} for g in json.load(f)["systems"]]
+
+
+def rel_errors(e4, e5, ref):
+    if not ref:
+        return None
+    return [{"nocc": g["nocc"], "nvir": g["nvir"], "emp4": abs(a - g["emp4"]) / abs(g["emp4"]),
+             "emp5": abs(b - g["emp5"]) / abs(g["emp5"])} for a, b, g in zip(e4, e5, ref)]
+
+
+def sub_leg_c3(T, R, steps, warmup):
+    """The precision workload at reduced length: nocc=30, nvir=400, log-uniform integral magnitudes,
+    the emulated form at its default 7 slices and the FP64 fused kernel, both against the reference's
+    totals for this system (tests/golden/big_c3_o30_v400_log.json)."""
+    o, v = C3
+    s = T.synth_system(o, v, seed=SEED, a=o + 1, dist=T.DIST_LOGUNIFORM)
+    n = T.count_triples(o)
+    out = {"workload": f"nocc={o} nvir={v}, log-uniform integral magnitudes in [1e-6, 1], all {n} triples of one a",
+           "steps": steps, "warmup": warmup}
+    ref = reference_fixture("big_c3_o30_v400_log")
+    for label, opt in (("emulated_7", dict(mode=T.MODE_EMULATED, slices=DEFAULT_SLICES)),
+                       ("fused_fp64", dict(mode=T.MODE_FUSED))):
+        with T.Plan([s], **opt, device=R.local) as p:
+            p.upload(stream=R.sp)
+            p.autotune()
+            sec, kms, launches, e4, e5 = time_plan(T, R, p, steps, warmup)
+        out[label] = {"value": n / sec, "unit": "triples/s", "ms_per_step": 1e3 * sec,
+                      "tflops_fp64_equiv": n * T.triple_flops(o, v) / sec / 1e12, "gpu_launches": launches,
+                      "rel_err_vs_reference": rel_errors(e4, e5, ref)}
+    out["speedup_emulated_vs_fp64"] = out["emulated_7"]["value"] / out["fused_fp64"]["value"]
+    return out
+
+
+def sub_leg_c4(T, R, steps, warmup, peak):
+    """Six systems of uneven size in one fused FP64 launch, aggregate triples/s, each system's totals
+    against the reference's (tests/golden/big_c4_six.json)."""
+    systems = [T.synth_system(o, v, seed=SEED + q, a=o + 1) for q, (o, v) in enumerate(C4)]
+    n = sum(T.count_triples(x.nocc) for x in systems)
+    flop = sum(T.count_triples(x.nocc) * T.triple_flops(x.nocc, x.nvir) for x in systems)
+    with T.Plan(systems, mode=T.MODE_FUSED, device=R.local) as p:
+        p.upload(stream=R.sp)
+        p.autotune()
+        sec, kms, launches, e4, e5 = time_plan(T, R, p, steps, warmup)
+    return {"workload": "six systems " + ", ".join(f"({o},{v})" for o, v in C4) + f" in one fused launch, {n} "
+                        f"triples", "steps": steps, "warmup": warmup,
+            "value": n / sec, "unit": "triples/s", "ms_per_step": 1e3 * sec, "tflops_fp64_equiv": flop / sec / 1e12,
+            "roofline_frac": (flop / (kms * 1e-3) / 1e12) / peak, "gpu_launches": launches,
+            "rel_err_vs_reference": rel_errors(e4, e5, reference_fixture("big_c4_six"))}
+
+
+def strong_split(T, R, args, steps, warmup):
+    """N > 1: the triples of the c2 system's first a split over the ranks (strong scaling), beside the
+    default split over a; every rank takes part (the same collective steps on all ranks)."""
+    s = T.synth_system(args.nocc, args.nvir, seed=SEED, a=args.nocc + 1)
+    with T.Plan([s], mode=T.MODE_FUSED, rank=R.rank, world=R.world, device=R.local) as p:
+        p.upload(stream=R.sp)
+        sec, kms, launches, e4, e5 = time_plan(T, R, p, steps, warmup)
+    n = T.count_triples(args.nocc)
+    return {"value": n / sec, "unit": "triples/s", "ms_per_step": 1e3 * sec, "n_gpus": R.world,
+            "workload": f"the {n} triples of one a at nocc={args.nocc} nvir={args.nvir}, split over the ranks",
+            "emp4": e4[0], "emp5": e5[0]}
 
 
 def run_c1(args, T, R, systems, in_bytes, n_all, flop_all, probe, cublas_dgemm, fp64_probe, peak):
@@ -590,7 +688,7 @@ def run_c1(args, T, R, systems, in_bytes, n_all, flop_all, probe, cublas_dgemm, 
                 "path": "trpdrv_plan_upload (pinned host) + trpdrv_plan_execute + trpdrv_plan_energies"},
         "gpu_launches": launches, "clocks": ck, "emp4": e4[0], "emp5": e5[0],
         "fused_fp64": {"value": n_all / fsec, "unit": "triples/s", "records_max_rel_dev_vs_plain": dev},
-        "cpu_baseline": cpu_leg(args, R, args.nocc, args.nvir),
+        "cpu_baseline": cpu_leg(args, R),
     })
     print(json.dumps(line), flush=True)
     R.close()
@@ -704,6 +802,16 @@ def run_b200_arm(args):
             s = systems[0]
             plain = plain_sample(T, R, s, T.triple_flops(s.nocc, s.nvir))
 
+    # default line: the precision and uneven-batch workloads at reduced length, and at N > 1 the strong
+    # split of one a beside the split over a
+    sub = None
+    if args.workload == "c2" and not args.profile and not args.no_sub_legs:
+        sub = {}
+        if R.world == 1:
+            sub["c3"] = sub_leg_c3(T, R, 3, 1)
+            sub["c4"] = sub_leg_c4(T, R, 2, 1, peak)
+        elif R.weak:
+            sub["strong_split"] = strong_split(T, R, args, 3, 1)
     if R.rank != 0:
         R.close()
         return
@@ -735,7 +843,7 @@ def run_b200_arm(args):
             "gpu_launches": emu["gpu_launches"] if emu else launches,
             "clocks": ck, "plain_gpu": plain,
             "speedup_vs_plain": (value / R.world / plain["value"]) if plain else None,  # per GPU
-            "cpu_baseline": cpu_leg(args, R, args.nocc, args.nvir),
+            "cpu_baseline": cpu_leg(args, R),
         })
     else:
         value = n_all / sec
@@ -760,14 +868,17 @@ def run_b200_arm(args):
         if args.workload == "c4":
             line["emp4"], line["emp5"] = e4, e5
             line["per_system_equals_single_runs"] = singles
-            line["cpu_baseline"] = cpu_leg(args, R, *C4[-1])
-            if line["cpu_baseline"]:
-                line["cpu_baseline"]["sample"] += " (largest system only)"
+            line["cpu_baseline"] = cpu_leg(args, R)
         else:
             line["emp4"], line["emp5"] = e4[0], e5[0]
-            line["cpu_baseline"] = cpu_leg(args, R, args.nocc, args.nvir)
+            # the all-reduced totals are one a's (T) contribution unless N > 1 ranks each ran their own a
+            one_a = (args.nocc, args.nvir) == (NOCC, NVIR) and not (R.weak and R.world > 1)
+            line["rel_err_vs_reference"] = rel_errors(e4, e5, reference_fixture("big_c2_o40_v300")) if one_a else None
+            line["cpu_baseline"] = cpu_leg(args, R)
             if not args.profile and not args.no_plain:
                 line["dropin"] = dropin_leg(T, systems[0])
+            if sub is not None:
+                line.update(sub)
             if emulated:
                 emu = emulated[str(DEFAULT_SLICES)]
                 tgt = emulated["target"]

@@ -32,6 +32,12 @@ extern "C" {
  * omp/test.c:39-52).  All arguments by reference; every pointer is caller-owned HOST memory.
  * tkj, jka, kka are offset by (k-klo)*nvir*nvir and tka, xka, jkj, kkj by (k-klo)*nocc*nvir, as in
  * the reference.  f1n..f4t are scratch: they are written back only when TRPDRV_WRITE_F=1.
+ * Device work per call: with even nocc and nvir (and TRPDRV_WRITE_F unset) the slices are staged
+ * into a fixed one-triple layout (host slices through a pinned buffer, copied by up to
+ * TRPDRV_STAGE_THREADS host threads, default 8, then one host->device copy; slices inside registered
+ * arrays gathered on the device) and one launch of the fused FP64 kernel computes the energies
+ * without writing f; otherwise (or with TRPDRV_DROPIN_PATH=plain) the plain per-triple path runs (16
+ * GEMMs into f, then the tengy reduction).  The call returns after the energies are back on the host.
  * Errors (bad sizes/indices, CUDA failure) print to stderr and abort, unless TRPDRV_ON_ERROR=return,
  * in which case emp4/emp5 are left unchanged and trpdrv_last_error() reports the status. */
 void ccsd_trpdrv_omp_cbody_(double *f1n, double *f1t, double *f2n, double *f2t,
@@ -242,8 +248,11 @@ int trpdrv_plan_destroy(trpdrv_plan *plan);
  * system is sampled (about 1/8 of its fused items, 64 triples in the emulated form) and the per-
  * system times are scaled to its full work.  EMULATED plans with target_digits first pick the fewest
  * slices (4..8) that meet the accuracy target on the same sample.  The choice is cached per device and set of shapes for
- * the life of the process; a later plan with the same key takes it without timing.  No counterpart
- * in the reference (its BLAS call sites have nothing to tune).  `result` may be NULL. */
+ * the life of the process; a later plan with the same key takes it without timing.  With
+ * TRPDRV_TUNE_CACHE naming a file, choices are also appended there (one text line each, keyed by the
+ * device model, the library version and the plan's shapes and options) and read back by later
+ * processes.  result->from_cache: 0 = timed now, 1 = this process's cache, 2 = the file.  No
+ * counterpart in the reference (its BLAS call sites have nothing to tune).  `result` may be NULL. */
 typedef struct trpdrv_tune_candidate {
     int staging;          /* FUSED: 1 cp.async, 2 TMA; 0 otherwise */
     int mma_k;            /* FUSED: FP64 MMA shape k (TMA: 8 or 16; cp.async: 4 or 8) */

@@ -341,7 +341,11 @@ __device__ __forceinline__ void producer(const trpdrv_dev_system *__restrict__ s
         const bool in_range = local >= 0 && qpos < S.ntriples && tt >= 0 && tt < S.nt && ai < S.n_a;
         const int packed = in_range ? S.triples[tt] : 0;
         const int i = packed & 1023, j = (packed >> 10) & 1023, k = (packed >> 20) & 1023;
-        const bool ok = in_range && B < S.nb && C < S.nb && i < O && j < O && k < O && k <= i && s < TRPDRV_TMA_MAX_SYSTEMS;
+        // occupied slots of the i, j and k roles in the tensors (a one-triple system holds two slots)
+        const int one = S.one_triple;
+        const int zi = one ? 0 : i, zj = one ? 0 : j, zk = one ? 1 : k, zO = one ? 2 : O;
+        const bool ok = in_range && B < S.nb && C < S.nb && i < O && j < O && k < O && (one || k <= i) &&
+                        (!one || ai == 0) && s < TRPDRV_TMA_MAX_SYSTEMS;
         const int B0 = B * T, C0 = C * T;
         if (!ok) {
             if (!mbar_wait(&empty[stage], phase ^ 1, status)) return;
@@ -362,13 +366,13 @@ __device__ __forceinline__ void producer(const trpdrv_dev_system *__restrict__ s
         const bool diag = (B == C);
         if (lane == 0) {
             cx.eorb = S.eorb;
-            const size_t ao = (size_t)ai * O;  // the a block of the a-dependent vectors
-            cx.dintc1 = S.dintc + (ao + i) * V;
-            cx.dintx1 = S.dintx + (ao + i) * V;
-            cx.t1v1 = S.t1v + (ao + i) * V;
-            cx.dintc2 = S.dintc + (ao + k) * V;
-            cx.dintx2 = S.dintx + (ao + k) * V;
-            cx.t1v2 = S.t1v + (ao + k) * V;
+            const size_t ao = (size_t)ai * zO;  // the a block of the a-dependent vectors
+            cx.dintc1 = S.dintc + (ao + zi) * V;
+            cx.dintx1 = S.dintx + (ao + zi) * V;
+            cx.t1v1 = S.t1v + (ao + zi) * V;
+            cx.dintc2 = S.dintc + (ao + zk) * V;
+            cx.dintx2 = S.dintx + (ao + zk) * V;
+            cx.t1v2 = S.t1v + (ao + zk) * V;
             cx.out = S.partial + (size_t)own * NCW * 4;
             // omp/ccsd_trpdrv_omp_cbody.c:126 (a is 1-based, i/j/k here 0-based)
             cx.eaijk = S.eorb[S.a - 1 + ai] - (S.eorb[S.ncor + i] + S.eorb[S.ncor + j] + S.eorb[S.ncor + k]);
@@ -385,9 +389,9 @@ __device__ __forceinline__ void producer(const trpdrv_dev_system *__restrict__ s
 
         // per-lane box: A_J (slots 0,1), A_K (2,3) rows; B_1 (4,5) and B_3 (6) columns
         const CUtensorMap *mp = maps.m[s];
-        const int za = fam ? k : i;                      // A operands: Jia/Kia (n), Jka/Kka (t)
-        const int zaj = za + (int)ai * O;                // J/K carry the a index, -T/-X do not
-        const int zb = fam ? j * O + i : j * O + k;      // B operands: Tkj/Kkj/Jkj (n), Tij/Kij/Jij (t)
+        const int za = fam ? zk : zi;                    // A operands: Jia/Kia (n), Jka/Kka (t)
+        const int zaj = za + (int)ai * zO;               // J/K carry the a index, -T/-X do not
+        const int zb = fam ? zj * zO + zi : zj * zO + zk;  // B operands: Tkj/Kkj/Jkj (n), Tij/Kij/Jij (t)
         const int ra = o ? C0 : B0;                      // A rows: B for (B,C), C for (C,B)
         const int cb = o ? B0 : C0;                      // B columns: C for (B,C), B for (C,B)
         const int half = slot & 1;                       // second 16-row box of a K-major panel
@@ -665,14 +669,17 @@ extern "C" int trpdrv_tma_prepare(const trpdrv_dev_system *h_sys, int nsys, void
     memset(M, 0, sizeof(*M));
     for (int s = 0; s < nsys && s < TRPDRV_TMA_MAX_SYSTEMS; ++s) {
         const trpdrv_dev_system &S = h_sys[s];
-        const unsigned long long V = S.nvir, O = S.nocc, O2 = O * O;
+        const unsigned long long V = S.nvir, O = S.nocc;
+        // occupied slots along the block dimension: nocc (x nocc for the j-blocked tensors), or the
+        // two slots (one j block) of a one-triple system
+        const unsigned long long X = S.one_triple ? 2 : O, O2 = S.one_triple ? 2 : O * O;
         CUtensorMap *m = M->m[s];
         int e = 0;
-        const unsigned long long OA = O * (unsigned long long)(S.n_a > 0 ? S.n_a : 1);
+        const unsigned long long OA = X * (unsigned long long)(S.n_a > 0 ? S.n_a : 1);
         e |= tma::make_map(&m[tma::M_J], S.jvv, V, V, OA, 16, tma::DK, true);    // [a][i][d][b]
         e |= tma::make_map(&m[tma::M_K], S.kvv, V, V, OA, 16, tma::DK, true);
-        e |= tma::make_map(&m[tma::M_NT], S.ntov, V, O, O, 16, tma::DK, true);  // [i][m][b]
-        e |= tma::make_map(&m[tma::M_NX], S.nxov, V, O, O, 16, tma::DK, true);
+        e |= tma::make_map(&m[tma::M_NT], S.ntov, V, O, X, 16, tma::DK, true);  // [i][m][b]
+        e |= tma::make_map(&m[tma::M_NX], S.nxov, V, O, X, 16, tma::DK, true);
         e |= tma::make_map(&m[tma::M_T2K], S.t2, V, V, O2, 16, tma::DK, true);  // [jx][d][c]: T(c,d)
         e |= tma::make_map(&m[tma::M_T2X], S.t2, V, V, O2, tma::DK, 32, true); // [jx][c][d]: T(d,c)
         e |= tma::make_map(&m[tma::M_JOV], S.jov, O, V, O2, tma::DK, 32, true);  // [jx][c][m]

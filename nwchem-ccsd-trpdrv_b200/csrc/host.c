@@ -7,12 +7,16 @@
 #include "launch.h"
 
 #include <cuda_runtime_api.h>
+#include <fcntl.h>
 #include <math.h>
+#include <omp.h>
 #include <pthread.h>
 #include <stdarg.h>
 #include <stdio.h>
 #include <stdlib.h>
 #include <string.h>
+#include <sys/file.h>
+#include <unistd.h>
 
 int trpdrv_fused_init(void);
 int trpdrv_plain_init(void);
@@ -1142,6 +1146,81 @@ static int tune_same(const tune_entry *a, const tune_entry *b)
            a->rank == b->rank && a->nsys == b->nsys && a->staging == b->staging && memcmp(a->shape, b->shape, sizeof a->shape) == 0;
 }
 
+/* ---- persistent tuning cache (TRPDRV_TUNE_CACHE = path of a text file shared by processes) ----
+ * One line per choice: "<key> -> <staging> <mma_k> <ctas_per_sm> <batch> <ms>", where the key names
+ * the device model (name, SM count), the library version and every field of tune_entry.  Lookups
+ * take the last matching line; stores append under an exclusive lock. */
+static int tune_file_key(const trpdrv_plan *p, const tune_entry *k, char *buf, size_t n)
+{
+    struct cudaDeviceProp prop;
+    if (cudaGetDeviceProperties(&prop, p->device) != cudaSuccess) return -1;
+    char name[96];
+    size_t q = 0;
+    for (const char *c = prop.name; *c && q + 1 < sizeof name; ++c) name[q++] = (*c == ' ' || *c == '>') ? '_' : *c;
+    name[q] = '\0';
+    int w = snprintf(buf, n, "trpdrv-tune v%d %s sm%d mode=%d slices=%d world=%d rank=%d staging=%d nsys=%d shapes=",
+                     trpdrv_version(), name, prop.multiProcessorCount, k->mode, k->slices, k->world, k->rank,
+                     k->staging, k->nsys);
+    for (int s = 0; s < k->nsys && s < TRPDRV_TMA_MAX_SYSTEMS && w > 0 && (size_t)w < n; ++s)
+        w += snprintf(buf + w, n - (size_t)w, "%s%d,%d,%d", s ? ";" : "", k->shape[3 * s], k->shape[3 * s + 1],
+                      k->shape[3 * s + 2]);
+    return (w > 0 && (size_t)w < n) ? 0 : -1;
+}
+
+static int tune_file_lookup(const char *key, trpdrv_tune_candidate *out)
+{
+    const char *path = getenv("TRPDRV_TUNE_CACHE");
+    if (!path || !*path) return 0;
+    FILE *f = fopen(path, "r");
+    if (!f) return 0;
+    flock(fileno(f), LOCK_SH);
+    char line[1024];
+    const size_t kl = strlen(key);
+    int found = 0;
+    while (fgets(line, sizeof line, f)) {
+        if (strncmp(line, key, kl) != 0 || strncmp(line + kl, " -> ", 4) != 0) continue;
+        trpdrv_tune_candidate c;
+        memset(&c, 0, sizeof c);
+        if (sscanf(line + kl + 4, "%d %d %d %d %lf", &c.staging, &c.mma_k, &c.ctas_per_sm, &c.batch, &c.ms_estimate) ==
+            5) {
+            *out = c;
+            found = 1;
+        }
+    }
+    flock(fileno(f), LOCK_UN);
+    fclose(f);
+    return found;
+}
+
+static void tune_file_store(const char *key, const trpdrv_tune_candidate *c)
+{
+    const char *path = getenv("TRPDRV_TUNE_CACHE");
+    if (!path || !*path) return;
+    const int fd = open(path, O_WRONLY | O_APPEND | O_CREAT, 0644);
+    if (fd < 0) return;
+    char line[1200];
+    const int n = snprintf(line, sizeof line, "%s -> %d %d %d %d %.6f\n", key, c->staging, c->mma_k, c->ctas_per_sm,
+                           c->batch, c->ms_estimate);
+    if (n > 0 && (size_t)n < sizeof line && flock(fd, LOCK_EX) == 0) {
+        ssize_t wr = write(fd, line, (size_t)n);
+        (void)wr;
+        flock(fd, LOCK_UN);
+    }
+    close(fd);
+}
+
+/* a cached choice is usable only if this plan can run it */
+static int tune_usable(const trpdrv_plan *p, const trpdrv_tune_candidate *c)
+{
+    if (p->opt.mode == TRPDRV_MODE_FUSED) {
+        if (c->staging == 2)
+            return p->opt.staging != 1 && p->tma_maps && trpdrv_tma_supported(p->h_dev, p->nsys) &&
+                   (c->mma_k == 8 || c->mma_k == 16);
+        return c->staging == 1 && p->opt.staging != 2 && (c->mma_k == 4 || c->mma_k == 8) && c->ctas_per_sm >= 1;
+    }
+    return c->batch >= 1 && c->batch <= p->fbuf_batch;
+}
+
 /* sets the plan's launch configuration to candidate c */
 static void tune_apply(trpdrv_plan *p, const trpdrv_tune_candidate *c)
 {
@@ -1362,14 +1441,32 @@ int trpdrv_plan_autotune(trpdrv_plan *p, trpdrv_tune_result *result)
         memset(&best, 0, sizeof best);
         if (hit >= 0) best = g_tune[hit].best;
         pthread_mutex_unlock(&g_tune_mu);
-        /* a cached TMA choice applies only where this plan can stage with TMA */
-        if (hit >= 0 && best.staging == 2 && !(p->tma_maps && trpdrv_tma_supported(p->h_dev, p->nsys))) hit = -1;
+        /* a cached choice applies only where this plan can run it */
+        if (hit >= 0 && !tune_usable(p, &best)) hit = -1;
         if (hit >= 0) {
             r->ncand = 1;
             r->chosen = 0;
             r->from_cache = 1;
             r->cand[0] = best;
             tune_apply(p, &best);
+            return TRPDRV_OK;
+        }
+        char fkey[768];
+        if (tune_file_key(p, &key, fkey, sizeof fkey) == 0 && tune_file_lookup(fkey, &best) && tune_usable(p, &best)) {
+            r->ncand = 1;
+            r->chosen = 0;
+            r->from_cache = 2;
+            r->cand[0] = best;
+            tune_apply(p, &best);
+            pthread_mutex_lock(&g_tune_mu);
+            int slot = -1;
+            for (int e = 0; e < (int)(sizeof g_tune / sizeof g_tune[0]) && slot < 0; ++e)
+                if (!g_tune[e].used) slot = e;
+            if (slot < 0) slot = 0;
+            g_tune[slot] = key;
+            g_tune[slot].used = 1;
+            g_tune[slot].best = best;
+            pthread_mutex_unlock(&g_tune_mu);
             return TRPDRV_OK;
         }
     }
@@ -1418,6 +1515,8 @@ int trpdrv_plan_autotune(trpdrv_plan *p, trpdrv_tune_result *result)
         g_tune[slot].used = 1;
         g_tune[slot].best = c[best];
         pthread_mutex_unlock(&g_tune_mu);
+        char fkey[768];
+        if (tune_file_key(p, &key, fkey, sizeof fkey) == 0) tune_file_store(fkey, &c[best]);
     }
     return TRPDRV_OK;
 }
@@ -1495,10 +1594,13 @@ static const double *reg_lookup(const double *p, size_t n)
     return NULL;
 }
 
+static void dif_release(void);
+
 static void di_release(void)
 {
     if (!g_di.ready) return;
     cudaSetDevice(g_di.device);
+    dif_release();
     reg_release();
     for (int q = 0; q < DI_NVV; ++q) cudaFree(g_di.vv[q]);
     for (int q = 0; q < DO_NOV; ++q) cudaFree(g_di.ov[q]);
@@ -1687,6 +1789,205 @@ static int di_tengy_launch(int ncor, int nocc, int nvir, double eaijk, const dou
     return TRPDRV_OK;
 }
 
+/* ---- the drop-in body on the fused TMA kernel --------------------------------------------
+ * One call stages its triple's inputs into a fixed "one-triple system" (trpdrv_dev_system with
+ * one_triple = 1): the i-role block of every tensor at occupied slot 0 and the k-role block at slot
+ * 1.  Host inputs go through a pinned mirror of that layout (copied by several host threads, then one
+ * host->device copy); inputs inside registered arrays are gathered device->device in one launch.
+ * Then one negate launch (-tov, -xov), one fused launch (one work item per tile pair, f never leaves
+ * the SMs), one per-triple reduction, and a 48-byte read of the record and the kernel status. */
+enum { DS_HDR, DS_T2, DS_JVV, DS_KVV, DS_TOV, DS_XOV, DS_JOV, DS_KOV, DS_DINTC, DS_DINTX, DS_T1V, DS_EORB,
+       DS_NTOV, DS_NXOV, DS_END };
+#define DS_HDR_DOUBLES 64 /* the system descriptor and the packed triple, 512 bytes */
+
+static struct dropin_fused {
+    int ready, ncor, nocc, nvir, nsm;
+    size_t off[DS_END + 1]; /* element offsets of the staging layout; off[DS_NTOV] ends the host part */
+    double *d_block, *h_block;
+    trpdrv_dev_system h_sys;
+    double *d_partial;
+    double *d_io, *h_io; /* rec[4], counter (as 8 bytes), status (as int) */
+    void *maps;
+} g_dif;
+
+static void dif_release(void)
+{
+    if (!g_dif.ready) return;
+    cudaFree(g_dif.d_block);
+    cudaFreeHost(g_dif.h_block);
+    cudaFree(g_dif.d_partial);
+    cudaFree(g_dif.d_io);
+    cudaFreeHost(g_dif.h_io);
+    free(g_dif.maps);
+    memset(&g_dif, 0, sizeof g_dif);
+}
+
+/* The fused drop-in path needs what the TMA kernel needs: even nvir and nocc (16-byte rows). */
+static int dif_eligible(int nocc, int nvir) { return !(nocc & 1) && !(nvir & 1); }
+
+static int dif_prepare(int ncor, int nocc, int nvir)
+{
+    if (g_dif.ready && g_dif.ncor == ncor && g_dif.nocc == nocc && g_dif.nvir == nvir) return TRPDRV_OK;
+    dif_release();
+    const size_t vv = (size_t)nvir * nvir, ov = (size_t)nocc * nvir, v = (size_t)nvir;
+    const size_t len[DS_END] = {DS_HDR_DOUBLES, 2 * vv, 2 * vv, 2 * vv, 2 * ov, 2 * ov, 2 * ov, 2 * ov,
+                                2 * v,          2 * v,  2 * v,  (size_t)(ncor + nocc + nvir), 2 * ov, 2 * ov};
+    size_t o = 0;
+    for (int q = 0; q < DS_END; ++q) {
+        if (q == DS_NTOV) o = (o + 31) & ~(size_t)31; /* device-only part on a 256-byte boundary */
+        g_dif.off[q] = o;
+        o += len[q];
+    }
+    g_dif.off[DS_END] = o;
+    const int nb = (nvir + TRPDRV_TILE - 1) / TRPDRV_TILE, npairs = nb * (nb + 1) / 2;
+    int dev = 0, nsm = 0;
+    TRY(ensure_device(g_di.device, &dev, &nsm));
+    CUDA_TRY(cudaMalloc((void **)&g_dif.d_block, sizeof(double) * o));
+    CUDA_TRY(cudaMallocHost((void **)&g_dif.h_block, sizeof(double) * g_dif.off[DS_NTOV]));
+    CUDA_TRY(cudaMalloc((void **)&g_dif.d_partial, sizeof(double) * 4 * TRPDRV_FUSED_SLOTS * (size_t)npairs));
+    CUDA_TRY(cudaMalloc((void **)&g_dif.d_io, sizeof(double) * 8));
+    CUDA_TRY(cudaMallocHost((void **)&g_dif.h_io, sizeof(double) * 8));
+    g_dif.ready = 1; /* from here dif_release frees whatever was allocated */
+    double *d = g_dif.d_block;
+    trpdrv_dev_system *S = &g_dif.h_sys;
+    memset(S, 0, sizeof *S);
+    S->ncor = ncor;
+    S->nocc = nocc;
+    S->nvir = nvir;
+    S->nb = nb;
+    S->npairs = npairs;
+    S->ntriples = 1;
+    S->nt = 1;
+    S->n_a = 1;
+    S->one_triple = 1;
+    S->item_begin = 0;
+    S->t2 = d + g_dif.off[DS_T2];
+    S->jvv = d + g_dif.off[DS_JVV];
+    S->kvv = d + g_dif.off[DS_KVV];
+    S->ntov = d + g_dif.off[DS_NTOV];
+    S->nxov = d + g_dif.off[DS_NXOV];
+    S->jov = d + g_dif.off[DS_JOV];
+    S->kov = d + g_dif.off[DS_KOV];
+    S->dintc = d + g_dif.off[DS_DINTC];
+    S->dintx = d + g_dif.off[DS_DINTX];
+    S->t1v = d + g_dif.off[DS_T1V];
+    S->eorb = d + g_dif.off[DS_EORB];
+    S->triples = (const int32_t *)(d + g_dif.off[DS_HDR]) + 2 * (sizeof(trpdrv_dev_system) / 8 + 1);
+    S->order = NULL;
+    S->partial = g_dif.d_partial;
+    S->rec = g_dif.d_io;
+    if (sizeof(trpdrv_dev_system) + 16 > DS_HDR_DOUBLES * sizeof(double))
+        return fail(TRPDRV_ERR_STATE, "drop-in staging header too small");
+    if (!trpdrv_tma_supported(S, 1)) return fail(TRPDRV_ERR_UNSUPPORTED, "TMA staging unavailable");
+    g_dif.maps = aligned_alloc(64, (trpdrv_tma_maps_bytes() + 63) & ~(size_t)63);
+    if (!g_dif.maps) return fail(TRPDRV_ERR_NOMEM, "host allocation failed");
+    const int e = trpdrv_tma_prepare(S, 1, g_dif.maps);
+    if (e) return fail(TRPDRV_ERR_CUDA, "tensor-map encoding failed (%d)", e);
+    g_dif.ncor = ncor;
+    g_dif.nocc = nocc;
+    g_dif.nvir = nvir;
+    g_dif.nsm = nsm;
+    return TRPDRV_OK;
+}
+
+/* Host threads for the staging copies: TRPDRV_STAGE_THREADS, else up to 8 of OpenMP's. */
+static int stage_threads(void)
+{
+    const char *v = getenv("TRPDRV_STAGE_THREADS");
+    int n = v ? atoi(v) : 0;
+    if (n <= 0) {
+        n = omp_get_max_threads();
+        if (n > 8) n = 8;
+    }
+    return n < 1 ? 1 : n;
+}
+
+typedef struct stage_piece {
+    double *dst;
+    const double *src;
+    size_t n;
+} stage_piece;
+
+/* Copies the pieces (split into blocks of at most 128 KB) with up to `threads` host threads. */
+static void stage_copy(const stage_piece *pc, int npc, int threads)
+{
+    enum { BLK = 16384 };
+    size_t total = 0;
+    int nblk = 0;
+    for (int q = 0; q < npc; ++q) {
+        total += pc[q].n;
+        nblk += (int)((pc[q].n + BLK - 1) / BLK);
+    }
+    if (threads <= 1 || total < 4 * BLK) {
+        for (int q = 0; q < npc; ++q) memcpy(pc[q].dst, pc[q].src, sizeof(double) * pc[q].n);
+        return;
+    }
+#pragma omp parallel for num_threads(threads) schedule(static)
+    for (int b = 0; b < nblk; ++b) {
+        int q = 0, r = b;
+        while (r >= (int)((pc[q].n + BLK - 1) / BLK)) {
+            r -= (int)((pc[q].n + BLK - 1) / BLK);
+            ++q;
+        }
+        const size_t lo = (size_t)r * BLK, n = pc[q].n - lo < BLK ? pc[q].n - lo : BLK;
+        memcpy(pc[q].dst + lo, pc[q].src + lo, sizeof(double) * n);
+    }
+}
+
+/* One triple through the fused kernel; rec[4] = emp4i, emp5i, emp4k, emp5k. */
+static int body_fused(int ncor, int nocc, int nvir, int a, int i, int j, int k, const double *const *in,
+                      const size_t *in_len, const int *in_slot, double *rec)
+{
+    TRY(dif_prepare(ncor, nocc, nvir));
+    cudaStream_t st = g_di.stream;
+    double *h = g_dif.h_block;
+    /* header: the system descriptor with this call's a, then the packed triple */
+    trpdrv_dev_system S = g_dif.h_sys;
+    S.a = a;
+    memcpy(h, &S, sizeof S);
+    ((int32_t *)h)[2 * (sizeof(trpdrv_dev_system) / 8 + 1)] = pack_triple(i, j, k);
+    stage_piece pc[24];
+    trpdrv_copy_list gl;
+    memset(&gl, 0, sizeof gl);
+    int npc = 0;
+    for (int q = 0; q < 21; ++q) {
+        const size_t dst = g_dif.off[in_slot[q] >> 1] + (size_t)(in_slot[q] & 1) * (in_len[q] == 0 ? 0 : in_len[q]);
+        const double *dsrc = reg_lookup(in[q], in_len[q]);
+        if (dsrc) {
+            gl.src[gl.n] = dsrc;
+            gl.dst[gl.n] = g_dif.d_block + dst;
+            gl.len[gl.n] = (long long)in_len[q];
+            ++gl.n;
+        } else {
+            pc[npc].dst = h + dst;
+            pc[npc].src = in[q];
+            pc[npc].n = in_len[q];
+            ++npc;
+        }
+    }
+    stage_copy(pc, npc, stage_threads());
+    const size_t up = npc ? g_dif.off[DS_NTOV] : (size_t)DS_HDR_DOUBLES;
+    CUDA_TRY(cudaMemcpyAsync(g_dif.d_block, h, sizeof(double) * up, cudaMemcpyHostToDevice, st));
+    if (gl.n) LAUNCH_TRY(trpdrv_launch_gather(&gl, st));
+    CUDA_TRY(cudaMemsetAsync(g_dif.d_io + 4, 0, 2 * sizeof(double), st));
+    /* -tia, -tka, -xia, -xka: tov|xov and ntov|nxov are adjacent */
+    LAUNCH_TRY(trpdrv_launch_negate(g_dif.d_block + g_dif.off[DS_TOV], g_dif.d_block + g_dif.off[DS_NTOV],
+                                    4 * (size_t)nocc * nvir, st));
+    const int npairs = g_dif.h_sys.npairs;
+    const int grid = npairs < g_dif.nsm ? npairs : g_dif.nsm;
+    const trpdrv_dev_system *d_sys = (const trpdrv_dev_system *)(g_dif.d_block + g_dif.off[DS_HDR]);
+    LAUNCH_TRY(trpdrv_launch_fused_tma(d_sys, 1, npairs, (unsigned long long *)(g_dif.d_io + 4), (int *)(g_dif.d_io + 5),
+                                       grid, g_dif.maps, 8, st));
+    LAUNCH_TRY(trpdrv_launch_item_reduce(&g_dif.h_sys, st));
+    CUDA_TRY(cudaMemcpyAsync(g_dif.h_io, g_dif.d_io, 6 * sizeof(double), cudaMemcpyDeviceToHost, st));
+    CUDA_TRY(cudaStreamSynchronize(st));
+    int status = 0;
+    memcpy(&status, g_dif.h_io + 5, sizeof status);
+    if (status) return fail(TRPDRV_ERR_DEVICE, "fused kernel reported status %d", status);
+    for (int q = 0; q < 4; ++q) rec[q] = g_dif.h_io[q];
+    return TRPDRV_OK;
+}
+
 /* omp/ccsd_trpdrv_omp_cbody.c:31-145 on the device, for one triple from host buffers. */
 static int body_impl(double *f1n, double *f1t, double *f2n, double *f2t, double *f3n, double *f3t, double *f4n,
                      double *f4t, double *eorb, int *ncor_, int *nocc_, int *nvir_, double *emp4_, double *emp5_,
@@ -1717,6 +2018,33 @@ static int body_impl(double *f1n, double *f1t, double *f2n, double *f2t, double 
     TRY(di_reserve(nocc, nvir, nbf));
     const size_t lnvv = (size_t)nvir * nvir, lnov = (size_t)nocc * nvir;
     const size_t vv = (size_t)(k - klo) * lnvv, ov = (size_t)(k - klo) * lnov;
+
+    if (!write_f && dif_eligible(nocc, nvir) && !env_flag("TRPDRV_DROPIN_PATH", "plain")) {
+        /* the 21 input slices and their slots in the one-triple staging layout ((tensor << 1) | role) */
+        const double *in[21] = {tij, tkj + vv, jia, jka + vv, kia, kka + vv, tia, tka + ov, xia, xka + ov,
+                                jij, jkj + ov, kij, kkj + ov, dintc1, dintc2, dintx1, dintx2, t1v1, t1v2, eorb};
+        const size_t v = (size_t)nvir;
+        const size_t len[21] = {lnvv, lnvv, lnvv, lnvv, lnvv, lnvv, lnov, lnov, lnov, lnov,
+                                lnov, lnov, lnov, lnov, v, v, v, v, v, v, (size_t)nbf};
+        const int slot[21] = {DS_T2 << 1, DS_T2 << 1 | 1, DS_JVV << 1, DS_JVV << 1 | 1, DS_KVV << 1, DS_KVV << 1 | 1,
+                              DS_TOV << 1, DS_TOV << 1 | 1, DS_XOV << 1, DS_XOV << 1 | 1, DS_JOV << 1,
+                              DS_JOV << 1 | 1, DS_KOV << 1, DS_KOV << 1 | 1, DS_DINTC << 1, DS_DINTC << 1 | 1,
+                              DS_DINTX << 1, DS_DINTX << 1 | 1, DS_T1V << 1, DS_T1V << 1 | 1, DS_EORB << 1};
+        double rec[4];
+        TRY(body_fused(ncor, nocc, nvir, a, i, j, k, in, len, slot, rec));
+        /* omp/ccsd_trpdrv_omp_cbody.c:133-142 */
+        double emp4 = *emp4_, emp5 = *emp5_;
+        emp4 += rec[0];
+        emp5 += rec[1];
+        if (i != k) {
+            emp4 += rec[2];
+            emp5 += rec[3];
+        }
+        *emp4_ = emp4;
+        *emp5_ = emp5;
+        return TRPDRV_OK;
+    }
+
     const double *dv[DI_NVV], *dov[DO_NOV], *dvec[6], *deorb;
     TRY(h2d(&dv[DI_JIA], g_di.vv[DI_JIA], jia, lnvv));
     TRY(h2d(&dv[DI_KIA], g_di.vv[DI_KIA], kia, lnvv));

@@ -31,6 +31,11 @@ typedef struct trpdrv_dev_system {
     int64_t ntriples;    /* records of this system in the plan: n_a * nt */
     int64_t nt;          /* triples per a (this rank's share): the length of `triples` and `order` */
     int n_a;             /* virtual indices a .. a + n_a - 1 swept (1 = the reference driver's single a) */
+    int one_triple;      /* 1: the tensors hold only what one triple (i, j, k) reads, the i-role block at
+                            occupied slot 0 and the k-role block at slot 1 (t2, jov, kov: one j block
+                            of two slots; jvv, kvv, ntov, nxov, dintc, dintx, t1v: two slots), as the
+                            drop-in entry points stage them; `triples` holds that triple (its i, j, k
+                            give eaijk) and n_a is 1.  TMA kernel only. */
     int64_t item_begin;  /* first fused work item of this system */
     const double *eorb, *t2, *jvv, *kvv, *ntov, *nxov, *jov, *kov, *dintc, *dintx, *t1v;
     const int32_t *triples; /* packed triples, driver order (energies are stored in this order) */
@@ -102,6 +107,16 @@ int trpdrv_launch_system_reduce(const double *rec, const int32_t *triples, int64
 
 /* dst[i] = -src[i]. */
 int trpdrv_launch_negate(const double *src, double *dst, size_t n, void *stream);
+
+/* Device-to-device copies dst[s][0..len[s]) = src[s][..] for s < n, in one launch. */
+#define TRPDRV_COPY_LIST_MAX 24
+typedef struct trpdrv_copy_list {
+    int n;
+    const double *src[TRPDRV_COPY_LIST_MAX];
+    double *dst[TRPDRV_COPY_LIST_MAX];
+    long long len[TRPDRV_COPY_LIST_MAX];
+} trpdrv_copy_list;
+int trpdrv_launch_gather(const trpdrv_copy_list *list, void *stream);
 
 /* Plain per-triple path: one grouped launch computes the eight f = A1*op(B1) + A2*B2 into
  * f[8][nvir][nvir] (order f1n f2n f3n f4n f1t f2t f3t f4t); b1_nt[x] = 1 if B1 is used transposed. */

@@ -6,6 +6,8 @@
 //                        omp/ccsd_trpdrv_omp_cbody.c:133-142), as a double-double (hi, lo) pair,
 //                        built with error-free TwoSum in a fixed order.
 //  negate_kernel:        dst = -src (the occupied A operands are stored negated).
+//  gather_kernel:        a list of device-to-device copies in one launch (the drop-in entry points'
+//                        registered inputs, gathered into their staging layout).
 
 #include "device_common.cuh"
 #include "launch.h"
@@ -100,9 +102,42 @@ __global__ void negate_kernel(const double *__restrict__ src, double *__restrict
         dst[i] = -src[i];
 }
 
+// One row of the grid per segment; 16-byte copies when source and destination allow them.
+__global__ void gather_kernel(const trpdrv_copy_list L)
+{
+    const int s = blockIdx.y;
+    if (s >= L.n) return;
+    const double *src = L.src[s];
+    double *dst = L.dst[s];
+    const long long n = L.len[s];
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    const long long t0 = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (((reinterpret_cast<uintptr_t>(src) | reinterpret_cast<uintptr_t>(dst)) & 15u) == 0) {
+        const long long n2 = n >> 1;
+        for (long long q = t0; q < n2; q += stride)
+            reinterpret_cast<double2 *>(dst)[q] = __ldg(reinterpret_cast<const double2 *>(src) + q);
+        if ((n & 1) && t0 == 0) dst[n - 1] = src[n - 1];
+    } else {
+        for (long long q = t0; q < n; q += stride) dst[q] = src[q];
+    }
+}
+
 }  // namespace trpdrv
 
 using namespace trpdrv;
+
+extern "C" int trpdrv_launch_gather(const trpdrv_copy_list *list, void *stream)
+{
+    if (!list || list->n <= 0) return 0;
+    if (list->n > TRPDRV_COPY_LIST_MAX) return (int)cudaErrorInvalidValue;
+    long long longest = 0;
+    for (int s = 0; s < list->n; ++s) longest = list->len[s] > longest ? list->len[s] : longest;
+    long long bx = (longest / 2 + 255) / 256;
+    if (bx < 1) bx = 1;
+    if (bx > 64) bx = 64;
+    gather_kernel<<<dim3((unsigned)bx, (unsigned)list->n), 256, 0, (cudaStream_t)stream>>>(*list);
+    return (int)cudaGetLastError();
+}
 
 extern "C" int trpdrv_launch_item_reduce(const trpdrv_dev_system *h_sys, void *stream)
 {

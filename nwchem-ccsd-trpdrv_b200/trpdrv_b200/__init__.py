@@ -470,12 +470,13 @@ class Plan:
 
     def autotune(self) -> dict:
         """trpdrv_plan_autotune: times the compiled variants on a sample of this plan's work and keeps the
-        fastest.  Returns {"candidates": [...], "chosen": i, "from_cache": bool}."""
+        fastest.  Returns {"candidates": [...], "chosen": i, "from_cache": 0 timed now, 1 process cache, 2 file
+        cache (TRPDRV_TUNE_CACHE)}."""
         r = TuneResult()
         _check(lib.trpdrv_plan_autotune(self.h, C.byref(r)))
         cands = [{"staging": c.staging, "mma_k": c.mma_k, "ctas_per_sm": c.ctas_per_sm, "batch": c.batch,
                   "ms_estimate": c.ms_estimate} for c in r.cand[:r.ncand]]
-        return {"candidates": cands, "chosen": r.chosen, "from_cache": bool(r.from_cache), "slices": r.slices,
+        return {"candidates": cands, "chosen": r.chosen, "from_cache": int(r.from_cache), "slices": r.slices,
                 "est_rel_err": r.est_rel_err}
 
     def staging(self) -> int:

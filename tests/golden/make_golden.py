@@ -9,6 +9,9 @@ inputs, so a change of the generator is detected rather than silently changing t
 
 It also records the known-answer print of the reference driver itself:
     oracle/_ref/test_c99 10 60 100000   ->   "emp4=2.647247 emp5=-1.560018"
+and of the reference's single-precision variant (gpu-omp/test.c + gpu-omp/ccsd_trpdrv_omp_cbody.c,
+unmodified, host build; `python tests/golden/make_golden.py fp32` writes only this file):
+    oracle/_ref/test_fp32 10 60 100000  ->   kat_test_fp32_10_60.json
 
 Run from the repository root where the reference sources exist:
     make -C oracle && python tests/golden/make_golden.py
@@ -42,7 +45,25 @@ def checksums(s):
     return {n: [float(np.sum(a)), float(np.sum(a * a))] for n, a in s.arrays.items()}
 
 
+def fp32_kat(out_dir):
+    runs = []
+    for argv in (["10", "60", "100000"], ["10", "60", "100000", "3"], ["12", "50", "100000", "2"]):
+        kat = subprocess.run([os.path.join(os.path.dirname(O.REF_TEST), "test_fp32"), *argv], capture_output=True,
+                             text=True, check=True,
+                             env=dict(os.environ, OMP_NUM_THREADS="1", OPENBLAS_NUM_THREADS="1"))
+        line = [ln for ln in kat.stdout.splitlines() if ln.startswith("emp4=")][0]
+        runs.append({"argv": argv, "line": line})
+        print("fp32", argv, line)
+    with open(os.path.join(out_dir, "kat_test_fp32_10_60.json"), "w") as f:
+        json.dump({"command": "test_fp32 10 60 100000", "line": runs[0]["line"], "runs": runs,
+                   "source": "reference gpu-omp/test.c + gpu-omp/ccsd_trpdrv_omp_cbody.c (single precision), "
+                             "unmodified, host build with OpenBLAS sgemm"}, f, indent=1)
+
+
 def main():
+    if len(sys.argv) > 1 and sys.argv[1] == "fp32":
+        fp32_kat(os.path.dirname(os.path.abspath(__file__)))
+        return
     if os.environ.get("OMP_NUM_THREADS") != "1":
         # one OpenMP thread inside the reference tengy: a fixed reduction order, reproducible fixtures
         os.execvpe(sys.executable, [sys.executable, os.path.abspath(__file__)],
@@ -77,6 +98,7 @@ def main():
         json.dump({"command": "test_c99 10 60 100000", "line": runs[0]["line"], "runs": runs,
                    "source": "reference omp/test.c + omp/ccsd_trpdrv_omp_cbody.c + omp/ccsd_tengy_c99.c, unmodified"},
                   f, indent=1)
+    fp32_kat(out_dir)
 
 
 if __name__ == "__main__":

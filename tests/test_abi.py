@@ -93,3 +93,27 @@ def test_c_caller_of_the_plan_interface_compiles_and_links(tmp_path):
     """A C99 program using the plan interface (tests/c_plan_caller.c) builds against the header and links
     against libtrpdrv_b200.so; running it needs a GPU (tests/test_gpu_parity.py)."""
     assert os.access(_build_c_caller(tmp_path), os.X_OK)
+
+
+HEADER_FP32 = os.path.join(ROOT, "include", "trpdrv_fp32.h")
+LIB_FP32 = os.path.join(ROOT, "nwchem-ccsd-trpdrv_b200", "lib", "libtrpdrv_b200_fp32.so")
+
+
+def test_fp32_library_exports_exactly_its_header():
+    """libtrpdrv_b200_fp32.so (the FP32 parity form) exports the float entry points of
+    include/trpdrv_fp32.h (gpu-omp/ccsd_trpdrv_omp_cbody.c:38-51, gpu-omp/ccsd_tengy_c99.c:5-14) and
+    nothing else."""
+    text = re.sub(r"/\*.*?\*/", "", open(HEADER_FP32).read(), flags=re.S)
+    decl = set(re.findall(r"^\s*(?:void|int|const char \*)\s*([A-Za-z_][A-Za-z0-9_]*)\s*\(", text, flags=re.M))
+    assert {"ccsd_trpdrv_omp_cbody_", "ccsd_trpdrv_omp_fbody_", "ccsd_tengy_omp"} <= decl
+    out = subprocess.run(["nm", "-D", "--defined-only", LIB_FP32], capture_output=True, text=True, check=True).stdout
+    exported = {ln.split()[-1] for ln in out.splitlines() if " T " in ln}
+    assert exported == decl
+
+
+def test_fp32_header_compiles_as_c_and_cxx(tmp_path):
+    src = tmp_path / "t32.c"
+    src.write_text('#include "trpdrv_fp32.h"\nint main(void){return trpdrv_fp32_last_error();}\n')
+    for comp, extra in (("gcc", ["-std=c99"]), ("g++", ["-x", "c++"])):
+        subprocess.run([comp, *extra, "-I", os.path.join(ROOT, "include"), "-c", str(src), "-o",
+                        str(tmp_path / "t32.o")], check=True)

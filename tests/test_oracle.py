@@ -116,3 +116,18 @@ def test_oracle_timed_loop_accumulates_like_the_driver(O, which):
     e4, e5 = O.time_body(s, which, t_begin=0, t_end=n // 3)
     e4, e5 = O.time_body(s, which, t_begin=n // 3, t_end=n, emp4=e4, emp5=e5)
     assert abs(e4 - tot[0]) <= 1e-12 * abs(tot[0]) and abs(e5 - tot[1]) <= 1e-12 * abs(tot[1])
+
+
+@pytest.mark.skipif(not os.path.exists(os.path.join(os.path.dirname(GOLDEN), "..", "oracle", "_ref", "test_fp32")),
+                    reason="reference single-precision driver not built")
+def test_reference_fp32_driver_kat(O):
+    """The reference's single-precision variant (gpu-omp/test.c + gpu-omp/ccsd_trpdrv_omp_cbody.c, host
+    build) reproduces its recorded known answers (one OpenMP/OpenBLAS thread: its float sums run in a
+    fixed order)."""
+    with open(os.path.join(GOLDEN, "kat_test_fp32_10_60.json")) as f:
+        runs = json.load(f)["runs"]
+    exe = os.path.join(os.path.dirname(O.REF_TEST), "test_fp32")
+    for run in runs:
+        out = subprocess.run([exe, *run["argv"]], capture_output=True, text=True, check=True,
+                             env=dict(os.environ, OMP_NUM_THREADS="1", OPENBLAS_NUM_THREADS="1"))
+        assert run["line"] in out.stdout and "SUCCESS" in out.stdout

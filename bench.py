@@ -850,7 +850,8 @@ def run_b200_arm(args):
         line = base_line(args, R, value, sec, config_for(args))
         line.update({
             "dtype": "f64",
-            "fused_mma": f"m16n8k{args.mma_k} f64",
+            "fused_mma": (f"m16n8k{tune['candidates'][tune['chosen']]['mma_k']} f64 (autotuned)"
+                          if tune and tune.get("candidates") else f"m16n8k{args.mma_k} f64"),
             "tflops_fp64_equiv": flop_all / sec / 1e12,
             "roofline": fp64_roofline(achieved, peak, traffic, kms),
             "fp64_probe_tflops": fp64_probe,

@@ -71,10 +71,22 @@ struct __align__(64) Maps {
 
 struct ItemCtx {
     const double *eorb, *dintc1, *dintx1, *t1v1, *dintc2, *dintx2, *t1v2;
-    double *out;
+    double *out, *out1;  // energy slots of the item's pair (and of the second pair of a packed item)
     double eaijk;
     int ncor, nocc, nvir, b0, c0, diag, nV, nch, state;  // state: 1 work, 0 malformed, -1 end
+    int packed, b1;      // packed edge item: pairs (b0, c0) and (b1, c0); b1 < 0 when the second is absent
 };
+
+// Packed edge items (systems with pack_edge: the last column tile E holds 1..16 valid indices).  The
+// pairs (B, E) and (B + 1, E), B even, run as one item: each family of a chunk gets its own stage
+// slot, in which the 4 KB panels are
+//   0, 1: J (or -T) rows of B and B + 1      2, 3: K (or -X) rows of B and B + 1   (K-major, 2 boxes)
+//   4: B_1 columns of E (1 K-major box, or 1 X-major box)   5: B_3 columns of E (X-major)
+//   6, 7: J / K (or -T / -X) rows of E (1 K-major box each)
+//   8, 9: B_1 columns of B and B + 1 (2 K-major boxes, or 1 X-major)   10, 11: B_3 columns (X-major)
+// and warp w computes pair w >> 2, rows 16 ((w & 3) >> 1) and columns 8 (w & 1) of it: the work of one
+// full pair over 8 warps instead of two half-idle pairs.
+constexpr int PK_A = 0, PK_B1E = 4, PK_B3E = 5, PK_AE = 6, PK_B1B = 8, PK_B3B = 10;
 
 // ------------------------------------------------------------------------------------------------
 // PTX helpers
@@ -227,6 +239,76 @@ __device__ __forceinline__ void ld_b16_X(const FragOffsets &fo, double (&b)[4], 
     fo.ldB_X(*reinterpret_cast<double(*)[2]>(&b[2]), P, 64);
 }
 
+// One family's products of a packed edge item in one stage slot (layout at PK_*): this warp's
+// sub-block of pair pp, f_x(b,c) = A_x(b,.) B_x(.,c) and f_x(c,b) through the operand-swapped MMA,
+// exactly as the normal items compute them from their o = 0 / o = 1 panels.
+template <int KS, int FAM>
+__device__ __forceinline__ void packed_family(const FragOffsets &fo, const char *st, int pp, bool ph1, int kval,
+                                              double (&f)[8][4], double (&gT)[8][4])
+{
+    constexpr int x0 = FAM * 4;
+    const char *AJ = st + (PK_A + pp) * PANEL_BYTES, *AK = st + (PK_A + 2 + pp) * PANEL_BYTES;
+    const char *B1 = st + PK_B1E * PANEL_BYTES, *B3 = st + PK_B3E * PANEL_BYTES;
+    const char *AJE = st + PK_AE * PANEL_BYTES, *AKE = st + (PK_AE + 1) * PANEL_BYTES;
+    const char *B1B = st + (PK_B1B + pp) * PANEL_BYTES, *B3B = st + (PK_B3B + pp) * PANEL_BYTES;
+    if (KS == 16 && kval > 8) {
+        double aJ[8], aK[8], b1[4], b3[4];
+        ld_a16_K(fo, aJ, AJ);
+        ld_a16_K(fo, aK, AK);
+        ld_b16_X(fo, b3, B3);
+        if (!ph1)
+            ld_b16_K(fo, b1, B1);
+        else
+            ld_b16_X(fo, b1, B1);
+        dmma_16x8x16(f[x0 + 0], aJ, b1);
+        dmma_16x8x16(f[x0 + 1], aK, b1);
+        dmma_16x8x16(f[x0 + 2], aJ, b3);
+        dmma_16x8x16(f[x0 + 3], aK, b3);
+        double a1[8], a3[8], bJ[4], bK[4];
+        ld_b16_K(fo, bJ, AJE);
+        ld_b16_K(fo, bK, AKE);
+        ld_a16_X(fo, a3, B3B);
+        if (!ph1)
+            ld_a16_K(fo, a1, B1B);
+        else
+            ld_a16_X(fo, a1, B1B);
+        dmma_16x8x16(gT[x0 + 0], a1, bJ);
+        dmma_16x8x16(gT[x0 + 1], a1, bK);
+        dmma_16x8x16(gT[x0 + 2], a3, bJ);
+        dmma_16x8x16(gT[x0 + 3], a3, bK);
+    } else {
+#pragma unroll
+        for (int ks = 0; ks < 2; ++ks) {
+            if (ks == 1 && kval <= 8) break;
+            const int kk = ks * 1024, kx = ks * 64;
+            double aJ[4], aK[4], b1[2], b3[2];
+            fo.ldA_K(aJ, AJ + kk);
+            fo.ldA_K(aK, AK + kk);
+            fo.ldB_X(b3, B3, kx);
+            if (!ph1)
+                fo.ldB_K(b1, B1 + kk);
+            else
+                fo.ldB_X(b1, B1, kx);
+            dmma_16x8x8(f[x0 + 0], aJ, b1);
+            dmma_16x8x8(f[x0 + 1], aK, b1);
+            dmma_16x8x8(f[x0 + 2], aJ, b3);
+            dmma_16x8x8(f[x0 + 3], aK, b3);
+            double a1[4], a3[4], bJ[2], bK[2];
+            fo.ldB_K(bJ, AJE + kk);
+            fo.ldB_K(bK, AKE + kk);
+            fo.ldA_X(a3, B3B, kx);
+            if (!ph1)
+                fo.ldA_K(a1, B1B + kk);
+            else
+                fo.ldA_X(a1, B1B, kx);
+            dmma_16x8x8(gT[x0 + 0], a1, bJ);
+            dmma_16x8x8(gT[x0 + 1], a1, bK);
+            dmma_16x8x8(gT[x0 + 2], a3, bJ);
+            dmma_16x8x8(gT[x0 + 3], a3, bK);
+        }
+    }
+}
+
 // Brings the 128-byte lines of the energy vectors the item's epilogue will read into L1 (lanes 0..27:
 // 7 vectors x {B, C} block x 2 lines), so the register epilogue does not wait on L2.
 __device__ __forceinline__ void prefetch_epilogue(const ItemCtx &cx, int lane)
@@ -306,7 +388,7 @@ __device__ __forceinline__ void producer(const trpdrv_dev_system *__restrict__ s
     long long next = 0;
     if (lane == 0) next = (long long)atomicAdd(counter, 1ULL);
     next = __shfl_sync(FULL, next, 0);
-    for (long long n = 0;; ++n) {
+    for (long long n = 0;;) {
         const long long item = next;
         if (item < total) {  // ticket for the following item, early
             if (lane == 0) next = (long long)atomicAdd(counter, 1ULL);
@@ -337,6 +419,9 @@ __device__ __forceinline__ void producer(const trpdrv_dev_system *__restrict__ s
             ++B;
         }
         const int C = B + rem;
+        // edge pairs (B, E) with B odd are computed by the packed item of B - 1
+        const bool pack = S.pack_edge && C == S.nb - 1 && B < C;
+        if (pack && (B & 1)) continue;
         const int O = S.nocc, V = S.nvir;
         const bool in_range = local >= 0 && qpos < S.ntriples && tt >= 0 && tt < S.nt && ai < S.n_a;
         const int packed = in_range ? S.triples[tt] : 0;
@@ -352,6 +437,7 @@ __device__ __forceinline__ void producer(const trpdrv_dev_system *__restrict__ s
             if (lane == 0) {
                 atomicOr(status, 1);
                 cx.state = 0;
+                cx.packed = 0;
                 cx.out = in_range ? S.partial + (size_t)own * NCW * 4 : nullptr;
                 cx.nch = 0;
                 mbar_arrive(&full[stage]);
@@ -360,6 +446,7 @@ __device__ __forceinline__ void producer(const trpdrv_dev_system *__restrict__ s
                 stage = 0;
                 phase ^= 1;
             }
+            ++n;
             continue;
         }
         const int nV = (V + DK - 1) / DK, nO = (O + DK - 1) / DK;
@@ -374,6 +461,12 @@ __device__ __forceinline__ void producer(const trpdrv_dev_system *__restrict__ s
             cx.dintx2 = S.dintx + (ao + zk) * V;
             cx.t1v2 = S.t1v + (ao + zk) * V;
             cx.out = S.partial + (size_t)own * NCW * 4;
+            // the second pair (B2, E) of a packed item: its own slots, at its triangular pair index
+            // (B2 = B + 1: nb - B - 1 pairs further)
+            const bool two = pack && B + 1 < C;
+            cx.out1 = cx.out + (two ? (S.nb - B - 1) * NCW * 4 : 0);
+            cx.packed = pack;
+            cx.b1 = two ? (B + 1) * T : -1;
             // omp/ccsd_trpdrv_omp_cbody.c:126 (a is 1-based, i/j/k here 0-based)
             cx.eaijk = S.eorb[S.a - 1 + ai] - (S.eorb[S.ncor + i] + S.eorb[S.ncor + j] + S.eorb[S.ncor + k]);
             cx.ncor = S.ncor;
@@ -387,8 +480,77 @@ __device__ __forceinline__ void producer(const trpdrv_dev_system *__restrict__ s
             cx.state = 1;
         }
 
-        // per-lane box: A_J (slots 0,1), A_K (2,3) rows; B_1 (4,5) and B_3 (6) columns
         const CUtensorMap *mp = maps.m[s];
+        if (pack) {
+            // one stage slot per (chunk, family); lanes 0..17 each own at most one box of the layout at
+            // PK_*: kind 0 / 1 = J / K-role A rows (K-major), 2 = B_1 columns, 3 = B_3 columns (X-major)
+            const int E = C, B2 = B + 1 < C ? B + 1 : -1;
+            int kind = 3, tb = -1, half = 0, off = 0;
+            if (lane < 8) {
+                const int pnl = lane >> 1;
+                kind = pnl >> 1;
+                tb = (pnl & 1) ? B2 : B;
+                half = lane & 1;
+                off = (PK_A + pnl) * PANEL_BYTES + half * KBOX;
+            } else if (lane < 12) {
+                kind = lane == 8 ? 2 : lane == 9 ? 3 : lane - 10;
+                tb = E;
+                off = (lane == 8 ? PK_B1E : lane == 9 ? PK_B3E : PK_AE + lane - 10) * PANEL_BYTES;
+            } else if (lane < 18) {
+                const int pp = lane < 16 ? (lane - 12) >> 1 : lane - 16;
+                kind = lane < 16 ? 2 : 3;
+                tb = pp ? B2 : B;
+                half = lane < 16 ? (lane & 1) : 0;
+                off = (lane < 16 ? PK_B1B + pp : PK_B3B + pp) * PANEL_BYTES + half * KBOX;
+            }
+            tb = tb >= 0 ? tb * T : -1;
+            const int nsl = 2 * (nV + nO);
+            for (int sl = 0; sl < nsl; ++sl) {
+                if (!mbar_wait(&empty[stage], phase ^ 1, status)) return;
+                const int fam = sl & 1, ch = sl >> 1;
+                const bool ph1 = ch >= nV;
+                const int kk0 = (ph1 ? ch - nV : ch) * DK;
+                const int za = fam ? zk : zi;
+                const int zb = fam ? zj * zO + zi : zj * zO + zk;
+                const CUtensorMap *m = nullptr;
+                int x = kk0, y = tb, z = zb;
+                unsigned bytes = 0;
+                if (tb >= 0) {
+                    if (kind < 2) {  // A rows: J / K (virtual), -T / -X (occupied)
+                        m = &mp[ph1 ? (kind ? M_NX : M_NT) : (kind ? M_K : M_J)];
+                        x = tb + 16 * half;
+                        y = kk0;
+                        z = ph1 ? za : za + (int)ai * zO;
+                        bytes = KBOX;
+                    } else if (kind == 2) {  // B_1 columns: T(c,d) K-major boxes, or one K(m,c) X-major box
+                        if (!ph1) {
+                            m = &mp[M_T2K];
+                            x = tb + 16 * half;
+                            y = kk0;
+                            bytes = KBOX;
+                        } else if (half == 0) {
+                            m = &mp[M_KOV];
+                            bytes = PANEL_BYTES;
+                        }
+                    } else {  // B_3 columns: T(d,c) / J(m,c), X-major
+                        m = &mp[ph1 ? M_JOV : M_T2X];
+                        bytes = PANEL_BYTES;
+                    }
+                }
+                const unsigned total = __reduce_add_sync(FULL, bytes);
+                if (lane == 0) mbar_arrive_expect_tx(&full[stage], total);
+                __syncwarp();
+                if (m) tma_load_3d(stages + (size_t)stage * STAGE_BYTES + off, m, &full[stage], x, y, z);
+                if (++stage == STAGES) {
+                    stage = 0;
+                    phase ^= 1;
+                }
+            }
+            ++n;
+            continue;
+        }
+
+        // per-lane box: A_J (slots 0,1), A_K (2,3) rows; B_1 (4,5) and B_3 (6) columns
         const int za = fam ? zk : zi;                    // A operands: Jia/Kia (n), Jka/Kka (t)
         const int zaj = za + (int)ai * zO;               // J/K carry the a index, -T/-X do not
         const int zb = fam ? zj * zO + zi : zj * zO + zk;  // B operands: Tkj/Kkj/Jkj (n), Tij/Kij/Jij (t)
@@ -423,6 +585,7 @@ __device__ __forceinline__ void producer(const trpdrv_dev_system *__restrict__ s
                 phase ^= 1;
             }
         }
+        ++n;
     }
 }
 
@@ -488,6 +651,43 @@ fused_tma_kernel(const trpdrv_dev_system *__restrict__ sys, int nsys, long long 
         for (int x = 0; x < 8; ++x)
 #pragma unroll
             for (int e = 0; e < 4; ++e) f[x][e] = gT[x][e] = 0.0;
+        if (cx.packed) {
+            // two edge pairs (b0, c0) and (b1, c0): warp w takes pair w >> 2, sub-block w & 3 of it; each
+            // (chunk, family) has its own stage slot
+            const int pp = warp >> 2, sub = warp & 3, prs = sub >> 1, pcs = sub & 1;
+            const FragOffsets fp(prs * 16, pcs * 8, g, t);
+            const int pb0 = pp ? cx.b1 : cx.b0;
+            const bool pactive = pb0 >= 0 && cx.c0 + pcs * 8 < cx.nvir;
+            const int nsl = 2 * cx.nch, pnV = cx.nV;
+            for (int sl = 0; sl < nsl; ++sl) {
+                if (sl > 0 && !mbar_wait(&full[stage], phase, status)) return;
+                const char *st = stages + (size_t)stage * STAGE_BYTES;
+                const int ch = sl >> 1;
+                const bool ph1 = ch >= pnV;
+                const int kval = ph1 ? cx.nocc - (ch - pnV) * DK : cx.nvir - ch * DK;
+                if (pactive) {
+                    if (sl & 1)
+                        packed_family<KS, 1>(fp, st, pp, ph1, kval, f, gT);
+                    else
+                        packed_family<KS, 0>(fp, st, pp, ph1, kval, f, gT);
+                }
+                __syncwarp();
+                if (lane == 0) mbar_arrive(&empty[stage]);
+                if (++stage == STAGES) {
+                    stage = 0;
+                    phase ^= 1;
+                }
+            }
+            if (pb0 >= 0) {  // this pair's slots: the 4 sub-blocks' sums, zeros in the other 4
+                double *out = pp ? cx.out1 : cx.out;
+                warp_epilogue(cx, f, gT, pb0 + prs * 16, cx.c0 + pcs * 8, g, t, lane, out + sub * 4);
+                if (lane == 0) {
+                    double *z = out + (sub + 4) * 4;
+                    z[0] = z[1] = z[2] = z[3] = 0.0;
+                }
+            }
+            continue;
+        }
         const int nch = cx.nch, nV = cx.nV;
         const bool active = (cx.b0 + rx0 < cx.nvir) && (cx.c0 + cx0 < cx.nvir);
         const bool diag = cx.diag != 0;
@@ -661,6 +861,16 @@ extern "C" int trpdrv_tma_supported(const trpdrv_dev_system *h_sys, int nsys)
             if (((uintptr_t)q) & 15u) return 0;
     }
     return 1;
+}
+
+// Packing needs at least two edge pairs and an edge tile of at most 16 valid columns (two 8-wide
+// column blocks per pair).  TRPDRV_TMA_PACK_EDGE=0 keeps the edge pairs as ordinary items.
+extern "C" int trpdrv_tma_pack_edge(int nvir)
+{
+    const char *v = getenv("TRPDRV_TMA_PACK_EDGE");
+    if (v && v[0] == '0') return 0;
+    const int nb = (nvir + tma::T - 1) / tma::T, w = nvir - (nb - 1) * tma::T;
+    return nb >= 3 && w >= 1 && w <= 16;
 }
 
 extern "C" int trpdrv_tma_prepare(const trpdrv_dev_system *h_sys, int nsys, void *maps_out)

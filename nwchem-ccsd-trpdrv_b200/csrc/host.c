@@ -383,6 +383,7 @@ static int plan_build(trpdrv_plan *p, const trpdrv_system *shape)
         d->a = shape[q].a;
         d->nb = b->nb;
         d->npairs = b->npairs;
+        d->pack_edge = trpdrv_tma_pack_edge(nvir);
         d->ntriples = b->ntriples;
         d->nt = b->nt;
         d->n_a = b->n_a;
@@ -1856,6 +1857,7 @@ static int dif_prepare(int ncor, int nocc, int nvir)
     S->nvir = nvir;
     S->nb = nb;
     S->npairs = npairs;
+    S->pack_edge = trpdrv_tma_pack_edge(nvir);
     S->ntriples = 1;
     S->nt = 1;
     S->n_a = 1;

@@ -36,6 +36,9 @@ typedef struct trpdrv_dev_system {
                             of two slots; jvv, kvv, ntov, nxov, dintc, dintx, t1v: two slots), as the
                             drop-in entry points stage them; `triples` holds that triple (its i, j, k
                             give eaijk) and n_a is 1.  TMA kernel only. */
+    int pack_edge;       /* 1: the last tile holds 1..16 valid virtual indices and the TMA kernel runs the
+                            edge pairs (B, E), (B + 1, E) (B even) as one packed work item; the item of
+                            (B + 1, E) is then skipped (its energy slots are written by the packed one) */
     int64_t item_begin;  /* first fused work item of this system */
     const double *eorb, *t2, *jvv, *kvv, *ntov, *nxov, *jov, *kov, *dintc, *dintx, *t1v;
     const int32_t *triples; /* packed triples, driver order (energies are stored in this order) */
@@ -62,6 +65,8 @@ int trpdrv_fused_init(void);
  * One CTA per SM.  *status bit 0: malformed queue entry; bit 1: a pipeline wait ran out. */
 #define TRPDRV_TMA_MAX_SYSTEMS 8
 int trpdrv_tma_supported(const trpdrv_dev_system *h_sys, int nsys);
+/* 1 if the TMA kernel packs the edge pairs of a system with this nvir (see pack_edge). */
+int trpdrv_tma_pack_edge(int nvir);
 size_t trpdrv_tma_maps_bytes(void);
 int trpdrv_tma_prepare(const trpdrv_dev_system *h_sys, int nsys, void *maps_out);
 int trpdrv_launch_fused_tma(const trpdrv_dev_system *d_sys, int nsys, int64_t total_items,

@@ -321,3 +321,25 @@ def test_c_caller_of_the_plan_interface_gives_the_python_plan_energies(T, tmp_pa
     # each process autotunes for itself and may keep another variant: compare at the parity bar
     assert_total_close(float(out[0]), e4[0], what="emp4")
     assert_total_close(float(out[1]), e5[0], what="emp5")
+
+
+@pytest.mark.parametrize("shape", [(6, 70, 31), (4, 104, 32), (6, 134, 33), (2, 48, 34)])
+@pytest.mark.parametrize("mma_k", [8, 16])
+def test_tma_packed_edge_items_match_the_oracle_and_the_unpacked_kernel(T, O, monkeypatch, shape, mma_k):
+    """Where the last tile holds at most 16 virtual indices the TMA kernel runs the edge pairs two to a
+    work item (the last one alone when their count is odd); with TRPDRV_TMA_PACK_EDGE=0 it runs them as
+    ordinary items.  Both match the oracle; the f values are the same products, so the two agree to
+    rounding of the per-warp sums."""
+    nocc, nvir, seed = shape
+    s = T.synth_system(nocc, nvir, seed=seed)
+    rec_o, tot_o, mism = O.run_system(s, "port", nthreads=4)
+    assert mism == 0
+    got = {}
+    for pack in ("1", "0"):
+        monkeypatch.setenv("TRPDRV_TMA_PACK_EDGE", pack)
+        e4, e5, recs, _ = _plan_run(T, [s], mode=1, staging=2, mma_k=mma_k)
+        assert_records_close(recs[0], rec_o)
+        assert_total_close(e4[0], tot_o[0], what="emp4")
+        assert_total_close(e5[0], tot_o[1], what="emp5")
+        got[pack] = recs[0]
+    assert_records_close(got["1"], got["0"], rtol=1e-13)

@@ -4,14 +4,16 @@ It serves callers that cannot call cudaMalloc when they need the work: an applic
 device memory up front in its own pool and gives libraries a fixed budget, a plug-in inside a
 framework that owns every device buffer, or a loop that cannot pay for an allocation per call.  Its
 scratch is one static device array, so it is checked here against the existing host drop-in entry
-point (ccsd_trpdrv_omp_cbody_) on two calls in a row, which must agree with each other and with the
-drop-in; the array keeps the previous call's contents, so the second call also shows that leftovers
+point (ccsd_trpdrv_omp_cbody_, on its plain per-triple path: the same kernels) on two calls in a row,
+which must agree with each other and with the drop-in; the array keeps the previous call's contents, so the second call also shows that leftovers
 do not leak into the result.  The cases cover the 16-byte vector copies and the scalar ones (odd nvir,
 pointers off a 16-byte boundary), the size limit (nocc = 64, nvir = 256), and every triple of a golden
 system made by the reference itself.  This file is named so that pytest collects it last: a failure
 here never stops a run before every other test has run.  The tests pass in a fresh process (the
 first call sets the device up) and after the other tests.
 """
+import os
+
 import numpy as np
 import pytest
 
@@ -72,11 +74,25 @@ def _noalloc_twice(T, s, dev, i, j, k):
     return calls
 
 
+def _dropin_plain(T, s, i, j, k):
+    """The existing entry point on its plain per-triple path (the kernels this entry point runs too),
+    from host buffers, starting from emp4 = emp5 = 0."""
+    old = os.environ.get("TRPDRV_DROPIN_PATH")
+    os.environ["TRPDRV_DROPIN_PATH"] = "plain"
+    try:
+        return T.cbody(s, i, j, k, 1)
+    finally:
+        if old is None:
+            del os.environ["TRPDRV_DROPIN_PATH"]
+        else:
+            os.environ["TRPDRV_DROPIN_PATH"] = old
+
+
 def _check_against_dropin(T, s, dev, triples):
     for (i, j, k) in triples:
         calls = _noalloc_twice(T, s, dev, i, j, k)
         assert np.array_equal(calls[0], calls[1]), (i, j, k)
-        e4, e5 = T.cbody(s, i, j, k, 1)  # existing entry point, host buffers, starting from emp4 = emp5 = 0
+        e4, e5 = _dropin_plain(T, s, i, j, k)
         for r in calls:
             got4 = r[0] + (r[2] if i != k else 0.0)
             got5 = r[1] + (r[3] if i != k else 0.0)

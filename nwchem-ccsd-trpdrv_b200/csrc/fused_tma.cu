@@ -49,9 +49,14 @@ constexpr int STAGES = 3;
 constexpr int NCW = TRPDRV_FUSED_SLOTS;  // consumer warps (8) = two warpgroups
 constexpr int NTHREAD = (NCW + 4) * 32;  // + one producer warpgroup (one thread issues)
 // Register split by setmaxnreg: launched at 65536 / 384 = 168 per thread; the producer warpgroup
-// drops to 56 and the two consumer warpgroups rise to 224:  2*128*224 + 128*56 = 64512 = 384*168.
-constexpr int REG_LAUNCH = 168, REG_CONSUMER = 224, REG_PRODUCER = 56;
-static_assert(2 * 128 * REG_CONSUMER + 128 * REG_PRODUCER <= NTHREAD * REG_LAUNCH, "register split exceeds the launch");
+// drops and the two consumer warpgroups rise, within 384 * 168 = 64512: the m16n8k16 kernel's MMA
+// warps take 224 (producer 56: 2*128*224 + 128*56 = 64512), the m16n8k8 kernel's 216 (producer 64),
+// the splits under which neither kernel's MMA loop spills.
+constexpr int REG_LAUNCH = 168;
+template <int KS> struct Regs {
+    static constexpr int CONSUMER = KS == 16 ? 224 : 216, PRODUCER = KS == 16 ? 56 : 64;
+    static_assert(2 * 128 * CONSUMER + 128 * PRODUCER <= NTHREAD * REG_LAUNCH, "register split exceeds the launch");
+};
 constexpr int PANEL_BYTES = 4096;
 constexpr int NPANEL = 16;
 constexpr int STAGE_BYTES = NPANEL * PANEL_BYTES;
@@ -614,11 +619,11 @@ fused_tma_kernel(const trpdrv_dev_system *__restrict__ sys, int nsys, long long 
     __syncthreads();
 
     if (warp >= NCW) {  // producer warpgroup: its first warp issues everything
-        asm volatile("setmaxnreg.dec.sync.aligned.u32 %0;" ::"n"(REG_PRODUCER));
+        asm volatile("setmaxnreg.dec.sync.aligned.u32 %0;" ::"n"(Regs<KS>::PRODUCER));
         if (warp == NCW) producer(sys, nsys, total, counter, status, maps, stages, full, empty, ring, lane);
         return;
     }
-    asm volatile("setmaxnreg.inc.sync.aligned.u32 %0;" ::"n"(REG_CONSUMER));
+    asm volatile("setmaxnreg.inc.sync.aligned.u32 %0;" ::"n"(Regs<KS>::CONSUMER));
 
     const int g = lane >> 2, t = lane & 3;
     // sub-block: rows (b) rs*16.., columns (c) cs*8..; warps w and w+4 share a scheduler and differ in both
@@ -666,10 +671,12 @@ fused_tma_kernel(const trpdrv_dev_system *__restrict__ sys, int nsys, long long 
                 const bool ph1 = ch >= pnV;
                 const int kval = ph1 ? cx.nocc - (ch - pnV) * DK : cx.nvir - ch * DK;
                 if (pactive) {
+                    // m16n8k8 here in both kernels: the packed path's extra fragment registers would
+                    // push the k16 kernel's MMA warps past their register budget
                     if (sl & 1)
-                        packed_family<KS, 1>(fp, st, pp, ph1, kval, f, gT);
+                        packed_family<8, 1>(fp, st, pp, ph1, kval, f, gT);
                     else
-                        packed_family<KS, 0>(fp, st, pp, ph1, kval, f, gT);
+                        packed_family<8, 0>(fp, st, pp, ph1, kval, f, gT);
                 }
                 __syncwarp();
                 if (lane == 0) mbar_arrive(&empty[stage]);
@@ -822,13 +829,14 @@ static PFN_cuTensorMapEncodeTiled_v12000 encode_fn()
 }
 
 // 3-D map over doubles: dims {d0 (contiguous), d1, d2}, box {b0, b1, 1}
+// zstride: distance in doubles between consecutive blocks of the third dimension (0 = d0 * d1, packed)
 static int make_map(CUtensorMap *m, const double *base, unsigned long long d0, unsigned long long d1,
-                    unsigned long long d2, unsigned b0, unsigned b1, bool swizzle)
+                    unsigned long long d2, unsigned b0, unsigned b1, bool swizzle, unsigned long long zstride = 0)
 {
     PFN_cuTensorMapEncodeTiled_v12000 fn = encode_fn();
     if (!fn) return 1;
     const cuuint64_t dims[3] = {d0, d1, d2};
-    const cuuint64_t strides[2] = {d0 * 8ull, d0 * d1 * 8ull};
+    const cuuint64_t strides[2] = {d0 * 8ull, (zstride ? zstride : d0 * d1) * 8ull};
     const cuuint32_t box[3] = {b0, b1, 1};
     const cuuint32_t estr[3] = {1, 1, 1};
     const CUresult r = fn(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3, const_cast<double *>(base), dims, strides, box, estr,
@@ -886,14 +894,16 @@ extern "C" int trpdrv_tma_prepare(const trpdrv_dev_system *h_sys, int nsys, void
         CUtensorMap *m = M->m[s];
         int e = 0;
         const unsigned long long OA = X * (unsigned long long)(S.n_a > 0 ? S.n_a : 1);
-        e |= tma::make_map(&m[tma::M_J], S.jvv, V, V, OA, 16, tma::DK, true);    // [a][i][d][b]
-        e |= tma::make_map(&m[tma::M_K], S.kvv, V, V, OA, 16, tma::DK, true);
-        e |= tma::make_map(&m[tma::M_NT], S.ntov, V, O, X, 16, tma::DK, true);  // [i][m][b]
-        e |= tma::make_map(&m[tma::M_NX], S.nxov, V, O, X, 16, tma::DK, true);
-        e |= tma::make_map(&m[tma::M_T2K], S.t2, V, V, O2, 16, tma::DK, true);  // [jx][d][c]: T(c,d)
-        e |= tma::make_map(&m[tma::M_T2X], S.t2, V, V, O2, tma::DK, 32, true); // [jx][c][d]: T(d,c)
-        e |= tma::make_map(&m[tma::M_JOV], S.jov, O, V, O2, tma::DK, 32, true);  // [jx][c][m]
-        e |= tma::make_map(&m[tma::M_KOV], S.kov, O, V, O2, tma::DK, 32, true);
+        // a one-triple system may place its two slots of every tensor slot_stride doubles apart
+        const unsigned long long zs = S.one_triple ? (unsigned long long)S.slot_stride : 0ull;
+        e |= tma::make_map(&m[tma::M_J], S.jvv, V, V, OA, 16, tma::DK, true, zs);    // [a][i][d][b]
+        e |= tma::make_map(&m[tma::M_K], S.kvv, V, V, OA, 16, tma::DK, true, zs);
+        e |= tma::make_map(&m[tma::M_NT], S.ntov, V, O, X, 16, tma::DK, true, zs);  // [i][m][b]
+        e |= tma::make_map(&m[tma::M_NX], S.nxov, V, O, X, 16, tma::DK, true, zs);
+        e |= tma::make_map(&m[tma::M_T2K], S.t2, V, V, O2, 16, tma::DK, true, zs);  // [jx][d][c]: T(c,d)
+        e |= tma::make_map(&m[tma::M_T2X], S.t2, V, V, O2, tma::DK, 32, true, zs); // [jx][c][d]: T(d,c)
+        e |= tma::make_map(&m[tma::M_JOV], S.jov, O, V, O2, tma::DK, 32, true, zs);  // [jx][c][m]
+        e |= tma::make_map(&m[tma::M_KOV], S.kov, O, V, O2, tma::DK, 32, true, zs);
         if (e) return e;
     }
     return 0;

@@ -1792,22 +1792,31 @@ static int di_tengy_launch(int ncor, int nocc, int nvir, double eaijk, const dou
 
 /* ---- the drop-in body on the fused TMA kernel --------------------------------------------
  * One call stages its triple's inputs into a fixed "one-triple system" (trpdrv_dev_system with
- * one_triple = 1): the i-role block of every tensor at occupied slot 0 and the k-role block at slot
- * 1.  Host inputs go through a pinned mirror of that layout (copied by several host threads, then one
- * host->device copy); inputs inside registered arrays are gathered device->device in one launch.
- * Then one negate launch (-tov, -xov), one fused launch (one work item per tile pair, f never leaves
- * the SMs), one per-triple reduction, and a 48-byte read of the record and the kernel status. */
-enum { DS_HDR, DS_T2, DS_JVV, DS_KVV, DS_TOV, DS_XOV, DS_JOV, DS_KOV, DS_DINTC, DS_DINTX, DS_T1V, DS_EORB,
-       DS_NTOV, DS_NXOV, DS_END };
+ * one_triple = 1) on the device and its pinned host mirror:
+ *   HDR   the system descriptor and the packed triple (512 bytes)
+ *   VEC   dintc, dintx, t1v as [2][nvir] (i role, k role), then eorb
+ *   I     the i-role blocks: tij, jia, kia, -tia, -xia, jij, kij
+ *   K     the k-role blocks: tkj, jka, kka, -tka, -xka, jkj, kkj, at the same offsets RS doubles on
+ * so that every TMA-read tensor is [2 slots] with slot stride RS.  Host slices are compared with the
+ * mirror block by block and copied (negated where the kernel wants -T / -X) only where they differ;
+ * a region goes to the device only when something in it changed (or the device copy is not known to
+ * match the mirror): the reference driver's k-inner loop changes only the K region from call to call.
+ * Slices inside registered arrays are gathered on the device instead.  One fused launch (one work item
+ * per tile pair; f never leaves the SMs) then writes the per-item energy slots, which come back with
+ * the kernel's status and are summed on the host in a fixed order. */
+enum { DR_HDR, DR_VEC, DR_I, DR_K, DR_N };
+enum { DT_T2, DT_JVV, DT_KVV, DT_NTOV, DT_NXOV, DT_JOV, DT_KOV, DT_N };
 #define DS_HDR_DOUBLES 64 /* the system descriptor and the packed triple, 512 bytes */
 
 static struct dropin_fused {
-    int ready, ncor, nocc, nvir, nsm;
-    size_t off[DS_END + 1]; /* element offsets of the staging layout; off[DS_NTOV] ends the host part */
+    int ready, ncor, nocc, nvir, nsm, npairs;
+    size_t reg_off[DR_N + 1];  /* region offsets (doubles) in the staging block */
+    size_t toff[DT_N];         /* tensor offsets inside an I / K region */
+    size_t vec_v;              /* nvir */
+    int dev_valid[DR_N];       /* the device copy of the region equals the host mirror */
     double *d_block, *h_block;
     trpdrv_dev_system h_sys;
-    double *d_partial;
-    double *d_io, *h_io; /* rec[4], counter (as 8 bytes), status (as int) */
+    double *d_io, *h_io; /* per-item energy slots [npairs][8][4], then counter (8 bytes) and status */
     void *maps;
 } g_dif;
 
@@ -1816,7 +1825,6 @@ static void dif_release(void)
     if (!g_dif.ready) return;
     cudaFree(g_dif.d_block);
     cudaFreeHost(g_dif.h_block);
-    cudaFree(g_dif.d_partial);
     cudaFree(g_dif.d_io);
     cudaFreeHost(g_dif.h_io);
     free(g_dif.maps);
@@ -1826,30 +1834,39 @@ static void dif_release(void)
 /* The fused drop-in path needs what the TMA kernel needs: even nvir and nocc (16-byte rows). */
 static int dif_eligible(int nocc, int nvir) { return !(nocc & 1) && !(nvir & 1); }
 
+static size_t round32(size_t n) { return (n + 31) & ~(size_t)31; }
+
 static int dif_prepare(int ncor, int nocc, int nvir)
 {
     if (g_dif.ready && g_dif.ncor == ncor && g_dif.nocc == nocc && g_dif.nvir == nvir) return TRPDRV_OK;
     dif_release();
     const size_t vv = (size_t)nvir * nvir, ov = (size_t)nocc * nvir, v = (size_t)nvir;
-    const size_t len[DS_END] = {DS_HDR_DOUBLES, 2 * vv, 2 * vv, 2 * vv, 2 * ov, 2 * ov, 2 * ov, 2 * ov,
-                                2 * v,          2 * v,  2 * v,  (size_t)(ncor + nocc + nvir), 2 * ov, 2 * ov};
+    const size_t tlen[DT_N] = {vv, vv, vv, ov, ov, ov, ov};
     size_t o = 0;
-    for (int q = 0; q < DS_END; ++q) {
-        if (q == DS_NTOV) o = (o + 31) & ~(size_t)31; /* device-only part on a 256-byte boundary */
-        g_dif.off[q] = o;
-        o += len[q];
+    for (int q = 0; q < DT_N; ++q) {
+        g_dif.toff[q] = o;
+        o += round32(tlen[q]);
     }
-    g_dif.off[DS_END] = o;
+    const size_t rs = o; /* region size = slot stride of every TMA-read tensor */
+    g_dif.reg_off[DR_HDR] = 0;
+    g_dif.reg_off[DR_VEC] = DS_HDR_DOUBLES;
+    g_dif.reg_off[DR_I] = DS_HDR_DOUBLES + round32(6 * v + (size_t)(ncor + nocc + nvir));
+    g_dif.reg_off[DR_K] = g_dif.reg_off[DR_I] + rs;
+    g_dif.reg_off[DR_N] = g_dif.reg_off[DR_K] + rs;
+    g_dif.vec_v = v;
     const int nb = (nvir + TRPDRV_TILE - 1) / TRPDRV_TILE, npairs = nb * (nb + 1) / 2;
     int dev = 0, nsm = 0;
     TRY(ensure_device(g_di.device, &dev, &nsm));
-    CUDA_TRY(cudaMalloc((void **)&g_dif.d_block, sizeof(double) * o));
-    CUDA_TRY(cudaMallocHost((void **)&g_dif.h_block, sizeof(double) * g_dif.off[DS_NTOV]));
-    CUDA_TRY(cudaMalloc((void **)&g_dif.d_partial, sizeof(double) * 4 * TRPDRV_FUSED_SLOTS * (size_t)npairs));
-    CUDA_TRY(cudaMalloc((void **)&g_dif.d_io, sizeof(double) * 8));
-    CUDA_TRY(cudaMallocHost((void **)&g_dif.h_io, sizeof(double) * 8));
+    const size_t total = g_dif.reg_off[DR_N];
+    CUDA_TRY(cudaMalloc((void **)&g_dif.d_block, sizeof(double) * total));
+    CUDA_TRY(cudaMallocHost((void **)&g_dif.h_block, sizeof(double) * total));
+    const size_t nslot = 4 * TRPDRV_FUSED_SLOTS * (size_t)npairs;
+    CUDA_TRY(cudaMalloc((void **)&g_dif.d_io, sizeof(double) * (nslot + 2)));
+    CUDA_TRY(cudaMallocHost((void **)&g_dif.h_io, sizeof(double) * (nslot + 2)));
     g_dif.ready = 1; /* from here dif_release frees whatever was allocated */
+    memset(g_dif.h_block, 0, sizeof(double) * total);
     double *d = g_dif.d_block;
+    const double *I = d + g_dif.reg_off[DR_I], *vec = d + g_dif.reg_off[DR_VEC];
     trpdrv_dev_system *S = &g_dif.h_sys;
     memset(S, 0, sizeof *S);
     S->ncor = ncor;
@@ -1862,22 +1879,23 @@ static int dif_prepare(int ncor, int nocc, int nvir)
     S->nt = 1;
     S->n_a = 1;
     S->one_triple = 1;
+    S->slot_stride = (int64_t)rs;
     S->item_begin = 0;
-    S->t2 = d + g_dif.off[DS_T2];
-    S->jvv = d + g_dif.off[DS_JVV];
-    S->kvv = d + g_dif.off[DS_KVV];
-    S->ntov = d + g_dif.off[DS_NTOV];
-    S->nxov = d + g_dif.off[DS_NXOV];
-    S->jov = d + g_dif.off[DS_JOV];
-    S->kov = d + g_dif.off[DS_KOV];
-    S->dintc = d + g_dif.off[DS_DINTC];
-    S->dintx = d + g_dif.off[DS_DINTX];
-    S->t1v = d + g_dif.off[DS_T1V];
-    S->eorb = d + g_dif.off[DS_EORB];
-    S->triples = (const int32_t *)(d + g_dif.off[DS_HDR]) + 2 * (sizeof(trpdrv_dev_system) / 8 + 1);
+    S->t2 = I + g_dif.toff[DT_T2];
+    S->jvv = I + g_dif.toff[DT_JVV];
+    S->kvv = I + g_dif.toff[DT_KVV];
+    S->ntov = I + g_dif.toff[DT_NTOV];
+    S->nxov = I + g_dif.toff[DT_NXOV];
+    S->jov = I + g_dif.toff[DT_JOV];
+    S->kov = I + g_dif.toff[DT_KOV];
+    S->dintc = vec;
+    S->dintx = vec + 2 * v;
+    S->t1v = vec + 4 * v;
+    S->eorb = vec + 6 * v;
+    S->triples = (const int32_t *)d + 2 * (sizeof(trpdrv_dev_system) / 8 + 1);
     S->order = NULL;
-    S->partial = g_dif.d_partial;
-    S->rec = g_dif.d_io;
+    S->partial = g_dif.d_io;
+    S->rec = NULL;
     if (sizeof(trpdrv_dev_system) + 16 > DS_HDR_DOUBLES * sizeof(double))
         return fail(TRPDRV_ERR_STATE, "drop-in staging header too small");
     if (!trpdrv_tma_supported(S, 1)) return fail(TRPDRV_ERR_UNSUPPORTED, "TMA staging unavailable");
@@ -1889,42 +1907,44 @@ static int dif_prepare(int ncor, int nocc, int nvir)
     g_dif.nocc = nocc;
     g_dif.nvir = nvir;
     g_dif.nsm = nsm;
+    g_dif.npairs = npairs;
     return TRPDRV_OK;
 }
 
-/* Host threads for the staging copies: TRPDRV_STAGE_THREADS, else up to 8 of OpenMP's. */
+/* Host threads for the staging copies: TRPDRV_STAGE_THREADS, else up to 16 of OpenMP's. */
 static int stage_threads(void)
 {
     const char *v = getenv("TRPDRV_STAGE_THREADS");
     int n = v ? atoi(v) : 0;
     if (n <= 0) {
         n = omp_get_max_threads();
-        if (n > 8) n = 8;
+        if (n > 16) n = 16;
     }
     return n < 1 ? 1 : n;
 }
+
+/* 64-bit words that may alias the doubles they are read from (bitwise comparison and negation) */
+typedef uint64_t __attribute__((may_alias)) word64;
 
 typedef struct stage_piece {
     double *dst;
     const double *src;
     size_t n;
+    int neg; /* the mirror holds -src */
 } stage_piece;
 
-/* Copies the pieces (split into blocks of at most 128 KB) with up to `threads` host threads. */
-static void stage_copy(const stage_piece *pc, int npc, int threads)
+/* Brings the mirror pieces up to date with their sources (negated where asked), in blocks of 16 KB
+ * spread over up to `threads` host threads; a block is written only where it differs bit for bit.
+ * Returns 1 if any block was written. */
+static int stage_update(const stage_piece *pc, int npc, int threads)
 {
-    enum { BLK = 16384 };
-    size_t total = 0;
+    enum { BLK = 2048 };
     int nblk = 0;
-    for (int q = 0; q < npc; ++q) {
-        total += pc[q].n;
-        nblk += (int)((pc[q].n + BLK - 1) / BLK);
-    }
-    if (threads <= 1 || total < 4 * BLK) {
-        for (int q = 0; q < npc; ++q) memcpy(pc[q].dst, pc[q].src, sizeof(double) * pc[q].n);
-        return;
-    }
-#pragma omp parallel for num_threads(threads) schedule(static)
+    for (int q = 0; q < npc; ++q) nblk += (int)((pc[q].n + BLK - 1) / BLK);
+    if (nblk == 0) return 0;
+    if (threads > nblk) threads = nblk;
+    int changed = 0;
+#pragma omp parallel for num_threads(threads) schedule(static) reduction(| : changed) if (threads > 1)
     for (int b = 0; b < nblk; ++b) {
         int q = 0, r = b;
         while (r >= (int)((pc[q].n + BLK - 1) / BLK)) {
@@ -1932,61 +1952,97 @@ static void stage_copy(const stage_piece *pc, int npc, int threads)
             ++q;
         }
         const size_t lo = (size_t)r * BLK, n = pc[q].n - lo < BLK ? pc[q].n - lo : BLK;
-        memcpy(pc[q].dst + lo, pc[q].src + lo, sizeof(double) * n);
+        const word64 *src = (const word64 *)(pc[q].src + lo);
+        word64 *dst = (word64 *)(pc[q].dst + lo);
+        const uint64_t flip = pc[q].neg ? 0x8000000000000000ull : 0ull; /* negation = sign bit */
+        uint64_t diff = 0;
+        for (size_t e = 0; e < n; ++e) diff |= dst[e] ^ src[e] ^ flip;
+        if (diff) {
+            for (size_t e = 0; e < n; ++e) dst[e] = src[e] ^ flip;
+            changed = 1;
+        }
     }
+    return changed;
 }
 
-/* One triple through the fused kernel; rec[4] = emp4i, emp5i, emp4k, emp5k. */
-static int body_fused(int ncor, int nocc, int nvir, int a, int i, int j, int k, const double *const *in,
-                      const size_t *in_len, const int *in_slot, double *rec)
+/* One triple through the fused kernel; rec[4] = emp4i, emp5i, emp4k, emp5k.  in[q], len[q]: the
+ * slice, reg[q]: its region (DR_VEC / DR_I / DR_K), off[q]: its offset in the block, neg[q]: stored
+ * negated. */
+static int body_fused(int ncor, int nocc, int nvir, int a, int i, int j, int k, int nin, const double *const *in,
+                      const size_t *len, const int *reg, const size_t *off, const int *neg, double *rec)
 {
     TRY(dif_prepare(ncor, nocc, nvir));
     cudaStream_t st = g_di.stream;
     double *h = g_dif.h_block;
+    const int threads = stage_threads();
     /* header: the system descriptor with this call's a, then the packed triple */
     trpdrv_dev_system S = g_dif.h_sys;
     S.a = a;
     memcpy(h, &S, sizeof S);
     ((int32_t *)h)[2 * (sizeof(trpdrv_dev_system) / 8 + 1)] = pack_triple(i, j, k);
-    stage_piece pc[24];
+
     trpdrv_copy_list gl;
     memset(&gl, 0, sizeof gl);
-    int npc = 0;
-    for (int q = 0; q < 21; ++q) {
-        const size_t dst = g_dif.off[in_slot[q] >> 1] + (size_t)(in_slot[q] & 1) * (in_len[q] == 0 ? 0 : in_len[q]);
-        const double *dsrc = reg_lookup(in[q], in_len[q]);
-        if (dsrc) {
+    int has_dev[DR_N] = {0, 0, 0, 0};
+    stage_piece pc[DR_N][24];
+    int npc[DR_N] = {0, 0, 0, 0};
+    for (int q = 0; q < nin; ++q) {
+        const double *dsrc = reg_lookup(in[q], len[q]);
+        if (dsrc && gl.n < TRPDRV_COPY_LIST_MAX) {
             gl.src[gl.n] = dsrc;
-            gl.dst[gl.n] = g_dif.d_block + dst;
-            gl.len[gl.n] = (long long)in_len[q];
+            gl.dst[gl.n] = g_dif.d_block + off[q];
+            gl.len[gl.n] = (long long)len[q];
+            gl.neg[gl.n] = neg[q];
             ++gl.n;
+            has_dev[reg[q]] = 1;
         } else {
-            pc[npc].dst = h + dst;
-            pc[npc].src = in[q];
-            pc[npc].n = in_len[q];
-            ++npc;
+            stage_piece *p = &pc[reg[q]][npc[reg[q]]++];
+            p->dst = h + off[q];
+            p->src = in[q];
+            p->n = len[q];
+            p->neg = neg[q];
         }
     }
-    stage_copy(pc, npc, stage_threads());
-    const size_t up = npc ? g_dif.off[DS_NTOV] : (size_t)DS_HDR_DOUBLES;
-    CUDA_TRY(cudaMemcpyAsync(g_dif.d_block, h, sizeof(double) * up, cudaMemcpyHostToDevice, st));
+    /* the large regions first, each sent as soon as it is up to date (the copy overlaps the next
+     * region's comparison); then the header and the vectors, always sent */
+    static const int order[2] = {DR_K, DR_I};
+    for (int r = 0; r < 2; ++r) {
+        const int R = order[r];
+        const int changed = stage_update(pc[R], npc[R], threads);
+        if (npc[R] && (changed || !g_dif.dev_valid[R])) {
+            const size_t lo = g_dif.reg_off[R], n = g_dif.reg_off[R + 1] - lo;
+            CUDA_TRY(cudaMemcpyAsync(g_dif.d_block + lo, h + lo, sizeof(double) * n, cudaMemcpyHostToDevice, st));
+        }
+        /* a region that received device slices no longer mirrors the host block */
+        g_dif.dev_valid[R] = npc[R] && !has_dev[R];
+    }
+    stage_update(pc[DR_VEC], npc[DR_VEC], 1);
+    CUDA_TRY(cudaMemcpyAsync(g_dif.d_block, h, sizeof(double) * g_dif.reg_off[DR_I], cudaMemcpyHostToDevice, st));
     if (gl.n) LAUNCH_TRY(trpdrv_launch_gather(&gl, st));
-    CUDA_TRY(cudaMemsetAsync(g_dif.d_io + 4, 0, 2 * sizeof(double), st));
-    /* -tia, -tka, -xia, -xka: tov|xov and ntov|nxov are adjacent */
-    LAUNCH_TRY(trpdrv_launch_negate(g_dif.d_block + g_dif.off[DS_TOV], g_dif.d_block + g_dif.off[DS_NTOV],
-                                    4 * (size_t)nocc * nvir, st));
-    const int npairs = g_dif.h_sys.npairs;
+    const size_t nslot = 4 * TRPDRV_FUSED_SLOTS * (size_t)g_dif.npairs;
+    CUDA_TRY(cudaMemsetAsync(g_dif.d_io + nslot, 0, 2 * sizeof(double), st));
+    const int npairs = g_dif.npairs;
     const int grid = npairs < g_dif.nsm ? npairs : g_dif.nsm;
-    const trpdrv_dev_system *d_sys = (const trpdrv_dev_system *)(g_dif.d_block + g_dif.off[DS_HDR]);
-    LAUNCH_TRY(trpdrv_launch_fused_tma(d_sys, 1, npairs, (unsigned long long *)(g_dif.d_io + 4), (int *)(g_dif.d_io + 5),
+    LAUNCH_TRY(trpdrv_launch_fused_tma((const trpdrv_dev_system *)g_dif.d_block, 1, npairs,
+                                       (unsigned long long *)(g_dif.d_io + nslot), (int *)(g_dif.d_io + nslot + 1),
                                        grid, g_dif.maps, 8, st));
-    LAUNCH_TRY(trpdrv_launch_item_reduce(&g_dif.h_sys, st));
-    CUDA_TRY(cudaMemcpyAsync(g_dif.h_io, g_dif.d_io, 6 * sizeof(double), cudaMemcpyDeviceToHost, st));
+    CUDA_TRY(cudaMemcpyAsync(g_dif.h_io, g_dif.d_io, sizeof(double) * (nslot + 2), cudaMemcpyDeviceToHost, st));
     CUDA_TRY(cudaStreamSynchronize(st));
     int status = 0;
-    memcpy(&status, g_dif.h_io + 5, sizeof status);
+    memcpy(&status, g_dif.h_io + nslot + 1, sizeof status);
     if (status) return fail(TRPDRV_ERR_DEVICE, "fused kernel reported status %d", status);
-    for (int q = 0; q < 4; ++q) rec[q] = g_dif.h_io[q];
+    /* the item slots in a fixed order */
+    double r0 = 0.0, r1 = 0.0, r2 = 0.0, r3 = 0.0;
+    for (size_t q = 0; q < nslot; q += 4) {
+        r0 += g_dif.h_io[q];
+        r1 += g_dif.h_io[q + 1];
+        r2 += g_dif.h_io[q + 2];
+        r3 += g_dif.h_io[q + 3];
+    }
+    rec[0] = r0;
+    rec[1] = r1;
+    rec[2] = r2;
+    rec[3] = r3;
     return TRPDRV_OK;
 }
 
@@ -2022,18 +2078,23 @@ static int body_impl(double *f1n, double *f1t, double *f2n, double *f2t, double 
     const size_t vv = (size_t)(k - klo) * lnvv, ov = (size_t)(k - klo) * lnov;
 
     if (!write_f && dif_eligible(nocc, nvir) && !env_flag("TRPDRV_DROPIN_PATH", "plain")) {
-        /* the 21 input slices and their slots in the one-triple staging layout ((tensor << 1) | role) */
-        const double *in[21] = {tij, tkj + vv, jia, jka + vv, kia, kka + vv, tia, tka + ov, xia, xka + ov,
-                                jij, jkj + ov, kij, kkj + ov, dintc1, dintc2, dintx1, dintx2, t1v1, t1v2, eorb};
-        const size_t v = (size_t)nvir;
-        const size_t len[21] = {lnvv, lnvv, lnvv, lnvv, lnvv, lnvv, lnov, lnov, lnov, lnov,
-                                lnov, lnov, lnov, lnov, v, v, v, v, v, v, (size_t)nbf};
-        const int slot[21] = {DS_T2 << 1, DS_T2 << 1 | 1, DS_JVV << 1, DS_JVV << 1 | 1, DS_KVV << 1, DS_KVV << 1 | 1,
-                              DS_TOV << 1, DS_TOV << 1 | 1, DS_XOV << 1, DS_XOV << 1 | 1, DS_JOV << 1,
-                              DS_JOV << 1 | 1, DS_KOV << 1, DS_KOV << 1 | 1, DS_DINTC << 1, DS_DINTC << 1 | 1,
-                              DS_DINTX << 1, DS_DINTX << 1 | 1, DS_T1V << 1, DS_T1V << 1 | 1, DS_EORB << 1};
-        double rec[4];
-        TRY(body_fused(ncor, nocc, nvir, a, i, j, k, in, len, slot, rec));
+        TRY(dif_prepare(ncor, nocc, nvir));
+        /* the 21 input slices: region, offset in the staging block, stored negated or not */
+        const size_t v = (size_t)nvir, I = g_dif.reg_off[DR_I], K = g_dif.reg_off[DR_K], VE = g_dif.reg_off[DR_VEC];
+        const size_t *T = g_dif.toff;
+        const double *in[21] = {tij, jia, kia, tia, xia, jij, kij, tkj + vv, jka + vv, kka + vv, tka + ov, xka + ov,
+                                jkj + ov, kkj + ov, dintc1, dintc2, dintx1, dintx2, t1v1, t1v2, eorb};
+        const size_t len[21] = {lnvv, lnvv, lnvv, lnov, lnov, lnov, lnov, lnvv, lnvv, lnvv, lnov, lnov,
+                                lnov, lnov, v, v, v, v, v, v, (size_t)nbf};
+        const int reg[21] = {DR_I, DR_I, DR_I, DR_I, DR_I, DR_I, DR_I, DR_K, DR_K, DR_K, DR_K, DR_K, DR_K, DR_K,
+                             DR_VEC, DR_VEC, DR_VEC, DR_VEC, DR_VEC, DR_VEC, DR_VEC};
+        const size_t off[21] = {I + T[DT_T2], I + T[DT_JVV], I + T[DT_KVV], I + T[DT_NTOV], I + T[DT_NXOV],
+                                I + T[DT_JOV], I + T[DT_KOV], K + T[DT_T2], K + T[DT_JVV], K + T[DT_KVV],
+                                K + T[DT_NTOV], K + T[DT_NXOV], K + T[DT_JOV], K + T[DT_KOV],
+                                VE, VE + v, VE + 2 * v, VE + 3 * v, VE + 4 * v, VE + 5 * v, VE + 6 * v};
+        const int neg[21] = {0, 0, 0, 1, 1, 0, 0, 0, 0, 0, 1, 1, 0, 0, 0, 0, 0, 0, 0, 0, 0};
+        double rec[4] = {0.0, 0.0, 0.0, 0.0};
+        TRY(body_fused(ncor, nocc, nvir, a, i, j, k, 21, in, len, reg, off, neg, rec));
         /* omp/ccsd_trpdrv_omp_cbody.c:133-142 */
         double emp4 = *emp4_, emp5 = *emp5_;
         emp4 += rec[0];

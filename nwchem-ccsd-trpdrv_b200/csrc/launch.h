@@ -36,6 +36,9 @@ typedef struct trpdrv_dev_system {
                             of two slots; jvv, kvv, ntov, nxov, dintc, dintx, t1v: two slots), as the
                             drop-in entry points stage them; `triples` holds that triple (its i, j, k
                             give eaijk) and n_a is 1.  TMA kernel only. */
+    int64_t slot_stride; /* one_triple: doubles between the i-role and k-role blocks of every TMA-read tensor
+                            (t2, jvv, kvv, ntov, nxov, jov, kov); 0 = the packed [2][block] layout.  The
+                            vectors (dintc, dintx, t1v) stay packed [2][nvir]. */
     int pack_edge;       /* 1: the last tile holds 1..16 valid virtual indices and the TMA kernel runs the
                             edge pairs (B, E), (B + 1, E) (B even) as one packed work item; the item of
                             (B + 1, E) is then skipped (its energy slots are written by the packed one) */
@@ -113,13 +116,14 @@ int trpdrv_launch_system_reduce(const double *rec, const int32_t *triples, int64
 /* dst[i] = -src[i]. */
 int trpdrv_launch_negate(const double *src, double *dst, size_t n, void *stream);
 
-/* Device-to-device copies dst[s][0..len[s]) = src[s][..] for s < n, in one launch. */
+/* Device-to-device copies dst[s][0..len[s]) = src[s][..] (negated where neg[s]) for s < n, in one launch. */
 #define TRPDRV_COPY_LIST_MAX 24
 typedef struct trpdrv_copy_list {
     int n;
     const double *src[TRPDRV_COPY_LIST_MAX];
     double *dst[TRPDRV_COPY_LIST_MAX];
     long long len[TRPDRV_COPY_LIST_MAX];
+    int neg[TRPDRV_COPY_LIST_MAX];  /* 1: dst = -src */
 } trpdrv_copy_list;
 int trpdrv_launch_gather(const trpdrv_copy_list *list, void *stream);
 

@@ -110,15 +110,18 @@ __global__ void gather_kernel(const trpdrv_copy_list L)
     const double *src = L.src[s];
     double *dst = L.dst[s];
     const long long n = L.len[s];
+    const double sg = L.neg[s] ? -1.0 : 1.0;
     const long long stride = (long long)gridDim.x * blockDim.x;
     const long long t0 = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (((reinterpret_cast<uintptr_t>(src) | reinterpret_cast<uintptr_t>(dst)) & 15u) == 0) {
         const long long n2 = n >> 1;
-        for (long long q = t0; q < n2; q += stride)
-            reinterpret_cast<double2 *>(dst)[q] = __ldg(reinterpret_cast<const double2 *>(src) + q);
-        if ((n & 1) && t0 == 0) dst[n - 1] = src[n - 1];
+        for (long long q = t0; q < n2; q += stride) {
+            const double2 v = __ldg(reinterpret_cast<const double2 *>(src) + q);
+            reinterpret_cast<double2 *>(dst)[q] = make_double2(sg * v.x, sg * v.y);
+        }
+        if ((n & 1) && t0 == 0) dst[n - 1] = sg * src[n - 1];
     } else {
-        for (long long q = t0; q < n; q += stride) dst[q] = src[q];
+        for (long long q = t0; q < n; q += stride) dst[q] = sg * src[q];
     }
 }
 

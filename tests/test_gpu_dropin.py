@@ -106,3 +106,38 @@ def test_full_size_dropin_matches_the_reference_fixture(T):
         e4, e5 = T.cbody(s, i, j, k, klo)
         w4, w5 = _want(recs[q], i, k)
         assert _close(e4, w4, scale=scale4) and _close(e5, w5, scale=scale5), (t, e4, w4, e5, w5)
+
+
+def _call_with_buffers(T, s, bufs, i, j, k, klo):
+    """ccsd_trpdrv_omp_cbody_ on caller buffers (dict of BODY_ORDER name -> array) for triple (i,j,k)."""
+    import ctypes as C
+    dp, ip = C.POINTER(C.c_double), C.POINTER(C.c_int)
+    fn = T.lib.ccsd_trpdrv_omp_cbody_
+    f = np.zeros((8, s.nvir * s.nvir))
+    ints = [C.c_int(v) for v in (s.ncor, s.nocc, s.nvir)]
+    idx = [C.c_int(v) for v in (s.a, i, j, k, klo)]
+    e4, e5 = C.c_double(0.0), C.c_double(0.0)
+    fn(*[f[q].ctypes.data_as(dp) for q in range(8)], s.arrays["eorb"].ctypes.data_as(dp), *[C.byref(v) for v in ints],
+       C.byref(e4), C.byref(e5), *[C.byref(v) for v in idx], *[bufs[n].ctypes.data_as(dp) for n in T.BODY_ORDER])
+    return e4.value, e5.value
+
+
+def test_refilled_buffers_are_seen_on_every_call(T):
+    """A caller that refills the same host buffers between calls (as the NWChem driver does per (i, a)
+    and (k, j) block): the staging compares contents, not pointers, so every call sees its own data,
+    including calls where only the k-role or only the i-role buffers change."""
+    s = T.synth_system(6, 40, seed=95)
+    O, V = s.nocc, s.nvir
+    sizes = {n: (V * V if n in ("tij", "tkj", "jia", "jka", "kia", "kka") else
+                 O * V if n in ("tia", "tka", "xia", "xka", "jij", "jkj", "kij", "kkj") else V) for n in T.BODY_ORDER}
+    bufs = {n: np.zeros(sizes[n]) for n in T.BODY_ORDER}
+    ijkl = T.enumerate_triples(O, 1)
+    for t in list(range(0, len(ijkl), 3)) + [5, 5, 0]:  # repeats and jumps: unchanged, k-only and full refills
+        i, j, k, klo = (int(v) for v in ijkl[t])
+        sl = T.triple_slices(s, i, j, k, k)  # the k-chunk base at k: the buffers hold exactly one block
+        for n in T.BODY_ORDER:
+            np.copyto(bufs[n], sl[n][:sizes[n]])
+        got = _call_with_buffers(T, s, bufs, i, j, k, k)
+        want = T.cbody(s, i, j, k, klo)
+        assert _close(got[0], want[0], 1e-12, abs(want[0]) + 1e-300) and \
+            _close(got[1], want[1], 1e-12, abs(want[1]) + 1e-300), (t, got, want)

@@ -209,7 +209,10 @@ struct trpdrv_plan {
     cudaStream_t last_stream;
     int use_tma;        /* the fused launch stages panels with TMA (fused_tma.cu) */
     int tma_mma_k;      /* FP64 MMA shape of the TMA kernel: 8 (m16n8k8) or 16 (m16n8k16) */
-    double *d_fbuf;     /* emulated form: f of one batch of triples [fbuf_batch][8][nvir][nvir] */
+    double *d_fbuf;     /* emulated form: f of two batches of triples [2][fbuf_batch][8][nvir][nvir] */
+    size_t fbuf_half;   /* doubles in one of the two halves */
+    cudaStream_t aux_stream;          /* emulated form: energies of batch n beside the products of n + 1 */
+    cudaEvent_t ev_gemm[2], ev_tengy[2];
     int fbuf_batch;     /* triples d_fbuf holds (>= opt.batch, and room for the autotuner's batches) */
     int tuned_staging;  /* FUSED staging chosen by the autotuner (1 cp.async, 2 TMA), 0 = none */
     void *tma_maps;     /* tensor maps of every system, passed by value to each launch */
@@ -272,6 +275,11 @@ static void plan_free(trpdrv_plan *p)
     if (p->d_tot) cudaFree(p->d_tot);
     if (p->d_f) cudaFree(p->d_f);
     if (p->d_fbuf) cudaFree(p->d_fbuf);
+    for (int h = 0; h < 2; ++h) {
+        if (p->ev_gemm[h]) cudaEventDestroy(p->ev_gemm[h]);
+        if (p->ev_tengy[h]) cudaEventDestroy(p->ev_tengy[h]);
+    }
+    if (p->aux_stream) cudaStreamDestroy(p->aux_stream);
     if (p->d_bpart) cudaFree(p->d_bpart);
     if (p->d_tcount) cudaFree(p->d_tcount);
     if (p->ev0) cudaEventDestroy(p->ev0);
@@ -406,7 +414,13 @@ static int plan_build(trpdrv_plan *p, const trpdrv_system *shape)
     CUDA_TRY(cudaMemset(p->d_tot, 0, sizeof(double) * 4 * (size_t)p->nsys));
     if (o->mode == TRPDRV_MODE_EMULATED) {
         p->fbuf_batch = o->batch > TUNE_MAX_BATCH ? o->batch : TUNE_MAX_BATCH;
-        CUDA_TRY(cudaMalloc((void **)&p->d_fbuf, sizeof(double) * 8 * (size_t)p->fbuf_batch * maxv * maxv));
+        p->fbuf_half = 8 * (size_t)p->fbuf_batch * maxv * maxv;
+        CUDA_TRY(cudaMalloc((void **)&p->d_fbuf, sizeof(double) * 2 * p->fbuf_half));
+        CUDA_TRY(cudaStreamCreateWithFlags(&p->aux_stream, cudaStreamNonBlocking));
+        for (int h = 0; h < 2; ++h) {
+            CUDA_TRY(cudaEventCreateWithFlags(&p->ev_gemm[h], cudaEventDisableTiming));
+            CUDA_TRY(cudaEventCreateWithFlags(&p->ev_tengy[h], cudaEventDisableTiming));
+        }
     }
     if (o->mode == TRPDRV_MODE_PLAIN) {
         CUDA_TRY(cudaMalloc((void **)&p->d_f, sizeof(double) * 8 * (size_t)maxv * maxv));
@@ -643,11 +657,42 @@ static int enqueue_fused(trpdrv_plan *p, cudaStream_t st, int capturing)
     return TRPDRV_OK;
 }
 
+/* Emulated form, positions [pos0, pos1) of one system in batches of `batch`: each batch's contraction
+ * launch writes its f into one half of d_fbuf, and its energies run on the auxiliary stream (128-thread
+ * CTAs beside the next batch's contraction kernel on the same SMs) while the next batch's products go
+ * to the other half.  *bi counts batches over a whole execution (it picks the half); a half is reused
+ * only after the energies that read it.  Finish with emulated_join. */
+static int emulated_batches(trpdrv_plan *p, const trpdrv_dev_system *d, const sysbuf *b, int64_t pos0, int64_t pos1,
+                            int batch, cudaStream_t st, int64_t *bi, int64_t *launches)
+{
+    for (int64_t pos = pos0; pos < pos1; pos += batch) {
+        const int n = (int)(pos1 - pos < batch ? pos1 - pos : batch);
+        const int h = (int)(*bi & 1);
+        double *fb = p->d_fbuf + (size_t)h * p->fbuf_half;
+        if (*bi >= 2) CUDA_TRY(cudaStreamWaitEvent(st, p->ev_tengy[h], 0));
+        LAUNCH_TRY(trpdrv_launch_oz_gemm(d, &b->oz, b->oz_maps, pos, n, fb, p->d_status, p->nsm, st));
+        CUDA_TRY(cudaEventRecord(p->ev_gemm[h], st));
+        CUDA_TRY(cudaStreamWaitEvent(p->aux_stream, p->ev_gemm[h], 0));
+        LAUNCH_TRY(trpdrv_launch_oz_tengy(d, pos, n, fb, 128, p->aux_stream));
+        CUDA_TRY(cudaEventRecord(p->ev_tengy[h], p->aux_stream));
+        ++*bi;
+        if (launches) *launches += 2;
+    }
+    return TRPDRV_OK;
+}
+
+/* the main stream waits for every energy launch of the batches enqueued so far */
+static int emulated_join(trpdrv_plan *p, cudaStream_t st, int64_t bi)
+{
+    for (int h = 0; h < 2 && h < bi; ++h) CUDA_TRY(cudaStreamWaitEvent(st, p->ev_tengy[h], 0));
+    return TRPDRV_OK;
+}
+
 /* Emulated form: slice every operand once per execution, then per batch of `batch` triples (in the
- * processing order) one contraction launch writing their f and one tengy launch. */
+ * processing order) one contraction launch writing their f and one energy launch beside the next. */
 static int enqueue_emulated(trpdrv_plan *p, cudaStream_t st, int capturing)
 {
-    int64_t launches = 0;
+    int64_t launches = 0, bi = 0;
     CUDA_TRY(cudaMemsetAsync(p->d_status, 0, sizeof(int), st));
     CUDA_TRY(cudaMemsetAsync(p->d_tot, 0, sizeof(double) * 4 * (size_t)p->nsys, st));
     CUDA_TRY(cudaEventRecordWithFlags(p->ev0, st, capturing ? cudaEventRecordExternal : cudaEventRecordDefault));
@@ -657,13 +702,9 @@ static int enqueue_emulated(trpdrv_plan *p, cudaStream_t st, int capturing)
         if (d->ntriples <= 0) continue;
         LAUNCH_TRY(trpdrv_launch_oz_slices(d, &b->oz, st));
         ++launches;
-        for (int64_t pos = 0; pos < d->ntriples; pos += p->opt.batch) {
-            const int n = (int)(d->ntriples - pos < p->opt.batch ? d->ntriples - pos : p->opt.batch);
-            LAUNCH_TRY(trpdrv_launch_oz_gemm(d, &b->oz, b->oz_maps, pos, n, p->d_fbuf, p->d_status, p->nsm, st));
-            LAUNCH_TRY(trpdrv_launch_oz_tengy(d, pos, n, p->d_fbuf, st));
-            launches += 2;
-        }
+        TRY(emulated_batches(p, d, b, 0, d->ntriples, p->opt.batch, st, &bi, &launches));
     }
+    TRY(emulated_join(p, st, bi));
     CUDA_TRY(cudaEventRecordWithFlags(p->ev1, st, capturing ? cudaEventRecordExternal : cudaEventRecordDefault));
     for (int q = 0; q < p->nsys; ++q) {
         if (p->h_dev[q].ntriples <= 0) continue;
@@ -1294,12 +1335,10 @@ static int tune_time(trpdrv_plan *p, const trpdrv_tune_candidate *c, double *est
             const int64_t n = d->ntriples < want ? d->ntriples : want;
             LAUNCH_TRY(trpdrv_launch_oz_slices(d, &b->oz, st));
             for (int rep = 0; rep < 2; ++rep) {
+                int64_t bi = 0;
                 CUDA_TRY(cudaEventRecord(p->ev0, st));
-                for (int64_t pos = 0; pos < n; pos += c->batch) {
-                    const int m = (int)(n - pos < c->batch ? n - pos : c->batch);
-                    LAUNCH_TRY(trpdrv_launch_oz_gemm(d, &b->oz, b->oz_maps, pos, m, p->d_fbuf, p->d_status, p->nsm, st));
-                    LAUNCH_TRY(trpdrv_launch_oz_tengy(d, pos, m, p->d_fbuf, st));
-                }
+                TRY(emulated_batches(p, d, b, 0, n, c->batch, st, &bi, NULL));
+                TRY(emulated_join(p, st, bi));
                 CUDA_TRY(cudaEventRecord(p->ev1, st));
                 TRY(tune_elapsed(p, &ms));
             }
@@ -1339,11 +1378,9 @@ static int tune_sample_records(trpdrv_plan *p, double **host)
         if (d->ntriples <= 0) continue;
         const int64_t n = d->ntriples < 64 ? d->ntriples : 64;
         LAUNCH_TRY(trpdrv_launch_oz_slices(d, &b->oz, st));
-        for (int64_t pos = 0; pos < n; pos += p->opt.batch) {
-            const int m = (int)(n - pos < p->opt.batch ? n - pos : p->opt.batch);
-            LAUNCH_TRY(trpdrv_launch_oz_gemm(d, &b->oz, b->oz_maps, pos, m, p->d_fbuf, p->d_status, p->nsm, st));
-            LAUNCH_TRY(trpdrv_launch_oz_tengy(d, pos, m, p->d_fbuf, st));
-        }
+        int64_t bi = 0;
+        TRY(emulated_batches(p, d, b, 0, n, p->opt.batch, st, &bi, NULL));
+        TRY(emulated_join(p, st, bi));
         LAUNCH_TRY(trpdrv_launch_item_reduce(d, st));
         CUDA_TRY(cudaMemcpyAsync(host[q], b->rec, sizeof(double) * 4 * (size_t)b->ntriples, cudaMemcpyDeviceToHost, st));
     }

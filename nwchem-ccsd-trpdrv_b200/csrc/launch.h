@@ -101,8 +101,10 @@ int trpdrv_oz_prepare(const trpdrv_oz_system *oz, void *maps_out);
 int trpdrv_launch_oz_slices(const trpdrv_dev_system *h_sys, const trpdrv_oz_system *oz, void *stream);
 int trpdrv_launch_oz_gemm(const trpdrv_dev_system *h_sys, const trpdrv_oz_system *oz, const void *maps,
                           int64_t pos0, int npos, double *fbuf, int *status, int grid, void *stream);
+/* threads: 256 to run alone, 128 to run beside the contraction kernel (emulated plans overlap the
+ * energies of one batch with the next batch's products on a second stream). */
 int trpdrv_launch_oz_tengy(const trpdrv_dev_system *h_sys, int64_t pos0, int npos, const double *fbuf,
-                           void *stream);
+                           int threads, void *stream);
 int trpdrv_oz_init(void);
 
 /* Per-triple sum of the per-item energies of one system (partial -> rec). */

@@ -539,8 +539,10 @@ __global__ void __launch_bounds__(256) oz_slice_kernel(const SliceParams P)
 // plan creation), so item_reduce sums them in a fixed order.
 // ------------------------------------------------------------------------------------------------
 constexpr int TW = 16;
-constexpr int TNTHREAD = 256;
 constexpr size_t TSMEM_BYTES = (size_t)16 * TW * (TW + 1) * sizeof(double);
+// 256 threads when the kernel runs alone; 128 (at most 96 registers) to run beside the persistent
+// contraction kernel on the same SMs: 128 x 96 registers and 35 KB of shared memory fit in what an
+// oz_gemm_kernel CTA leaves free on its SM.
 
 struct TengyParams {
     trpdrv_dev_system sys;
@@ -548,7 +550,8 @@ struct TengyParams {
     const double *fbuf;
 };
 
-__global__ void __launch_bounds__(TNTHREAD) oz_tengy_kernel(const TengyParams P)
+template <int TNTHREAD>
+__global__ void __launch_bounds__(TNTHREAD, TNTHREAD == 128 ? 5 : 1) oz_tengy_kernel(const TengyParams P)
 {
     extern __shared__ __align__(16) double park[];
     __shared__ double red[4 * (TNTHREAD / 32)];
@@ -753,7 +756,7 @@ extern "C" int trpdrv_launch_oz_gemm(const trpdrv_dev_system *h_sys, const trpdr
 }
 
 extern "C" int trpdrv_launch_oz_tengy(const trpdrv_dev_system *h_sys, int64_t pos0, int npos, const double *fbuf,
-                                      void *stream)
+                                      int threads, void *stream)
 {
     if (npos <= 0) return 0;
     const int np = oz::tengy_pairs(h_sys->nvir);
@@ -762,7 +765,13 @@ extern "C" int trpdrv_launch_oz_tengy(const trpdrv_dev_system *h_sys, int64_t po
     P.sys = *h_sys;
     P.pos0 = pos0;
     P.fbuf = fbuf;
-    oz::oz_tengy_kernel<<<dim3((unsigned)np, (unsigned)npos), oz::TNTHREAD, oz::TSMEM_BYTES, (cudaStream_t)stream>>>(P);
+    const dim3 grid((unsigned)np, (unsigned)npos);
+    if (threads == 128)
+        oz::oz_tengy_kernel<128><<<grid, 128, oz::TSMEM_BYTES, (cudaStream_t)stream>>>(P);
+    else if (threads == 256)
+        oz::oz_tengy_kernel<256><<<grid, 256, oz::TSMEM_BYTES, (cudaStream_t)stream>>>(P);
+    else
+        return (int)cudaErrorInvalidValue;
     return (int)cudaGetLastError();
 }
 
@@ -774,6 +783,9 @@ extern "C" int trpdrv_oz_init(void)
     if ((e = oz::set_attr<6>()) != 0) return e;
     if ((e = oz::set_attr<7>()) != 0) return e;
     if ((e = oz::set_attr<8>()) != 0) return e;
-    return (int)cudaFuncSetAttribute(oz::oz_tengy_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    if ((e = (int)cudaFuncSetAttribute(oz::oz_tengy_kernel<128>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)oz::TSMEM_BYTES)) != 0)
+        return e;
+    return (int)cudaFuncSetAttribute(oz::oz_tengy_kernel<256>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      (int)oz::TSMEM_BYTES);
 }

@@ -243,7 +243,8 @@ int trpdrv_plan_last_kernel_ms(trpdrv_plan *plan, double *ms);
 int trpdrv_plan_destroy(trpdrv_plan *plan);
 
 /* Autotuner: times every compiled variant of the plan's mode on a sample of the plan's own work and
- * keeps the fastest (FUSED: TMA vs cp.async staging, FP64 MMA shape m16n8k8 vs m16n8k4, CTAs per SM;
+ * keeps the fastest (FUSED: TMA vs cp.async staging, FP64 MMA shape (TMA m16n8k8 / m16n8k16, cp.async
+ * m16n8k8 / m16n8k4), edge tile shape (TMA: packed 2 x 32x16 or 32x32 items), CTAs per SM;
  * EMULATED: triples per launch pair, 4 / 8 / 16 / 32).  Needs a bound plan (after upload or bind); each
  * system is sampled (about 1/8 of its fused items, 64 triples in the emulated form) and the per-
  * system times are scaled to its full work.  EMULATED plans with target_digits first pick the fewest
@@ -258,6 +259,8 @@ typedef struct trpdrv_tune_candidate {
     int mma_k;            /* FUSED: FP64 MMA shape k (TMA: 8 or 16; cp.async: 4 or 8) */
     int ctas_per_sm;      /* FUSED cp.async grid */
     int batch;            /* EMULATED: triples per launch pair */
+    int edge_pack;        /* FUSED TMA: 1 = where the last tile holds at most 16 virtual indices, its tile
+                             pairs run two to a work item (2 x 32x16 tiles); 0 = one 32x32 pair per item */
     double ms_estimate;   /* estimated device time of one execution with this candidate */
 } trpdrv_tune_candidate;
 typedef struct trpdrv_tune_result {

@@ -1189,7 +1189,7 @@ static int tune_same(const tune_entry *a, const tune_entry *b)
 }
 
 /* ---- persistent tuning cache (TRPDRV_TUNE_CACHE = path of a text file shared by processes) ----
- * One line per choice: "<key> -> <staging> <mma_k> <ctas_per_sm> <batch> <ms>", where the key names
+ * One line per choice: "<key> -> <staging> <mma_k> <ctas_per_sm> <batch> <edge_pack> <ms>", where the key names
  * the device model (name, SM count), the library version and every field of tune_entry.  Lookups
  * take the last matching line; stores append under an exclusive lock. */
 static int tune_file_key(const trpdrv_plan *p, const tune_entry *k, char *buf, size_t n)
@@ -1223,8 +1223,8 @@ static int tune_file_lookup(const char *key, trpdrv_tune_candidate *out)
         if (strncmp(line, key, kl) != 0 || strncmp(line + kl, " -> ", 4) != 0) continue;
         trpdrv_tune_candidate c;
         memset(&c, 0, sizeof c);
-        if (sscanf(line + kl + 4, "%d %d %d %d %lf", &c.staging, &c.mma_k, &c.ctas_per_sm, &c.batch, &c.ms_estimate) ==
-            5) {
+        if (sscanf(line + kl + 4, "%d %d %d %d %d %lf", &c.staging, &c.mma_k, &c.ctas_per_sm, &c.batch, &c.edge_pack,
+                   &c.ms_estimate) == 6) {
             *out = c;
             found = 1;
         }
@@ -1241,8 +1241,8 @@ static void tune_file_store(const char *key, const trpdrv_tune_candidate *c)
     const int fd = open(path, O_WRONLY | O_APPEND | O_CREAT, 0644);
     if (fd < 0) return;
     char line[1200];
-    const int n = snprintf(line, sizeof line, "%s -> %d %d %d %d %.6f\n", key, c->staging, c->mma_k, c->ctas_per_sm,
-                           c->batch, c->ms_estimate);
+    const int n = snprintf(line, sizeof line, "%s -> %d %d %d %d %d %.6f\n", key, c->staging, c->mma_k,
+                           c->ctas_per_sm, c->batch, c->edge_pack, c->ms_estimate);
     if (n > 0 && (size_t)n < sizeof line && flock(fd, LOCK_EX) == 0) {
         ssize_t wr = write(fd, line, (size_t)n);
         (void)wr;
@@ -1263,6 +1263,20 @@ static int tune_usable(const trpdrv_plan *p, const trpdrv_tune_candidate *c)
     return c->batch >= 1 && c->batch <= p->fbuf_batch;
 }
 
+/* the TMA kernel's edge tile shape on every system (host mirror and device copy of the descriptors) */
+static int tune_set_edge_pack(trpdrv_plan *p, int pack)
+{
+    int changed = 0;
+    for (int q = 0; q < p->nsys; ++q) {
+        const int v = pack ? trpdrv_tma_pack_edge(p->s[q].shape.nvir) : 0;
+        changed |= p->h_dev[q].pack_edge != v;
+        p->h_dev[q].pack_edge = v;
+    }
+    if (changed && p->d_dev)
+        CUDA_TRY(cudaMemcpy(p->d_dev, p->h_dev, sizeof(trpdrv_dev_system) * (size_t)p->nsys, cudaMemcpyHostToDevice));
+    return TRPDRV_OK;
+}
+
 /* sets the plan's launch configuration to candidate c */
 static void tune_apply(trpdrv_plan *p, const trpdrv_tune_candidate *c)
 {
@@ -1270,6 +1284,7 @@ static void tune_apply(trpdrv_plan *p, const trpdrv_tune_candidate *c)
         p->use_tma = c->staging == 2;
         p->tuned_staging = c->staging; /* a later upload/bind keeps it where TMA remains possible */
         if (c->staging == 2) p->tma_mma_k = c->mma_k;
+        if (c->staging == 2) tune_set_edge_pack(p, c->edge_pack);
         if (c->staging == 1) {
             p->opt.mma_k = c->mma_k;
             p->opt.ctas_per_sm = c->ctas_per_sm;
@@ -1318,6 +1333,7 @@ static int tune_time(trpdrv_plan *p, const trpdrv_tune_candidate *c, double *est
                 CUDA_TRY(cudaMemcpyAsync(p->d_counter, &first, sizeof first, cudaMemcpyHostToDevice, st));
                 CUDA_TRY(cudaStreamSynchronize(st)); /* `first` is a host stack value */
                 CUDA_TRY(cudaEventRecord(p->ev0, st));
+                if (c->staging == 2) TRY(tune_set_edge_pack(p, c->edge_pack));
                 if (c->staging == 2)
                     LAUNCH_TRY(trpdrv_launch_fused_tma(p->d_dev, p->nsys, d->item_begin + sample, p->d_counter,
                                                        p->d_status, grid, p->tma_maps, c->mma_k, st));
@@ -1516,18 +1532,24 @@ int trpdrv_plan_autotune(trpdrv_plan *p, trpdrv_tune_result *result)
         int occ = 1;
         if (trpdrv_fused_max_ctas_per_sm(&occ) != 0 || occ < 1) occ = 1;
         if (p->opt.staging != 1 && trpdrv_tma_supported(p->h_dev, p->nsys) && p->tma_maps) {
-            c[n++] = (trpdrv_tune_candidate){2, 8, 1, 0, 0.0};
-            c[n++] = (trpdrv_tune_candidate){2, 16, 1, 0, 0.0};
+            int packable = 0;
+            for (int q = 0; q < p->nsys; ++q) packable |= trpdrv_tma_pack_edge(p->s[q].shape.nvir);
+            c[n++] = (trpdrv_tune_candidate){2, 8, 1, 0, packable, 0.0};
+            c[n++] = (trpdrv_tune_candidate){2, 16, 1, 0, packable, 0.0};
+            if (packable) {
+                c[n++] = (trpdrv_tune_candidate){2, 8, 1, 0, 0, 0.0};
+                c[n++] = (trpdrv_tune_candidate){2, 16, 1, 0, 0, 0.0};
+            }
         }
         if (p->opt.staging != 2) {
-            c[n++] = (trpdrv_tune_candidate){1, 8, occ, 0, 0.0};
-            c[n++] = (trpdrv_tune_candidate){1, 4, occ, 0, 0.0};
-            if (occ > 1) c[n++] = (trpdrv_tune_candidate){1, 8, 1, 0, 0.0};
+            c[n++] = (trpdrv_tune_candidate){1, 8, occ, 0, 0, 0.0};
+            c[n++] = (trpdrv_tune_candidate){1, 4, occ, 0, 0, 0.0};
+            if (occ > 1 && n < 8) c[n++] = (trpdrv_tune_candidate){1, 8, 1, 0, 0, 0.0};
         }
     } else {
         static const int batches[4] = {4, 8, 16, 32};
         for (int k = 0; k < 4; ++k)
-            if (batches[k] <= p->fbuf_batch) c[n++] = (trpdrv_tune_candidate){0, 0, 0, batches[k], 0.0};
+            if (batches[k] <= p->fbuf_batch) c[n++] = (trpdrv_tune_candidate){0, 0, 0, batches[k], 0, 0.0};
     }
     r->ncand = n;
     if (n == 0) return TRPDRV_OK;
@@ -2068,18 +2090,16 @@ static int body_fused(int ncor, int nocc, int nvir, int a, int i, int j, int k, 
     int status = 0;
     memcpy(&status, g_dif.h_io + nslot + 1, sizeof status);
     if (status) return fail(TRPDRV_ERR_DEVICE, "fused kernel reported status %d", status);
-    /* the item slots in a fixed order */
-    double r0 = 0.0, r1 = 0.0, r2 = 0.0, r3 = 0.0;
-    for (size_t q = 0; q < nslot; q += 4) {
-        r0 += g_dif.h_io[q];
-        r1 += g_dif.h_io[q + 1];
-        r2 += g_dif.h_io[q + 2];
-        r3 += g_dif.h_io[q + 3];
+    /* the item slots in a fixed order, compensated (Neumaier) */
+    for (int c = 0; c < 4; ++c) {
+        double sum = 0.0, comp = 0.0;
+        for (size_t q = (size_t)c; q < nslot; q += 4) {
+            const double x = g_dif.h_io[q], t = sum + x;
+            comp += fabs(sum) >= fabs(x) ? (sum - t) + x : (x - t) + sum;
+            sum = t;
+        }
+        rec[c] = sum + comp;
     }
-    rec[0] = r0;
-    rec[1] = r1;
-    rec[2] = r2;
-    rec[3] = r3;
     return TRPDRV_OK;
 }
 

@@ -1,6 +1,6 @@
 // Deterministic energy reductions and small device utilities.
 //
-//  item_reduce_kernel:   per triple, the sum of its tile-pair items (fixed order) -> rec[t][4]
+//  item_reduce_kernel:   per triple, the compensated sum of its tile-pair items (fixed order) -> rec[t][4]
 //  system_reduce_kernel: per system, the compensated total of emp4i + [i != k] emp4k and of
 //                        emp5i + [i != k] emp5k over the triples (the accumulation of
 //                        omp/ccsd_trpdrv_omp_cbody.c:133-142), as a double-double (hi, lo) pair,
@@ -22,22 +22,21 @@ __global__ void item_reduce_kernel(const double *__restrict__ partial, int npair
     if (t >= ntriples) return;
     const int nslot = npairs * TRPDRV_FUSED_SLOTS;
     const double *p = partial + 4 * t * (long long)nslot;
-    double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
+    // compensated per lane (error-free TwoSum, errors carried in lo), then the lanes' hi and lo sums
+    double hi[4] = {0.0, 0.0, 0.0, 0.0}, lo[4] = {0.0, 0.0, 0.0, 0.0};
     for (int q = lane; q < nslot; q += 32) {
-        s0 += p[4 * q + 0];
-        s1 += p[4 * q + 1];
-        s2 += p[4 * q + 2];
-        s3 += p[4 * q + 3];
+#pragma unroll
+        for (int c = 0; c < 4; ++c) {
+            double s, e;
+            two_sum(hi[c], p[4 * q + c], s, e);
+            hi[c] = s;
+            lo[c] += e;
+        }
     }
-    s0 = warp_sum(s0);
-    s1 = warp_sum(s1);
-    s2 = warp_sum(s2);
-    s3 = warp_sum(s3);
-    if (lane == 0) {
-        rec[4 * t + 0] = s0;
-        rec[4 * t + 1] = s1;
-        rec[4 * t + 2] = s2;
-        rec[4 * t + 3] = s3;
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+        const double h = warp_sum(hi[c]), l = warp_sum(lo[c]);
+        if (lane == 0) rec[4 * t + c] = h + l;
     }
 }
 

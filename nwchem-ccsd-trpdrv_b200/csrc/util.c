@@ -9,7 +9,7 @@
 #include <stdlib.h>
 #include <string.h>
 
-int trpdrv_version(void) { return 10000; /* 1.0.0 */ }
+int trpdrv_version(void) { return 10100; /* 1.1.0 */ }
 
 int64_t trpdrv_count_triples(int nocc)
 {

@@ -102,7 +102,7 @@ _proto("trpdrv_plan_staging", C.c_int, [C.c_void_p])
 
 class TuneCandidate(C.Structure):
     _fields_ = [("staging", C.c_int), ("mma_k", C.c_int), ("ctas_per_sm", C.c_int), ("batch", C.c_int),
-                ("ms_estimate", C.c_double)]
+                ("edge_pack", C.c_int), ("ms_estimate", C.c_double)]
 
 
 class TuneResult(C.Structure):
@@ -475,7 +475,7 @@ class Plan:
         r = TuneResult()
         _check(lib.trpdrv_plan_autotune(self.h, C.byref(r)))
         cands = [{"staging": c.staging, "mma_k": c.mma_k, "ctas_per_sm": c.ctas_per_sm, "batch": c.batch,
-                  "ms_estimate": c.ms_estimate} for c in r.cand[:r.ncand]]
+                  "edge_pack": c.edge_pack, "ms_estimate": c.ms_estimate} for c in r.cand[:r.ncand]]
         return {"candidates": cands, "chosen": r.chosen, "from_cache": int(r.from_cache), "slices": r.slices,
                 "est_rel_err": r.est_rel_err}
 

@@ -110,3 +110,20 @@ def test_tuning_cache_file_is_read_by_a_second_process(T, tmp_path):
     lines = cache.read_text().splitlines()
     assert len(lines) == 1 and "trpdrv-tune" in lines[0] and "shapes=8,64,1" in lines[0]
     assert abs(runs[1]["e4"] - runs[0]["e4"]) <= 1e-12 * abs(runs[0]["e4"])
+
+
+def test_edge_tile_shape_is_a_tuning_choice_and_keeps_parity(T, O):
+    """nvir = 134: the last tile holds 6 indices, so the TMA candidates come with packed (two 32x16 pairs
+    per item) and ordinary edge items; whichever is chosen matches the oracle."""
+    s = T.synth_system(6, 134, seed=65)
+    rec_o, tot_o, mism = O.run_system(s, "port", nthreads=4)
+    assert mism == 0
+    with T.Plan([s], mode=T.MODE_FUSED) as p:
+        p.upload()
+        r = p.autotune()
+        tma = [c for c in r["candidates"] if c["staging"] == 2]
+        assert {c["edge_pack"] for c in tma} == {0, 1} and {c["mma_k"] for c in tma} == {8, 16}
+        e4, e5, recs = _energies(p)
+    assert_records_close(recs[0], rec_o)
+    assert_total_close(e4[0], tot_o[0], what="emp4")
+    assert_total_close(e5[0], tot_o[1], what="emp5")

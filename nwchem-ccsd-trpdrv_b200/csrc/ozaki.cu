@@ -550,16 +550,17 @@ struct TengyParams {
     const double *fbuf;
 };
 
+// One work item = (16-wide tile pair, batch position); CTA b takes items b, b + grid, ...  With one
+// CTA per item (the standalone launch) every CTA does one; the launch beside the contraction kernel
+// uses one CTA per SM, so that its CTAs never hold an SM the contraction kernel's CTAs need.
 template <int TNTHREAD>
-__global__ void __launch_bounds__(TNTHREAD, TNTHREAD == 128 ? 5 : 1) oz_tengy_kernel(const TengyParams P)
+__device__ __forceinline__ void tengy_item(const TengyParams &P, int np, int pairi, int y, double *park, double *red)
 {
-    extern __shared__ __align__(16) double park[];
-    __shared__ double red[4 * (TNTHREAD / 32)];
     constexpr int TP = TW + 1, TILE = TW * TP;
     const trpdrv_dev_system &S = P.sys;
     const int nvir = S.nvir, tid = threadIdx.x;
     const int nb = (nvir + TW - 1) / TW;
-    const long long pos = P.pos0 + blockIdx.y;  // a position over the records ([a][triple])
+    const long long pos = P.pos0 + y;  // a position over the records ([a][triple])
     if (pos >= S.ntriples || S.nt <= 0) return;
     const unsigned ai = pos >= S.nt ? (unsigned)pos / (unsigned)S.nt : 0u;  // records < 2^31
     const long long tpos = pos - (long long)ai * S.nt;
@@ -568,7 +569,7 @@ __global__ void __launch_bounds__(TNTHREAD, TNTHREAD == 128 ? 5 : 1) oz_tengy_ke
     const int packed = S.triples[tt];
     const int i = packed & 1023, j = (packed >> 10) & 1023, k = (packed >> 20) & 1023;
 
-    int B = 0, rem = blockIdx.x;
+    int B = 0, rem = pairi;
     while (B < nb && rem >= nb - B) {
         rem -= nb - B;
         ++B;
@@ -577,7 +578,7 @@ __global__ void __launch_bounds__(TNTHREAD, TNTHREAD == 128 ? 5 : 1) oz_tengy_ke
     const int b0 = B * TW, c0 = Cb * TW;
     const bool diag = (B == Cb);
     const size_t lnvv = (size_t)nvir * nvir;
-    const double *f = P.fbuf + (size_t)blockIdx.y * 8 * lnvv;
+    const double *f = P.fbuf + (size_t)y * 8 * lnvv;
 
     // park f(B,C) (o = 0) and f(C,B) (o = 1) tiles of all eight f; column q of a tile is contiguous in f.
     // Every copy of a thread is issued before any is waited for (cp.async, zero fill outside nvir), so
@@ -611,12 +612,24 @@ __global__ void __launch_bounds__(TNTHREAD, TNTHREAD == 128 ? 5 : 1) oz_tengy_ke
     tengy_tile_pair_w<TW>(park, b0, c0, diag, v, tid, TNTHREAD, su);
     const TengySums tot = block_sum4(su, red);
     if (tid == 0) {  // block_sum4's result is valid in thread 0
-        double *out = S.partial + ((size_t)((long long)ai * S.nt + tt) * S.npairs * TRPDRV_FUSED_SLOTS + blockIdx.x) * 4;
+        double *out = S.partial + ((size_t)((long long)ai * S.nt + tt) * S.npairs * TRPDRV_FUSED_SLOTS + pairi) * 4;
         out[0] = tot.e4i;
         out[1] = tot.e5i;
         out[2] = tot.e4k;
         out[3] = tot.e5k;
     }
+    __syncthreads();  // the park and the reduction scratch are reused by the CTA's next item
+}
+
+template <int TNTHREAD>
+__global__ void __launch_bounds__(TNTHREAD, TNTHREAD == 128 ? 5 : 1)
+oz_tengy_kernel(const TengyParams P, int np, int npos)
+{
+    extern __shared__ __align__(16) double park[];
+    __shared__ double red[4 * (TNTHREAD / 32)];
+    const long long items = (long long)np * npos;
+    for (long long w = blockIdx.x; w < items; w += gridDim.x)
+        tengy_item<TNTHREAD>(P, np, (int)(w % np), (int)(w / np), park, red);
 }
 
 // number of 16-wide tile pairs (must fit in the npairs * TRPDRV_FUSED_SLOTS slots of a triple)
@@ -765,13 +778,19 @@ extern "C" int trpdrv_launch_oz_tengy(const trpdrv_dev_system *h_sys, int64_t po
     P.sys = *h_sys;
     P.pos0 = pos0;
     P.fbuf = fbuf;
-    const dim3 grid((unsigned)np, (unsigned)npos);
-    if (threads == 128)
-        oz::oz_tengy_kernel<128><<<grid, 128, oz::TSMEM_BYTES, (cudaStream_t)stream>>>(P);
-    else if (threads == 256)
-        oz::oz_tengy_kernel<256><<<grid, 256, oz::TSMEM_BYTES, (cudaStream_t)stream>>>(P);
-    else
+    const long long items = (long long)np * npos;
+    if (threads == 128) {  // beside the contraction kernel: one CTA per SM
+        int dev = 0, nsm = 1;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+        const unsigned grid = (unsigned)(items < nsm ? items : nsm);
+        oz::oz_tengy_kernel<128><<<grid, 128, oz::TSMEM_BYTES, (cudaStream_t)stream>>>(P, np, npos);
+    } else if (threads == 256) {
+        if (items > 0x7fffffffLL) return (int)cudaErrorInvalidValue;
+        oz::oz_tengy_kernel<256><<<(unsigned)items, 256, oz::TSMEM_BYTES, (cudaStream_t)stream>>>(P, np, npos);
+    } else {
         return (int)cudaErrorInvalidValue;
+    }
     return (int)cudaGetLastError();
 }
 

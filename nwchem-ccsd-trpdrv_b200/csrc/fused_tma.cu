@@ -80,6 +80,9 @@ struct ItemCtx {
     double eaijk;
     int ncor, nocc, nvir, b0, c0, diag, nV, nch, state;  // state: 1 work, 0 malformed, -1 end
     int packed, b1;      // packed edge item: pairs (b0, c0) and (b1, c0); b1 < 0 when the second is absent
+    int split, ch0, cstep;  // split item: this half runs chunks ch0, ch0 + cstep, ... (cstep 2, else 1)
+    double *scr;         // split item: [2 halves][64][256] partial f / gT of this item
+    unsigned *cnt;       // split item: arrivals of the two halves
 };
 
 // Packed edge items (systems with pack_edge: the last column tile E holds 1..16 valid indices).  The
@@ -410,7 +413,9 @@ __device__ __forceinline__ void producer(const trpdrv_dev_system *__restrict__ s
         int s = 0;
         while (s + 1 < nsys && item >= sys[s + 1].item_begin) ++s;
         const trpdrv_dev_system &S = sys[s];
-        const long long local = item - S.item_begin;
+        // a split system has two work items (halves of the contraction) per pair
+        const int hpart = S.split ? (int)((item - S.item_begin) & 1) : 0;
+        const long long local = S.split ? (item - S.item_begin) >> 1 : item - S.item_begin;
         const long long qpos = local / S.npairs;  // processing position over the system's records
         const int p = (int)(local - qpos * S.npairs);
         // a index (records are [a][triple], fewer than 2^31: the host checks); no division for a single a
@@ -481,7 +486,12 @@ __device__ __forceinline__ void producer(const trpdrv_dev_system *__restrict__ s
             cx.c0 = C0;
             cx.diag = diag;
             cx.nV = nV;
-            cx.nch = nV + nO;
+            cx.split = S.split;
+            cx.ch0 = S.split ? hpart : 0;
+            cx.cstep = S.split ? 2 : 1;
+            cx.nch = S.split ? (nV + nO - hpart + 1) / 2 : nV + nO;
+            cx.scr = S.split ? S.split_scratch + (size_t)own * 2 * 64 * 256 : nullptr;
+            cx.cnt = S.split ? S.split_count + own : nullptr;
             cx.state = 1;
         }
 
@@ -509,10 +519,11 @@ __device__ __forceinline__ void producer(const trpdrv_dev_system *__restrict__ s
                 off = (lane < 16 ? PK_B1B + pp : PK_B3B + pp) * PANEL_BYTES + half * KBOX;
             }
             tb = tb >= 0 ? tb * T : -1;
-            const int nsl = 2 * (nV + nO);
+            const int pch0 = S.split ? hpart : 0, pstep = S.split ? 2 : 1;
+            const int nsl = 2 * (S.split ? (nV + nO - hpart + 1) / 2 : nV + nO);
             for (int sl = 0; sl < nsl; ++sl) {
                 if (!mbar_wait(&empty[stage], phase ^ 1, status)) return;
-                const int fam = sl & 1, ch = sl >> 1;
+                const int fam = sl & 1, ch = pch0 + (sl >> 1) * pstep;
                 const bool ph1 = ch >= nV;
                 const int kk0 = (ph1 ? ch - nV : ch) * DK;
                 const int za = fam ? zk : zi;
@@ -565,7 +576,7 @@ __device__ __forceinline__ void producer(const trpdrv_dev_system *__restrict__ s
         const int pnl = fam * 8 + (slot < 2 ? 0 : slot < 4 ? 2 : slot < 6 ? 4 : 6) + o;
         const bool mine = lane < 28 && (!diag || o == 0);
         const unsigned bytes = (diag ? NPANEL / 2 : NPANEL) * PANEL_BYTES;
-        for (int ch = 0; ch < nV + nO; ++ch) {
+        for (int ch = S.split ? hpart : 0; ch < nV + nO; ch += S.split ? 2 : 1) {
             if (!mbar_wait(&empty[stage], phase ^ 1, status)) return;
             if (lane == 0) mbar_arrive_expect_tx(&full[stage], bytes);
             __syncwarp();
@@ -595,6 +606,52 @@ __device__ __forceinline__ void producer(const trpdrv_dev_system *__restrict__ s
 }
 
 // ------------------------------------------------------------------------------------------------
+// Split items: both halves write their partial f and f-transposed to scratch (thread-major, so the
+// 256 consumer threads write consecutive addresses), make them visible (fence), and one thread counts
+// the arrival.  The second half to arrive adds the first's partials and finishes the item (fin = 1);
+// the first stops there.  Two rounds of the consumer barrier order the writes before the count and
+// broadcast its result; the counter is reset by the second arrival.  Nothing waits for the other CTA.
+// Returns false when a barrier wait ran out (status set).
+__device__ __forceinline__ bool split_combine(const ItemCtx &cx, double (&f)[8][4], double (&gT)[8][4], int warp,
+                                              int lane, unsigned long long *xbar, unsigned &xphase, int *flag,
+                                              int *status, int &fin)
+{
+    const int tc = warp * 32 + lane;
+    double *mine = cx.scr + (size_t)(cx.ch0 ? 64 * 256 : 0) + tc;
+#pragma unroll
+    for (int x = 0; x < 8; ++x)
+#pragma unroll
+        for (int e = 0; e < 4; ++e) {
+            mine[(x * 4 + e) * 256] = f[x][e];
+            mine[(32 + x * 4 + e) * 256] = gT[x][e];
+        }
+    __threadfence();
+    __syncwarp();
+    if (lane == 0) mbar_arrive(xbar);
+    if (!mbar_wait(xbar, xphase, status)) return false;
+    xphase ^= 1;
+    if (tc == 0) *flag = (int)atomicAdd(cx.cnt, 1u);
+    __syncwarp();
+    if (lane == 0) mbar_arrive(xbar);
+    if (!mbar_wait(xbar, xphase, status)) return false;
+    xphase ^= 1;
+    fin = *flag != 0;
+    if (fin) {
+        __threadfence();
+        const double *other = cx.scr + (size_t)(cx.ch0 ? 0 : 64 * 256) + tc;
+#pragma unroll
+        for (int x = 0; x < 8; ++x)
+#pragma unroll
+            for (int e = 0; e < 4; ++e) {
+                f[x][e] += __ldcg(other + (x * 4 + e) * 256);
+                gT[x][e] += __ldcg(other + (32 + x * 4 + e) * 256);
+            }
+        if (tc == 0) *cx.cnt = 0u;
+    }
+    return true;
+}
+
+// ------------------------------------------------------------------------------------------------
 template <int KS>
 __global__ void __launch_bounds__(NTHREAD, 1)
 fused_tma_kernel(const trpdrv_dev_system *__restrict__ sys, int nsys, long long total, unsigned long long *counter,
@@ -605,6 +662,7 @@ fused_tma_kernel(const trpdrv_dev_system *__restrict__ sys, int nsys, long long 
     __shared__ ItemCtx ring[RING];
     __shared__ double xbuf[2 * XBUF];                       // diagonal-pair transpose exchange
     __shared__ __align__(8) unsigned long long xbar[1];
+    __shared__ int split_flag[1];
     char *stages = reinterpret_cast<char *>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~(uintptr_t)1023);
 
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -667,7 +725,7 @@ fused_tma_kernel(const trpdrv_dev_system *__restrict__ sys, int nsys, long long 
             for (int sl = 0; sl < nsl; ++sl) {
                 if (sl > 0 && !mbar_wait(&full[stage], phase, status)) return;
                 const char *st = stages + (size_t)stage * STAGE_BYTES;
-                const int ch = sl >> 1;
+                const int ch = cx.ch0 + (sl >> 1) * cx.cstep;
                 const bool ph1 = ch >= pnV;
                 const int kval = ph1 ? cx.nocc - (ch - pnV) * DK : cx.nvir - ch * DK;
                 if (pactive) {
@@ -685,6 +743,11 @@ fused_tma_kernel(const trpdrv_dev_system *__restrict__ sys, int nsys, long long 
                     phase ^= 1;
                 }
             }
+            if (cx.split) {
+                int fin = 0;
+                if (!split_combine(cx, f, gT, warp, lane, xbar, xphase, split_flag, status, fin)) return;
+                if (!fin) continue;
+            }
             if (pb0 >= 0) {  // this pair's slots: the 4 sub-blocks' sums, zeros in the other 4
                 double *out = pp ? cx.out1 : cx.out;
                 warp_epilogue(cx, f, gT, pb0 + prs * 16, cx.c0 + pcs * 8, g, t, lane, out + sub * 4);
@@ -699,13 +762,14 @@ fused_tma_kernel(const trpdrv_dev_system *__restrict__ sys, int nsys, long long 
         const bool active = (cx.b0 + rx0 < cx.nvir) && (cx.c0 + cx0 < cx.nvir);
         const bool diag = cx.diag != 0;
         const int pf = nch > 3 ? nch - 3 : 0;
-        for (int ch = 0; ch < nch; ++ch) {
-            if (ch > 0 && !mbar_wait(&full[stage], phase, status)) return;
+        for (int c = 0; c < nch; ++c) {
+            const int ch = cx.ch0 + c * cx.cstep;
+            if (c > 0 && !mbar_wait(&full[stage], phase, status)) return;
             const char *st = stages + (size_t)stage * STAGE_BYTES;
             const bool ph1 = ch >= nV;
             // the second k-step of a chunk is skipped when it lies entirely in the zero padding
             const int kval = ph1 ? cx.nocc - (ch - nV) * DK : cx.nvir - ch * DK;
-            if (ch == pf) prefetch_epilogue(cx, lane);
+            if (c == pf) prefetch_epilogue(cx, lane);
             if (KS == 16 && active && kval > 8) {
                 // one m16n8k16 per product: the fragments of both k-steps of the chunk side by side
 #pragma unroll
@@ -788,6 +852,11 @@ fused_tma_kernel(const trpdrv_dev_system *__restrict__ sys, int nsys, long long 
                 stage = 0;
                 phase ^= 1;
             }
+        }
+        if (cx.split) {  // the second half to arrive adds the first's partial sums and finishes the item
+            int fin = 0;
+            if (!split_combine(cx, f, gT, warp, lane, xbar, xphase, split_flag, status, fin)) return;
+            if (!fin) continue;
         }
         if (diag) {
             // f(c,b) of a diagonal pair is f at the mirrored position of the same 32x32 block, held

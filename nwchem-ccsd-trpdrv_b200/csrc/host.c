@@ -1875,7 +1875,9 @@ static struct dropin_fused {
     int dev_valid[DR_N];       /* the device copy of the region equals the host mirror */
     double *d_block, *h_block;
     trpdrv_dev_system h_sys;
-    double *d_io, *h_io; /* per-item energy slots [npairs][8][4], then counter (8 bytes) and status */
+    double *d_io, *h_io; /* per-item energy slots [npairs][8][4], then the work counter (8 bytes), the status
+                            and the split items' arrival counters, all cleared before every launch */
+    double *d_split;     /* split items: partial f of both halves of every item */
     void *maps;
 } g_dif;
 
@@ -1886,6 +1888,7 @@ static void dif_release(void)
     cudaFreeHost(g_dif.h_block);
     cudaFree(g_dif.d_io);
     cudaFreeHost(g_dif.h_io);
+    cudaFree(g_dif.d_split);
     free(g_dif.maps);
     memset(&g_dif, 0, sizeof g_dif);
 }
@@ -1920,9 +1923,11 @@ static int dif_prepare(int ncor, int nocc, int nvir)
     CUDA_TRY(cudaMalloc((void **)&g_dif.d_block, sizeof(double) * total));
     CUDA_TRY(cudaMallocHost((void **)&g_dif.h_block, sizeof(double) * total));
     const size_t nslot = 4 * TRPDRV_FUSED_SLOTS * (size_t)npairs;
-    CUDA_TRY(cudaMalloc((void **)&g_dif.d_io, sizeof(double) * (nslot + 2)));
+    CUDA_TRY(cudaMalloc((void **)&g_dif.d_io, sizeof(double) * (nslot + 2 + (size_t)(npairs + 1) / 2)));
     CUDA_TRY(cudaMallocHost((void **)&g_dif.h_io, sizeof(double) * (nslot + 2)));
     g_dif.ready = 1; /* from here dif_release frees whatever was allocated */
+    /* every tile pair's contraction runs as two halves on two SMs (one triple has only npairs items) */
+    CUDA_TRY(cudaMalloc((void **)&g_dif.d_split, sizeof(double) * 2 * 64 * 256 * (size_t)npairs));
     memset(g_dif.h_block, 0, sizeof(double) * total);
     double *d = g_dif.d_block;
     const double *I = d + g_dif.reg_off[DR_I], *vec = d + g_dif.reg_off[DR_VEC];
@@ -1938,6 +1943,9 @@ static int dif_prepare(int ncor, int nocc, int nvir)
     S->nt = 1;
     S->n_a = 1;
     S->one_triple = 1;
+    S->split = 1;
+    S->split_scratch = g_dif.d_split;
+    S->split_count = (unsigned *)(g_dif.d_io + nslot + 2);
     S->slot_stride = (int64_t)rs;
     S->item_begin = 0;
     S->t2 = I + g_dif.toff[DT_T2];
@@ -2079,10 +2087,10 @@ static int body_fused(int ncor, int nocc, int nvir, int a, int i, int j, int k, 
     CUDA_TRY(cudaMemcpyAsync(g_dif.d_block, h, sizeof(double) * g_dif.reg_off[DR_I], cudaMemcpyHostToDevice, st));
     if (gl.n) LAUNCH_TRY(trpdrv_launch_gather(&gl, st));
     const size_t nslot = 4 * TRPDRV_FUSED_SLOTS * (size_t)g_dif.npairs;
-    CUDA_TRY(cudaMemsetAsync(g_dif.d_io + nslot, 0, 2 * sizeof(double), st));
-    const int npairs = g_dif.npairs;
-    const int grid = npairs < g_dif.nsm ? npairs : g_dif.nsm;
-    LAUNCH_TRY(trpdrv_launch_fused_tma((const trpdrv_dev_system *)g_dif.d_block, 1, npairs,
+    CUDA_TRY(cudaMemsetAsync(g_dif.d_io + nslot, 0, sizeof(double) * (2 + (size_t)(g_dif.npairs + 1) / 2), st));
+    const int items = 2 * g_dif.npairs; /* two halves per tile pair */
+    const int grid = items < g_dif.nsm ? items : g_dif.nsm;
+    LAUNCH_TRY(trpdrv_launch_fused_tma((const trpdrv_dev_system *)g_dif.d_block, 1, items,
                                        (unsigned long long *)(g_dif.d_io + nslot), (int *)(g_dif.d_io + nslot + 1),
                                        grid, g_dif.maps, 8, st));
     CUDA_TRY(cudaMemcpyAsync(g_dif.h_io, g_dif.d_io, sizeof(double) * (nslot + 2), cudaMemcpyDeviceToHost, st));

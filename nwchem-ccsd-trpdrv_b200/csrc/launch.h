@@ -39,6 +39,12 @@ typedef struct trpdrv_dev_system {
     int64_t slot_stride; /* one_triple: doubles between the i-role and k-role blocks of every TMA-read tensor
                             (t2, jvv, kvv, ntov, nxov, jov, kov); 0 = the packed [2][block] layout.  The
                             vectors (dintc, dintx, t1v) stay packed [2][nvir]. */
+    int split;           /* 1 (one_triple systems): every item's contraction runs as two work items (even and
+                            odd chunks, item indices 2 q and 2 q + 1) on two SMs; each writes its partial f to
+                            split_scratch [item][2][64][256] and the second to arrive (split_count[item])
+                            adds the other's and runs the energy epilogue */
+    double *split_scratch;
+    unsigned *split_count;  /* one per item, zero at launch; left at zero */
     int pack_edge;       /* 1: the last tile holds 1..16 valid virtual indices and the TMA kernel runs the
                             edge pairs (B, E), (B + 1, E) (B even) as one packed work item; the item of
                             (B + 1, E) is then skipped (its energy slots are written by the packed one) */

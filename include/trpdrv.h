@@ -33,11 +33,12 @@ extern "C" {
  * tkj, jka, kka are offset by (k-klo)*nvir*nvir and tka, xka, jkj, kkj by (k-klo)*nocc*nvir, as in
  * the reference.  f1n..f4t are scratch: they are written back only when TRPDRV_WRITE_F=1.
  * Device work per call: with even nocc and nvir (and TRPDRV_WRITE_F unset) the slices are staged
- * into a fixed one-triple layout (host slices through a pinned buffer, copied by up to
- * TRPDRV_STAGE_THREADS host threads, default 8, then one host->device copy; slices inside registered
- * arrays gathered on the device) and one launch of the fused FP64 kernel computes the energies
- * without writing f; otherwise (or with TRPDRV_DROPIN_PATH=plain) the plain per-triple path runs (16
- * GEMMs into f, then the tengy reduction).  The call returns after the energies are back on the host.
+ * into a fixed one-triple layout (host slices compared with a pinned mirror and copied where they
+ * differ by up to TRPDRV_STAGE_THREADS host threads, default up to 16; the i-role and k-role blocks
+ * sent to the device only when changed; slices inside registered arrays gathered on the device) and
+ * one launch of the fused FP64 kernel computes the energies without writing f; otherwise (or with
+ * TRPDRV_DROPIN_PATH=plain) the plain per-triple path runs (16 GEMMs into f, then the tengy
+ * reduction).  The call returns after the energies are back on the host.
  * Errors (bad sizes/indices, CUDA failure) print to stderr and abort, unless TRPDRV_ON_ERROR=return,
  * in which case emp4/emp5 are left unchanged and trpdrv_last_error() reports the status. */
 void ccsd_trpdrv_omp_cbody_(double *f1n, double *f1t, double *f2n, double *f2t,

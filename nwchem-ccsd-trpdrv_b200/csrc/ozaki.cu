@@ -550,9 +550,8 @@ struct TengyParams {
     const double *fbuf;
 };
 
-// One work item = (16-wide tile pair, batch position); CTA b takes items b, b + grid, ...  With one
-// CTA per item (the standalone launch) every CTA does one; the launch beside the contraction kernel
-// uses one CTA per SM, so that its CTAs never hold an SM the contraction kernel's CTAs need.
+// One work item = (16-wide tile pair, batch position); CTA b takes items b, b + grid, ... (the
+// launches use one CTA per item).
 template <int TNTHREAD>
 __device__ __forceinline__ void tengy_item(const TengyParams &P, int np, int pairi, int y, double *park, double *red)
 {
@@ -779,12 +778,11 @@ extern "C" int trpdrv_launch_oz_tengy(const trpdrv_dev_system *h_sys, int64_t po
     P.pos0 = pos0;
     P.fbuf = fbuf;
     const long long items = (long long)np * npos;
-    if (threads == 128) {  // beside the contraction kernel: one CTA per SM
-        int dev = 0, nsm = 1;
-        cudaGetDevice(&dev);
-        cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-        const unsigned grid = (unsigned)(items < nsm ? items : nsm);
-        oz::oz_tengy_kernel<128><<<grid, 128, oz::TSMEM_BYTES, (cudaStream_t)stream>>>(P, np, npos);
+    if (items > 0x7fffffffLL) return (int)cudaErrorInvalidValue;
+    // one CTA per item: a launch of one CTA per SM beside the contraction kernel (each CTA looping
+    // over many items) was measured 30 % slower overall, too little memory parallelism per SM
+    if (threads == 128) {
+        oz::oz_tengy_kernel<128><<<(unsigned)items, 128, oz::TSMEM_BYTES, (cudaStream_t)stream>>>(P, np, npos);
     } else if (threads == 256) {
         if (items > 0x7fffffffLL) return (int)cudaErrorInvalidValue;
         oz::oz_tengy_kernel<256><<<(unsigned)items, 256, oz::TSMEM_BYTES, (cudaStream_t)stream>>>(P, np, npos);

@@ -673,7 +673,7 @@ static int emulated_batches(trpdrv_plan *p, const trpdrv_dev_system *d, const sy
         LAUNCH_TRY(trpdrv_launch_oz_gemm(d, &b->oz, b->oz_maps, pos, n, fb, p->d_status, p->nsm, st));
         CUDA_TRY(cudaEventRecord(p->ev_gemm[h], st));
         CUDA_TRY(cudaStreamWaitEvent(p->aux_stream, p->ev_gemm[h], 0));
-        LAUNCH_TRY(trpdrv_launch_oz_tengy(d, pos, n, fb, 128, p->aux_stream));
+        LAUNCH_TRY(trpdrv_launch_oz_tengy(d, pos, n, fb, 128, p->d_status, p->aux_stream));
         CUDA_TRY(cudaEventRecord(p->ev_tengy[h], p->aux_stream));
         ++*bi;
         if (launches) *launches += 2;

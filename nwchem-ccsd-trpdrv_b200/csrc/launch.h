@@ -108,9 +108,11 @@ int trpdrv_launch_oz_slices(const trpdrv_dev_system *h_sys, const trpdrv_oz_syst
 int trpdrv_launch_oz_gemm(const trpdrv_dev_system *h_sys, const trpdrv_oz_system *oz, const void *maps,
                           int64_t pos0, int npos, double *fbuf, int *status, int grid, void *stream);
 /* threads: 256 to run alone, 128 to run beside the contraction kernel (emulated plans overlap the
- * energies of one batch with the next batch's products on a second stream). */
+ * energies of one batch with the next batch's products on a second stream).  Even nvir: the tiles
+ * arrive by TMA (fbuf 16-byte aligned), with a bounded wait that sets *status bit 1 when it runs out;
+ * odd nvir (or TRPDRV_OZ_TENGY_TMA=0): cp.async copies. */
 int trpdrv_launch_oz_tengy(const trpdrv_dev_system *h_sys, int64_t pos0, int npos, const double *fbuf,
-                           int threads, void *stream);
+                           int threads, int *status, void *stream);
 int trpdrv_oz_init(void);
 
 /* Per-triple sum of the per-item energies of one system (partial -> rec). */

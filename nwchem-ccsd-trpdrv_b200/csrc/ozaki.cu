@@ -540,78 +540,108 @@ __global__ void __launch_bounds__(256) oz_slice_kernel(const SliceParams P)
 // ------------------------------------------------------------------------------------------------
 constexpr int TW = 16;
 constexpr size_t TSMEM_BYTES = (size_t)16 * TW * (TW + 1) * sizeof(double);
+// TMA form (even nvir): the eight f tiles of one orientation arrive as one 16 x 16 x 8 box with the
+// 128-byte swizzle; both orientations take 32 KB on a 1024-byte boundary.
+constexpr int TBOX = TW * TW * 8;  // doubles of one orientation
+constexpr size_t TSMEM_TMA_BYTES = (size_t)2 * TBOX * sizeof(double) + 1024;
 // 256 threads when the kernel runs alone; 128 (at most 96 registers) to run beside the persistent
-// contraction kernel on the same SMs: 128 x 96 registers and 35 KB of shared memory fit in what an
+// contraction kernel on the same SMs: 128 x 96 registers and 33-35 KB of shared memory fit in what an
 // oz_gemm_kernel CTA leaves free on its SM.
 
 struct TengyParams {
+    CUtensorMap fmap;  // TMA form: fbuf as {nvir rows (contiguous), nvir columns, 8 * npos planes}
     trpdrv_dev_system sys;
     long long pos0;
     const double *fbuf;
+    int *status;  // bit 1: a wait for the tiles ran out (the item's energies are not written)
 };
 
-// One work item = (16-wide tile pair, batch position); CTA b takes items b, b + grid, ... (the
-// launches use one CTA per item).
-template <int TNTHREAD>
-__device__ __forceinline__ void tengy_item(const TengyParams &P, int np, int pairi, int y, double *park, double *red)
-{
-    constexpr int TP = TW + 1, TILE = TW * TP;
-    const trpdrv_dev_system &S = P.sys;
-    const int nvir = S.nvir, tid = threadIdx.x;
-    const int nb = (nvir + TW - 1) / TW;
-    const long long pos = P.pos0 + y;  // a position over the records ([a][triple])
-    if (pos >= S.ntriples || S.nt <= 0) return;
-    const unsigned ai = pos >= S.nt ? (unsigned)pos / (unsigned)S.nt : 0u;  // records < 2^31
-    const long long tpos = pos - (long long)ai * S.nt;
-    const long long tt = S.order ? (long long)S.order[tpos] : tpos;
-    if (tt < 0 || tt >= S.nt) return;
-    const int packed = S.triples[tt];
-    const int i = packed & 1023, j = (packed >> 10) & 1023, k = (packed >> 20) & 1023;
+struct TengyItem {
+    int i, j, k, pairi, y, b0, c0;
+    bool diag;
+    unsigned ai;
+    long long tt;
+};
 
+// Work item = (16-wide tile pair, batch position); false for positions past the end of the system.
+__device__ __forceinline__ bool tengy_decode(const TengyParams &P, int np, int pairi, int y, TengyItem &it)
+{
+    const trpdrv_dev_system &S = P.sys;
+    const long long pos = P.pos0 + y;  // a position over the records ([a][triple])
+    if (pos >= S.ntriples || S.nt <= 0) return false;
+    it.ai = pos >= S.nt ? (unsigned)pos / (unsigned)S.nt : 0u;  // records < 2^31
+    const long long tpos = pos - (long long)it.ai * S.nt;
+    it.tt = S.order ? (long long)S.order[tpos] : tpos;
+    if (it.tt < 0 || it.tt >= S.nt) return false;
+    const int packed = S.triples[it.tt];
+    it.i = packed & 1023;
+    it.j = (packed >> 10) & 1023;
+    it.k = (packed >> 20) & 1023;
+    const int nb = (S.nvir + TW - 1) / TW;
     int B = 0, rem = pairi;
     while (B < nb && rem >= nb - B) {
         rem -= nb - B;
         ++B;
     }
-    const int Cb = B + rem;
-    const int b0 = B * TW, c0 = Cb * TW;
-    const bool diag = (B == Cb);
-    const size_t lnvv = (size_t)nvir * nvir;
-    const double *f = P.fbuf + (size_t)y * 8 * lnvv;
+    it.pairi = pairi;
+    it.y = y;
+    it.b0 = B * TW;
+    it.c0 = (B + rem) * TW;
+    it.diag = rem == 0;
+    return true;
+}
 
-    // park f(B,C) (o = 0) and f(C,B) (o = 1) tiles of all eight f; column q of a tile is contiguous in f.
-    // Every copy of a thread is issued before any is waited for (cp.async, zero fill outside nvir), so
-    // that a CTA keeps its whole 32 KB in flight instead of one load per thread.
-    const int ntiles = diag ? 8 : 16;
-    for (int idx = tid; idx < ntiles * TW * TW; idx += TNTHREAD) {
+// cp.async form: park f(B,C) (o = 0) and f(C,B) (o = 1) tiles of all eight f, W x (W + 1) doubles
+// each; column q of a tile is contiguous in f.  Every copy of a thread is issued before any is
+// waited for (zero fill outside nvir), so that a CTA keeps its whole 32 KB in flight.
+template <int TNTHREAD>
+__device__ __forceinline__ void tengy_park_cpasync(const TengyParams &P, const TengyItem &it, double *park)
+{
+    constexpr int TP = TW + 1, TILE = TW * TP;
+    const int nvir = P.sys.nvir;
+    const size_t lnvv = (size_t)nvir * nvir;
+    const double *f = P.fbuf + (size_t)it.y * 8 * lnvv;
+    const int ntiles = it.diag ? 8 : 16;
+    for (int idx = threadIdx.x; idx < ntiles * TW * TW; idx += TNTHREAD) {
         const int tile = idx / (TW * TW), q = (idx / TW) % TW, r = idx % TW;
         const int o = tile >> 3, xf = tile & 7;
-        const int row = (o ? c0 : b0) + r, col = (o ? b0 : c0) + q;
+        const int row = (o ? it.c0 : it.b0) + r, col = (o ? it.b0 : it.c0) + q;
         const bool ok = row < nvir && col < nvir;
         cp_async_8(park + tile * TILE + r * TP + q, ok ? f + (size_t)xf * lnvv + row + (size_t)col * nvir : f, ok);
     }
     cp_async_commit();
     cp_async_wait<0>();
     __syncthreads();
+}
 
+// Energies of one item from its parked tiles (either layout), summed over the CTA into its slot.
+template <int TNTHREAD, bool TMA>
+__device__ __forceinline__ void tengy_finish(const TengyParams &P, const TengyItem &it, const double *park, double *red)
+{
+    const trpdrv_dev_system &S = P.sys;
+    const int nvir = S.nvir, tid = threadIdx.x;
     TengyVecs v;
     v.eorb = S.eorb;
-    const size_t ao = (size_t)ai * S.nocc;  // the a block of the a-dependent vectors
-    v.dintc1 = S.dintc + (ao + i) * nvir;
-    v.dintx1 = S.dintx + (ao + i) * nvir;
-    v.t1v1 = S.t1v + (ao + i) * nvir;
-    v.dintc2 = S.dintc + (ao + k) * nvir;
-    v.dintx2 = S.dintx + (ao + k) * nvir;
-    v.t1v2 = S.t1v + (ao + k) * nvir;
+    const size_t ao = (size_t)it.ai * S.nocc;  // the a block of the a-dependent vectors
+    v.dintc1 = S.dintc + (ao + it.i) * nvir;
+    v.dintx1 = S.dintx + (ao + it.i) * nvir;
+    v.t1v1 = S.t1v + (ao + it.i) * nvir;
+    v.dintc2 = S.dintc + (ao + it.k) * nvir;
+    v.dintx2 = S.dintx + (ao + it.k) * nvir;
+    v.t1v2 = S.t1v + (ao + it.k) * nvir;
     v.voff = S.ncor + S.nocc;
     v.nvir = nvir;
     // omp/ccsd_trpdrv_omp_cbody.c:126 (a is 1-based, i/j/k here 0-based)
-    v.eaijk = S.eorb[S.a - 1 + ai] - (S.eorb[S.ncor + i] + S.eorb[S.ncor + j] + S.eorb[S.ncor + k]);
+    v.eaijk = S.eorb[S.a - 1 + it.ai] - (S.eorb[S.ncor + it.i] + S.eorb[S.ncor + it.j] + S.eorb[S.ncor + it.k]);
     TengySums su = {0.0, 0.0, 0.0, 0.0};
-    tengy_tile_pair_w<TW>(park, b0, c0, diag, v, tid, TNTHREAD, su);
+    if (TMA)
+        tengy_tile_pair_swz16<TNTHREAD>(park, it.b0, it.c0, it.diag, v, tid, su);
+    else
+        tengy_tile_pair_factored<TW>(park, it.b0, it.c0, it.diag, v, tid, TNTHREAD, su);
     const TengySums tot = block_sum4(su, red);
     if (tid == 0) {  // block_sum4's result is valid in thread 0
-        double *out = S.partial + ((size_t)((long long)ai * S.nt + tt) * S.npairs * TRPDRV_FUSED_SLOTS + pairi) * 4;
+        double *out =
+            S.partial + ((size_t)((long long)it.ai * S.nt + it.tt) * S.npairs * TRPDRV_FUSED_SLOTS + it.pairi) * 4;
         out[0] = tot.e4i;
         out[1] = tot.e5i;
         out[2] = tot.e4k;
@@ -620,15 +650,44 @@ __device__ __forceinline__ void tengy_item(const TengyParams &P, int np, int pai
     __syncthreads();  // the park and the reduction scratch are reused by the CTA's next item
 }
 
-template <int TNTHREAD>
+// CTA b takes items b, b + grid, ... (the launches use one CTA per item).
+template <int TNTHREAD, bool TMA>
 __global__ void __launch_bounds__(TNTHREAD, TNTHREAD == 128 ? 5 : 1)
-oz_tengy_kernel(const TengyParams P, int np, int npos)
+oz_tengy_kernel(const __grid_constant__ TengyParams P, int np, int npos)
 {
-    extern __shared__ __align__(16) double park[];
+    extern __shared__ __align__(16) double tsmem[];
     __shared__ double red[4 * (TNTHREAD / 32)];
+    __shared__ __align__(8) unsigned long long tbar[1];
+    double *park = TMA ? reinterpret_cast<double *>((reinterpret_cast<uintptr_t>(tsmem) + 1023) & ~(uintptr_t)1023)
+                       : tsmem;
+    if (TMA) {
+        if (threadIdx.x == 0) {
+            mbar_init(tbar, 1);
+            asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        }
+        __syncthreads();
+    }
+    unsigned phase = 0;
     const long long items = (long long)np * npos;
-    for (long long w = blockIdx.x; w < items; w += gridDim.x)
-        tengy_item<TNTHREAD>(P, np, (int)(w % np), (int)(w / np), park, red);
+    for (long long w = blockIdx.x; w < items; w += gridDim.x) {
+        TengyItem it;
+        if (!tengy_decode(P, np, (int)(w % np), (int)(w / np), it)) continue;  // uniform over the CTA
+        if (TMA) {
+            if (threadIdx.x == 0) {
+                // the previous item's reads of the park (generic proxy) precede these writes
+                asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+                mbar_arrive_expect_tx(tbar, (it.diag ? 1u : 2u) * (unsigned)(TBOX * sizeof(double)));
+                tma_load_3d(park, &P.fmap, tbar, it.b0, it.c0, it.y * 8);
+                if (!it.diag) tma_load_3d(park + TBOX, &P.fmap, tbar, it.c0, it.b0, it.y * 8);
+            }
+            const bool ok = mbar_wait(tbar, phase, P.status);
+            phase ^= 1;
+            if (__syncthreads_or(!ok)) return;  // status bit 1 is set
+        } else {
+            tengy_park_cpasync<TNTHREAD>(P, it, park);
+        }
+        tengy_finish<TNTHREAD, TMA>(P, it, park, red);
+    }
 }
 
 // number of 16-wide tile pairs (must fit in the npairs * TRPDRV_FUSED_SLOTS slots of a triple)
@@ -668,6 +727,34 @@ static int make_map_i8(CUtensorMap *m, const signed char *base, unsigned long lo
                           estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_64B,
                           CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     return r == CUDA_SUCCESS ? 0 : 2;
+}
+
+// 3-D map over the f of a batch for the TMA form of the energies: dims {nvir rows (contiguous), nvir
+// columns, planes}, box {16, 16, 8} (the eight f of one triple), 128-byte swizzle, zero fill past nvir.
+// Needs even nvir (row pitch a multiple of 16 bytes) and a 16-byte aligned base.
+static int make_map_f64(CUtensorMap *m, const double *base, int nvir, unsigned long long planes)
+{
+    PFN_cuTensorMapEncodeTiled_v12000 fn = encode_fn();
+    if (!fn || nvir < 2 || (nvir & 1) || (reinterpret_cast<uintptr_t>(base) & 15)) return 1;
+    const cuuint64_t dims[3] = {(cuuint64_t)nvir, (cuuint64_t)nvir, planes};
+    const cuuint64_t strides[2] = {(cuuint64_t)nvir * sizeof(double), (cuuint64_t)nvir * nvir * sizeof(double)};
+    const cuuint32_t box[3] = {(cuuint32_t)TW, (cuuint32_t)TW, 8};
+    const cuuint32_t estr[3] = {1, 1, 1};
+    const CUresult r = fn(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3, const_cast<double *>(base), dims, strides, box, estr,
+                          CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                          CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    return r == CUDA_SUCCESS ? 0 : 2;
+}
+
+// TRPDRV_OZ_TENGY_TMA=0 keeps the cp.async form of the energies for every nvir.
+static bool tengy_tma_enabled()
+{
+    static int on = -1;
+    if (on < 0) {
+        const char *e = getenv("TRPDRV_OZ_TENGY_TMA");
+        on = (e && e[0] == '0') ? 0 : 1;
+    }
+    return on != 0;
 }
 
 template <int S>
@@ -768,27 +855,33 @@ extern "C" int trpdrv_launch_oz_gemm(const trpdrv_dev_system *h_sys, const trpdr
 }
 
 extern "C" int trpdrv_launch_oz_tengy(const trpdrv_dev_system *h_sys, int64_t pos0, int npos, const double *fbuf,
-                                      int threads, void *stream)
+                                      int threads, int *status, void *stream)
 {
     if (npos <= 0) return 0;
     const int np = oz::tengy_pairs(h_sys->nvir);
     if (np > h_sys->npairs * TRPDRV_FUSED_SLOTS) return (int)cudaErrorInvalidValue;
+    if (threads != 128 && threads != 256) return (int)cudaErrorInvalidValue;
+    const long long items = (long long)np * npos;
+    if (items > 0x7fffffffLL) return (int)cudaErrorInvalidValue;
     oz::TengyParams P;
+    memset(&P, 0, sizeof(P));
     P.sys = *h_sys;
     P.pos0 = pos0;
     P.fbuf = fbuf;
-    const long long items = (long long)np * npos;
-    if (items > 0x7fffffffLL) return (int)cudaErrorInvalidValue;
+    P.status = status;
+    const bool tma = oz::tengy_tma_enabled() && oz::make_map_f64(&P.fmap, fbuf, h_sys->nvir, 8ull * npos) == 0;
     // one CTA per item: a launch of one CTA per SM beside the contraction kernel (each CTA looping
     // over many items) was measured 30 % slower overall, too little memory parallelism per SM
-    if (threads == 128) {
-        oz::oz_tengy_kernel<128><<<(unsigned)items, 128, oz::TSMEM_BYTES, (cudaStream_t)stream>>>(P, np, npos);
-    } else if (threads == 256) {
-        if (items > 0x7fffffffLL) return (int)cudaErrorInvalidValue;
-        oz::oz_tengy_kernel<256><<<(unsigned)items, 256, oz::TSMEM_BYTES, (cudaStream_t)stream>>>(P, np, npos);
-    } else {
-        return (int)cudaErrorInvalidValue;
-    }
+    cudaStream_t st = (cudaStream_t)stream;
+    const unsigned grid = (unsigned)items;
+    if (tma && threads == 128)
+        oz::oz_tengy_kernel<128, true><<<grid, 128, oz::TSMEM_TMA_BYTES, st>>>(P, np, npos);
+    else if (tma)
+        oz::oz_tengy_kernel<256, true><<<grid, 256, oz::TSMEM_TMA_BYTES, st>>>(P, np, npos);
+    else if (threads == 128)
+        oz::oz_tengy_kernel<128, false><<<grid, 128, oz::TSMEM_BYTES, st>>>(P, np, npos);
+    else
+        oz::oz_tengy_kernel<256, false><<<grid, 256, oz::TSMEM_BYTES, st>>>(P, np, npos);
     return (int)cudaGetLastError();
 }
 
@@ -800,9 +893,9 @@ extern "C" int trpdrv_oz_init(void)
     if ((e = oz::set_attr<6>()) != 0) return e;
     if ((e = oz::set_attr<7>()) != 0) return e;
     if ((e = oz::set_attr<8>()) != 0) return e;
-    if ((e = (int)cudaFuncSetAttribute(oz::oz_tengy_kernel<128>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       (int)oz::TSMEM_BYTES)) != 0)
-        return e;
-    return (int)cudaFuncSetAttribute(oz::oz_tengy_kernel<256>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     (int)oz::TSMEM_BYTES);
+    const cudaFuncAttribute dyn = cudaFuncAttributeMaxDynamicSharedMemorySize;
+    if ((e = (int)cudaFuncSetAttribute(oz::oz_tengy_kernel<128, false>, dyn, (int)oz::TSMEM_BYTES)) != 0) return e;
+    if ((e = (int)cudaFuncSetAttribute(oz::oz_tengy_kernel<256, false>, dyn, (int)oz::TSMEM_BYTES)) != 0) return e;
+    if ((e = (int)cudaFuncSetAttribute(oz::oz_tengy_kernel<128, true>, dyn, (int)oz::TSMEM_TMA_BYTES)) != 0) return e;
+    return (int)cudaFuncSetAttribute(oz::oz_tengy_kernel<256, true>, dyn, (int)oz::TSMEM_TMA_BYTES);
 }

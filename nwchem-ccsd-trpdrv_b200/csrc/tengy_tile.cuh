@@ -48,6 +48,73 @@ __device__ __forceinline__ void tengy_tile_pair_w(const double *park, int b0, in
     }
 }
 
+// The same sums with one thread per (b, c) of B x C: the 16 values at (b, c) and (c, b) are loaded
+// once, the denominator (equal for both) is formed once, and the factored forms give the terms of
+// (b, c) and, off the diagonal, of (c, b).  Equal to tengy_tile_pair_w up to reassociation.
+template <int W>
+__device__ __forceinline__ void tengy_tile_pair_factored(const double *park, int b0, int c0, bool diag,
+                                                         const TengyVecs &v, int tid, int nthreads, TengySums &su)
+{
+    constexpr int P = W + 1, TILE = W * P;
+    for (int idx = tid; idx < W * W; idx += nthreads) {
+        const int r = idx / W, q = idx % W;
+        const int b = b0 + r, c = c0 + q;
+        if (b < v.nvir && c < v.nvir) {
+            const double *bcT = park + r * P + q;                          // f_x(B + r, C + q)
+            const double *cbT = park + (diag ? 0 : 8) * TILE + q * P + r;  // f_x(C + q, B + r)
+            double fbc[8], fcb[8];
+#pragma unroll
+            for (int f = 0; f < 8; ++f) {
+                fbc[f] = bcT[f * TILE];
+                fcb[f] = cbT[f * TILE];
+            }
+            const double denom = -1.0 / (__ldg(v.eorb + v.voff + b) + __ldg(v.eorb + v.voff + c) + v.eaijk);
+            tengy_term_factored(fbc, fcb, denom, __ldg(v.t1v1 + b), __ldg(v.t1v2 + b), __ldg(v.dintx1 + c),
+                                __ldg(v.dintx2 + c), __ldg(v.dintc1 + c), __ldg(v.dintc2 + c), su);
+            if (!diag)
+                tengy_term_factored(fcb, fbc, denom, __ldg(v.t1v1 + c), __ldg(v.t1v2 + c), __ldg(v.dintx1 + b),
+                                    __ldg(v.dintx2 + b), __ldg(v.dintc1 + b), __ldg(v.dintc2 + b), su);
+        }
+    }
+}
+
+// Element x of the 16-double row `col` in a box landed with the 128-byte swizzle: the 16-byte chunk
+// index is XORed with col mod 8 (rows are 128 bytes, the box starts on a 1024-byte boundary).
+__device__ __forceinline__ int swz128(int x, int col) { return (((x >> 1) ^ (col & 7)) << 1) | (x & 1); }
+
+// The same sums over 16-wide tiles as TMA lands them: the (B, C) box, then off the diagonal the
+// (C, B) box, each 8 planes (one per f) of 16 columns x 16 rows, row index contiguous and swizzled
+// by swz128.  Each half-warp walks one diagonal q = (r + d) mod 16: both the (b, c) reads (row r of
+// column q) and the (c, b) reads (row q of column r) then hit 16 different 8-byte bank pairs.
+template <int NTHREAD>
+__device__ __forceinline__ void tengy_tile_pair_swz16(const double *park, int b0, int c0, bool diag,
+                                                      const TengyVecs &v, int tid, TengySums &su)
+{
+    constexpr int PLANE = 16 * 16, BOX = 8 * PLANE;
+    static_assert(NTHREAD % 16 == 0 && NTHREAD <= 256, "half-warps walk the 16 diagonals");
+    const int r = tid & 15;
+    for (int d = tid >> 4; d < 16; d += NTHREAD / 16) {
+        const int q = (r + d) & 15;
+        const int b = b0 + r, c = c0 + q;
+        if (b < v.nvir && c < v.nvir) {
+            const double *bcT = park + q * 16 + swz128(r, q);                       // f_x(B + r, C + q)
+            const double *cbT = park + (diag ? 0 : BOX) + r * 16 + swz128(q, r);    // f_x(C + q, B + r)
+            double fbc[8], fcb[8];
+#pragma unroll
+            for (int f = 0; f < 8; ++f) {
+                fbc[f] = bcT[f * PLANE];
+                fcb[f] = cbT[f * PLANE];
+            }
+            const double denom = -1.0 / (__ldg(v.eorb + v.voff + b) + __ldg(v.eorb + v.voff + c) + v.eaijk);
+            tengy_term_factored(fbc, fcb, denom, __ldg(v.t1v1 + b), __ldg(v.t1v2 + b), __ldg(v.dintx1 + c),
+                                __ldg(v.dintx2 + c), __ldg(v.dintc1 + c), __ldg(v.dintc2 + c), su);
+            if (!diag)
+                tengy_term_factored(fcb, fbc, denom, __ldg(v.t1v1 + c), __ldg(v.t1v2 + c), __ldg(v.dintx1 + b),
+                                    __ldg(v.dintx2 + b), __ldg(v.dintc1 + b), __ldg(v.dintc2 + b), su);
+        }
+    }
+}
+
 __device__ __forceinline__ void tengy_tile_pair(const double *park, int b0, int c0, bool diag,
                                                 const TengyVecs &v, int tid, int nthreads, TengySums &su)
 {

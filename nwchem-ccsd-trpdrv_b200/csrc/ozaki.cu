@@ -164,13 +164,36 @@ __device__ __forceinline__ unsigned long long sdesc_sw64(const void *p)
            (1ull << 46) | (4ull << 61);
 }
 
-__device__ __forceinline__ void mma_i8(unsigned d, unsigned long long a, unsigned long long b, int accumulate)
+// A-operand collector buffer use of one MMA: the first MMA of a run that shares its A tile fills the
+// buffer, the following ones read A from it instead of shared memory, the last one releases it.
+enum { COL_DISCARD = 0, COL_FILL = 1, COL_USE = 2, COL_LASTUSE = 3 };
+#ifndef OZ_COLLECTOR
+#define OZ_COLLECTOR 1
+#endif
+
+__device__ __forceinline__ void mma_i8(unsigned d, unsigned long long a, unsigned long long b, int accumulate,
+                                       int col = COL_DISCARD)
 {
-    asm volatile(
-        "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
-        " tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n}\n" ::"r"(d),
-        "l"(a), "l"(b), "r"(IDESC), "r"(accumulate), "r"(0), "r"(0), "r"(0), "r"(0)
-        : "memory");
+#define OZ_MMA_I8(Q)                                                                                          \
+    asm volatile("{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"                                                 \
+                 " tcgen05.mma.cta_group::1.kind::i8" Q " [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n}\n" ::"r"(d), \
+                 "l"(a), "l"(b), "r"(IDESC), "r"(accumulate), "r"(0), "r"(0), "r"(0), "r"(0)                 \
+                 : "memory")
+    if (col == COL_FILL)
+        OZ_MMA_I8(".collector::a::fill");
+    else if (col == COL_USE)
+        OZ_MMA_I8(".collector::a::use");
+    else if (col == COL_LASTUSE)
+        OZ_MMA_I8(".collector::a::lastuse");
+    else
+        OZ_MMA_I8("");
+#undef OZ_MMA_I8
+}
+
+// collector use of the q-th of n MMAs in a row that share one A tile
+__host__ __device__ constexpr int collector_op(int q, int n)
+{
+    return n == 1 ? COL_DISCARD : q == 0 ? COL_FILL : q == n - 1 ? COL_LASTUSE : COL_USE;
 }
 
 __device__ __forceinline__ void mma_commit(unsigned long long *bar)
@@ -338,11 +361,11 @@ __global__ void __launch_bounds__(NTHREAD, 1) oz_gemm_kernel(const __grid_consta
 #pragma unroll
                                 for (int p = 0; p < S; ++p)
 #pragma unroll
-                                    for (int q = 0; p + q < S; ++q)
+                                    for (int q = 0; p + q < S; ++q)  // S - p MMAs share A slice p
                                         mma_i8(tmem + (unsigned)((p + q) * BN),
                                                dA + (unsigned long long)(p * (SLICE_A >> 4) + ks * (KSTEP >> 4)),
                                                dB + (unsigned long long)(q * (SLICE_B >> 4) + ks * (KSTEP >> 4)),
-                                               (kg > 0 || p > 0) ? 1 : 0);
+                                               (kg > 0 || p > 0) ? 1 : 0, OZ_COLLECTOR ? collector_op(q, S - p) : COL_DISCARD);
                             }
                         }
                         mma_commit(&empty[stage]);  // the stage is free once these MMAs have read it

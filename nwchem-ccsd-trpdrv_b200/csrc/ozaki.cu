@@ -127,6 +127,32 @@ __device__ __forceinline__ bool mbar_wait(unsigned long long *b, unsigned parity
     }
 }
 
+// L2 cache policies for loads and stores: evict_last for data read again soon (the digit planes, reused
+// across the tiles and triples that share them), evict_first for data read once
+__device__ __forceinline__ unsigned long long policy_evict_last()
+{
+    unsigned long long pol;
+    asm volatile("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(pol));
+    return pol;
+}
+
+__device__ __forceinline__ unsigned long long policy_evict_first()
+{
+    unsigned long long pol;
+    asm volatile("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(pol));
+    return pol;
+}
+
+__device__ __forceinline__ void tma_load_3d_hint(void *dst, const CUtensorMap *map, unsigned long long *bar, int x,
+                                                 int y, int z, unsigned long long pol)
+{
+    asm volatile(
+        "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes.L2::cache_hint [%0], [%1, {%3, "
+        "%4, %5}], [%2], %6;" ::"r"(saddr(dst)),
+        "l"(map), "r"(saddr(bar)), "r"(x), "r"(y), "r"(z), "l"(pol)
+        : "memory");
+}
+
 __device__ __forceinline__ void tma_load_3d(void *dst, const CUtensorMap *map, unsigned long long *bar, int x, int y,
                                             int z)
 {
@@ -169,6 +195,15 @@ __device__ __forceinline__ unsigned long long sdesc_sw64(const void *p)
 enum { COL_DISCARD = 0, COL_FILL = 1, COL_USE = 2, COL_LASTUSE = 3 };
 #ifndef OZ_COLLECTOR
 #define OZ_COLLECTOR 1
+#endif
+#ifndef OZ_F_STREAMING
+#define OZ_F_STREAMING 1
+#endif
+#ifndef OZ_DIGIT_EVICT_LAST
+#define OZ_DIGIT_EVICT_LAST 1
+#endif
+#ifndef OZ_F_LOAD_EVICT_FIRST
+#define OZ_F_LOAD_EVICT_FIRST 1
 #endif
 
 __device__ __forceinline__ void mma_i8(unsigned d, unsigned long long a, unsigned long long b, int accumulate,
@@ -304,6 +339,7 @@ __global__ void __launch_bounds__(NTHREAD, 1) oz_gemm_kernel(const __grid_consta
 
     if (warp == 0) {
         if (lane == 0) {  // TMA producer: runs ahead across tiles, bounded by the stage ring
+            const unsigned long long pol = policy_evict_last();
             int stage = 0;
             unsigned phase = 0;
             bool alive = true;
@@ -322,10 +358,16 @@ __global__ void __launch_bounds__(NTHREAD, 1) oz_gemm_kernel(const __grid_consta
                     char *sA = stages + (size_t)stage * C::STAGE, *sB = sA + S * SLICE_A;
 #pragma unroll
                     for (int p = 0; p < S; ++p)
-                        tma_load_3d(sA + p * SLICE_A, &P.mapA, &full[stage], kc * KC, d.m0, d.planeA * S + p);
+                        if (OZ_DIGIT_EVICT_LAST)
+                            tma_load_3d_hint(sA + p * SLICE_A, &P.mapA, &full[stage], kc * KC, d.m0, d.planeA * S + p, pol);
+                        else
+                            tma_load_3d(sA + p * SLICE_A, &P.mapA, &full[stage], kc * KC, d.m0, d.planeA * S + p);
 #pragma unroll
                     for (int q = 0; q < S; ++q)
-                        tma_load_3d(sB + q * SLICE_B, &P.mapB, &full[stage], kc * KC, d.n0, d.planeB * S + q);
+                        if (OZ_DIGIT_EVICT_LAST)
+                            tma_load_3d_hint(sB + q * SLICE_B, &P.mapB, &full[stage], kc * KC, d.n0, d.planeB * S + q, pol);
+                        else
+                            tma_load_3d(sB + q * SLICE_B, &P.mapB, &full[stage], kc * KC, d.n0, d.planeB * S + q);
                     if (++stage == C::STAGES) {
                         stage = 0;
                         phase ^= 1;
@@ -437,7 +479,13 @@ __global__ void __launch_bounds__(NTHREAD, 1) oz_gemm_kernel(const __grid_consta
                     const int col = d.n0 + half * WC + c;
                     if (col < 2 * V) {
                         const int ch = col >= V ? 1 : 0, cc = col - ch * V;
-                        fj[(size_t)(rh + 2 * ch) * vv + b + (size_t)cc * V] = acc[c] * sa * __ldg(eb + col);
+                    {
+                        double *dst = fj + (size_t)(rh + 2 * ch) * vv + b + (size_t)cc * V;
+                        if (OZ_F_STREAMING)
+                            __stcs(dst, acc[c] * sa * __ldg(eb + col));  // evict-first: keeps the digits in L2
+                        else
+                            *dst = acc[c] * sa * __ldg(eb + col);
+                    }
                     }
                 }
             }
@@ -700,8 +748,14 @@ oz_tengy_kernel(const __grid_constant__ TengyParams P, int np, int npos)
                 // the previous item's reads of the park (generic proxy) precede these writes
                 asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
                 mbar_arrive_expect_tx(tbar, (it.diag ? 1u : 2u) * (unsigned)(TBOX * sizeof(double)));
-                tma_load_3d(park, &P.fmap, tbar, it.b0, it.c0, it.y * 8);
-                if (!it.diag) tma_load_3d(park + TBOX, &P.fmap, tbar, it.c0, it.b0, it.y * 8);
+                if (OZ_F_LOAD_EVICT_FIRST) {
+                    const unsigned long long pol = policy_evict_first();
+                    tma_load_3d_hint(park, &P.fmap, tbar, it.b0, it.c0, it.y * 8, pol);
+                    if (!it.diag) tma_load_3d_hint(park + TBOX, &P.fmap, tbar, it.c0, it.b0, it.y * 8, pol);
+                } else {
+                    tma_load_3d(park, &P.fmap, tbar, it.b0, it.c0, it.y * 8);
+                    if (!it.diag) tma_load_3d(park + TBOX, &P.fmap, tbar, it.c0, it.b0, it.y * 8);
+                }
             }
             const bool ok = mbar_wait(tbar, phase, P.status);
             phase ^= 1;

@@ -657,20 +657,43 @@ static int enqueue_fused(trpdrv_plan *p, cudaStream_t st, int capturing)
     return TRPDRV_OK;
 }
 
-/* Emulated form, positions [pos0, pos1) of one system in batches of `batch`: each batch's contraction
- * launch writes its f into one half of d_fbuf, and its energies run on the auxiliary stream (128-thread
- * CTAs beside the next batch's contraction kernel on the same SMs) while the next batch's products go
- * to the other half.  *bi counts batches over a whole execution (it picks the half); a half is reused
- * only after the energies that read it.  Finish with emulated_join. */
+/* Emulated form, positions [pos0, pos1) of one system in batches of `batch`; *bi counts batches over a
+ * whole execution (it picks the half of d_fbuf a batch's f goes to).  Default: each batch's contraction
+ * launch writes its f into one half, and its energies run on the auxiliary stream (128-thread CTAs)
+ * while the next batch's products go to the other half; a half is reused only after the energies that
+ * read it.  TRPDRV_OZ_FUSED_ENERGY=1 (even nvir): each contraction launch's energy warps compute the
+ * energies of the previous batch, from the half the previous launch (on the same stream) filled, and
+ * an energies-only launch closes the system.  Finish with emulated_join. */
 static int emulated_batches(trpdrv_plan *p, const trpdrv_dev_system *d, const sysbuf *b, int64_t pos0, int64_t pos1,
                             int batch, cudaStream_t st, int64_t *bi, int64_t *launches)
 {
+    if (trpdrv_oz_fused_energy_supported(d->nvir)) {
+        int64_t epos = 0;
+        int en = 0;
+        const double *efb = NULL;
+        for (int64_t pos = pos0;; pos += batch) {
+            const int n = pos < pos1 ? (int)(pos1 - pos < batch ? pos1 - pos : batch) : 0;
+            if (n == 0 && en == 0) break;
+            const int h = (int)(*bi & 1);
+            double *fb = p->d_fbuf + (size_t)h * p->fbuf_half;
+            if (n > 0 && *bi >= 2) CUDA_TRY(cudaStreamWaitEvent(st, p->ev_tengy[h], 0));  /* separate-launch readers */
+            LAUNCH_TRY(trpdrv_launch_oz_gemm(d, &b->oz, b->oz_maps, pos, n, fb, epos, en, efb, p->d_status, p->nsm,
+                                             st));
+            if (launches) *launches += 1;
+            if (n == 0) break;
+            epos = pos;
+            en = n;
+            efb = fb;
+            ++*bi;
+        }
+        return TRPDRV_OK;
+    }
     for (int64_t pos = pos0; pos < pos1; pos += batch) {
         const int n = (int)(pos1 - pos < batch ? pos1 - pos : batch);
         const int h = (int)(*bi & 1);
         double *fb = p->d_fbuf + (size_t)h * p->fbuf_half;
         if (*bi >= 2) CUDA_TRY(cudaStreamWaitEvent(st, p->ev_tengy[h], 0));
-        LAUNCH_TRY(trpdrv_launch_oz_gemm(d, &b->oz, b->oz_maps, pos, n, fb, p->d_status, p->nsm, st));
+        LAUNCH_TRY(trpdrv_launch_oz_gemm(d, &b->oz, b->oz_maps, pos, n, fb, 0, 0, NULL, p->d_status, p->nsm, st));
         CUDA_TRY(cudaEventRecord(p->ev_gemm[h], st));
         CUDA_TRY(cudaStreamWaitEvent(p->aux_stream, p->ev_gemm[h], 0));
         LAUNCH_TRY(trpdrv_launch_oz_tengy(d, pos, n, fb, 128, p->d_status, p->aux_stream));

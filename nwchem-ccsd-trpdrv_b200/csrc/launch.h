@@ -105,8 +105,14 @@ int trpdrv_oz_dp(int nocc, int nvir);
 size_t trpdrv_oz_maps_bytes(void);
 int trpdrv_oz_prepare(const trpdrv_oz_system *oz, void *maps_out);
 int trpdrv_launch_oz_slices(const trpdrv_dev_system *h_sys, const trpdrv_oz_system *oz, void *stream);
+/* Products of positions pos0 .. pos0 + npos - 1 into fbuf; enpos > 0 (requires
+ * trpdrv_oz_fused_energy_supported(nvir)): the same launch's energy warps also compute the energies
+ * of positions epos0 .. epos0 + enpos - 1, whose f an earlier launch stored at efbuf.  npos = 0 gives an
+ * energies-only launch. */
 int trpdrv_launch_oz_gemm(const trpdrv_dev_system *h_sys, const trpdrv_oz_system *oz, const void *maps,
-                          int64_t pos0, int npos, double *fbuf, int *status, int grid, void *stream);
+                          int64_t pos0, int npos, double *fbuf, int64_t epos0, int enpos, const double *efbuf,
+                          int *status, int grid, void *stream);
+int trpdrv_oz_fused_energy_supported(int nvir);
 /* threads: 256 to run alone, 128 to run beside the contraction kernel (emulated plans overlap the
  * energies of one batch with the next batch's products on a second stream).  Even nvir: the tiles
  * arrive by TMA (fbuf 16-byte aligned), with a bounded wait that sets *status bit 1 when it runs out;

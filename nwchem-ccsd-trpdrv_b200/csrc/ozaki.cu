@@ -46,18 +46,29 @@ constexpr int BN = 64;          // output columns per tile (TMEM columns per lev
 constexpr int KC = 64;          // contraction bytes (= int8 indices) per stage
 constexpr int KSTEP = 32;       // contraction indices per MMA
 constexpr int NREC = 8;         // recombination warps: two per TMEM lane quadrant, 32 columns each
-constexpr int NTHREAD = 32 * (2 + NREC);  // warp 0 TMA, warp 1 MMA + TMEM, warps 2.. recombination
+constexpr int NENG = 4;         // energy warps (energies fused into the launch)
+// Warpgroup 0: warp 0 TMA, warp 1 MMA + TMEM (warps 2, 3 idle); warpgroups 1, 2 (warps 4 .. 11)
+// recombination; warpgroup 3 (warps 12 .. 15) energies.
+constexpr int REC0 = 4, ENG0 = REC0 + NREC;
+constexpr int NTHREAD = 32 * (ENG0 + NENG);
+// Register split by setmaxnreg: launched at 65536 / 512 = 128 per thread, the recombination
+// warpgroups rise to 168 (their drain spills below that), the others drop.
+constexpr int REG_LAUNCH = 128, REG_CTRL = 72, REG_REC = 168, REG_ENG = 104;
+static_assert(128 * REG_CTRL + 256 * REG_REC + 128 * REG_ENG <= NTHREAD * REG_LAUNCH, "register split exceeds the launch");
 constexpr unsigned SLICE_A = BM * KC;
 constexpr unsigned SLICE_B = BN * KC;
 constexpr int SMEM_AVAIL = 227 * 1024 - 2048;
 constexpr unsigned long long WAIT_LIMIT_NS = 4000000000ull;
 
+// fused energies: the f tiles of one tile pair (both orientations, 8 planes of 16 x 16 doubles each)
+constexpr unsigned PARK_BYTES = 2u * 8u * 16u * 16u * 8u;
+
 template <int S>
 struct Cfg {
     static constexpr unsigned STAGE = S * (SLICE_A + SLICE_B);
-    static constexpr int FIT = SMEM_AVAIL / (int)STAGE;
+    static constexpr int FIT = (SMEM_AVAIL - (int)PARK_BYTES) / (int)STAGE;
     static constexpr int STAGES = FIT > 4 ? 4 : FIT;
-    static constexpr size_t SMEM = (size_t)STAGES * STAGE + 1024;
+    static constexpr size_t SMEM = (size_t)STAGES * STAGE + PARK_BYTES + 1024;  // stages, then the park
     static constexpr unsigned TMEM_COLS = S * BN <= 256 ? 256u : 512u;
     static_assert(STAGES >= 2, "fewer than two stages fit");
     static_assert(S * BN <= 512, "level accumulators exceed tensor memory");
@@ -70,10 +81,16 @@ constexpr unsigned IDESC = (2u << 4) | (1u << 7) | (1u << 10) | ((unsigned)(BN >
 
 struct GemmParams {
     CUtensorMap mapA, mapB;  // 64-byte aligned members first
+    CUtensorMap fmap;        // fused energies: efbuf as {V rows (contiguous), V columns, 8 * enpos planes}
+    trpdrv_dev_system sys;   // fused energies: vectors, triples and energy slots of the system
     const double *ea, *eb;   // power-of-two scales per A row / B column
     const int32_t *triples, *order;
     long long pos0, ntriples, nt;  // ntriples records = n_a * nt triples per a
     double *fbuf;            // [batch][8][V][V]
+    // fused energies: the energies of positions epos0 .. epos0 + enpos - 1, whose f an earlier launch
+    // stored (at the fmap's base); unit u = tile pair u % np of position epos0 + u / np
+    long long epos0;
+    int enpos, np;
     int V, O, nks, mtiles, ntiles, tiles;  // tiles = 2 * npos * mtiles * ntiles
     int *status;
 };
@@ -274,6 +291,166 @@ __device__ __forceinline__ double level_weight(int L)
 }
 
 // ------------------------------------------------------------------------------------------------
+constexpr int TW = 16;
+constexpr size_t TSMEM_BYTES = (size_t)16 * TW * (TW + 1) * sizeof(double);
+// TMA form (even nvir): the eight f tiles of one orientation arrive as one 16 x 16 x 8 box with the
+// 128-byte swizzle; both orientations take 32 KB on a 1024-byte boundary.
+constexpr int TBOX = TW * TW * 8;  // doubles of one orientation
+constexpr size_t TSMEM_TMA_BYTES = (size_t)2 * TBOX * sizeof(double) + 1024;
+// 256 threads when the kernel runs alone; 128 (at most 96 registers) to run beside the persistent
+// contraction kernel on the same SMs: 128 x 96 registers and 33-35 KB of shared memory fit in what an
+// oz_gemm_kernel CTA leaves free on its SM.
+
+
+struct TengyItem {
+    int i, j, k, pairi, y, b0, c0;
+    bool diag;
+    unsigned ai;
+    long long tt;
+};
+
+// Work item = (16-wide tile pair, batch position y after pos0); false for positions past the end of
+// the system.
+__device__ __forceinline__ bool tengy_decode(const trpdrv_dev_system &S, long long pos0, int pairi, int y,
+                                             TengyItem &it)
+{
+    const long long pos = pos0 + y;  // a position over the records ([a][triple])
+    if (pos >= S.ntriples || S.nt <= 0) return false;
+    it.ai = pos >= S.nt ? (unsigned)pos / (unsigned)S.nt : 0u;  // records < 2^31
+    const long long tpos = pos - (long long)it.ai * S.nt;
+    it.tt = S.order ? (long long)S.order[tpos] : tpos;
+    if (it.tt < 0 || it.tt >= S.nt) return false;
+    const int packed = S.triples[it.tt];
+    it.i = packed & 1023;
+    it.j = (packed >> 10) & 1023;
+    it.k = (packed >> 20) & 1023;
+    const int nb = (S.nvir + TW - 1) / TW;
+    int B = 0, rem = pairi;
+    while (B < nb && rem >= nb - B) {
+        rem -= nb - B;
+        ++B;
+    }
+    it.pairi = pairi;
+    it.y = y;
+    it.b0 = B * TW;
+    it.c0 = (B + rem) * TW;
+    it.diag = rem == 0;
+    return true;
+}
+
+// The vectors and eaijk of an item's triple.
+__device__ __forceinline__ TengyVecs tengy_vecs(const trpdrv_dev_system &S, const TengyItem &it)
+{
+    const int nvir = S.nvir;
+    TengyVecs v;
+    v.eorb = S.eorb;
+    const size_t ao = (size_t)it.ai * S.nocc;  // the a block of the a-dependent vectors
+    v.dintc1 = S.dintc + (ao + it.i) * nvir;
+    v.dintx1 = S.dintx + (ao + it.i) * nvir;
+    v.t1v1 = S.t1v + (ao + it.i) * nvir;
+    v.dintc2 = S.dintc + (ao + it.k) * nvir;
+    v.dintx2 = S.dintx + (ao + it.k) * nvir;
+    v.t1v2 = S.t1v + (ao + it.k) * nvir;
+    v.voff = S.ncor + S.nocc;
+    v.nvir = nvir;
+    // omp/ccsd_trpdrv_omp_cbody.c:126 (a is 1-based, i/j/k here 0-based)
+    v.eaijk = S.eorb[S.a - 1 + it.ai] - (S.eorb[S.ncor + it.i] + S.eorb[S.ncor + it.j] + S.eorb[S.ncor + it.k]);
+    return v;
+}
+
+// The item's four energy slots (e4i, e5i, e4k, e5k).
+__device__ __forceinline__ double *tengy_slot(const trpdrv_dev_system &S, const TengyItem &it)
+{
+    return S.partial + ((size_t)((long long)it.ai * S.nt + it.tt) * S.npairs * TRPDRV_FUSED_SLOTS + it.pairi) * 4;
+}
+
+// number of 16-wide tile pairs (must fit in the npairs * TRPDRV_FUSED_SLOTS slots of a triple)
+__host__ __device__ inline int tengy_pairs(int nvir)
+{
+    const int nb = (nvir + TW - 1) / TW;
+    return nb * (nb + 1) / 2;
+}
+
+
+// ------------------------------------------------------------------------------------------------
+// energies fused into the contraction kernel: once every tile of a position has stored its f, the
+// recombination warps of any CTA take that position's tile pairs (units) in order and compute their
+// energies from f that is still in L2, in the time the next tile's products run on the tensor cores
+// ------------------------------------------------------------------------------------------------
+constexpr int NENG_THREADS = 32 * NENG;
+
+// named barrier 1 over the energy warps (barrier 0 is the CTA's)
+__device__ __forceinline__ void eng_bar() { asm volatile("bar.sync 1, %0;" ::"n"(NENG_THREADS) : "memory"); }
+
+// the energy barrier, true in every thread when p is true in any
+__device__ __forceinline__ bool eng_bar_or(bool p)
+{
+    unsigned r;
+    asm volatile("{\n .reg .pred a, b;\n setp.ne.u32 a, %1, 0;\n bar.red.or.pred b, 1, %2, a;\n selp.u32 %0, 1, 0, b;\n}\n"
+                 : "=r"(r)
+                 : "r"((unsigned)p), "n"(NENG_THREADS)
+                 : "memory");
+    return r != 0;
+}
+
+// One unit's energies, by the energy threads (te = 0 .. NENG_THREADS - 1); false if the wait for its
+// tiles ran out (status bit 1 set).
+__device__ __forceinline__ bool fused_unit(const GemmParams &P, int u, double *park, unsigned long long *ubar,
+                                           unsigned &uphase, double *red, int te)
+{
+    TengyItem it;
+    if (!tengy_decode(P.sys, P.epos0, u % P.np, u / P.np, it)) return true;  // same outcome in every thread
+    if (te == 0) {
+        // this park's previous reads (generic proxy) before the tensor-copy writes
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        mbar_arrive_expect_tx(ubar, (it.diag ? 1u : 2u) * (PARK_BYTES / 2u));
+        const unsigned long long pol = policy_evict_first();
+        tma_load_3d_hint(park, &P.fmap, ubar, it.b0, it.c0, it.y * 8, pol);
+        if (!it.diag) tma_load_3d_hint(park + PARK_BYTES / 16u, &P.fmap, ubar, it.c0, it.b0, it.y * 8, pol);
+    }
+    const bool ok = mbar_wait(ubar, uphase, P.status);
+    uphase ^= 1u;
+    if (eng_bar_or(!ok)) return false;
+    const TengyVecs v = tengy_vecs(P.sys, it);
+    TengySums su = {0.0, 0.0, 0.0, 0.0};
+    tengy_tile_pair_swz16<NENG_THREADS>(park, it.b0, it.c0, it.diag, v, te, su);
+    su.e4i = warp_sum(su.e4i);
+    su.e5i = warp_sum(su.e5i);
+    su.e4k = warp_sum(su.e4k);
+    su.e5k = warp_sum(su.e5k);
+    const int we = te >> 5;
+    if ((te & 31) == 0) {
+        red[4 * we + 0] = su.e4i;
+        red[4 * we + 1] = su.e5i;
+        red[4 * we + 2] = su.e4k;
+        red[4 * we + 3] = su.e5k;
+    }
+    eng_bar();  // also: every read of the park is done before the next unit's copies
+    if (te == 0) {
+        double t[4] = {0.0, 0.0, 0.0, 0.0};
+        for (int w = 0; w < NENG; ++w)  // fixed order: the sums do not depend on which CTA ran the unit
+            for (int e = 0; e < 4; ++e) t[e] += red[4 * w + e];
+        double *out = tengy_slot(P.sys, it);
+        out[0] = t[0];
+        out[1] = t[1];
+        out[2] = t[2];
+        out[3] = t[3];
+    }
+    return true;
+}
+
+// The energy warps' loop: CTA b takes units b, b + grid, ... of the positions whose f an earlier
+// launch stored, while this launch's tiles run on the tensor cores.
+__device__ __forceinline__ void fused_energies(const GemmParams &P, double *park, unsigned long long *ubar,
+                                               double *red, int te)
+{
+    const unsigned total = (unsigned)P.enpos * (unsigned)P.np;
+    unsigned uphase = 0;
+    for (unsigned u = blockIdx.x; u < total; u += gridDim.x)
+        if (!fused_unit(P, (int)u, park, ubar, uphase, red, te)) return;
+}
+
+// ------------------------------------------------------------------------------------------------
 // contraction kernel (persistent: CTA b takes tiles b, b + grid, ...)
 // ------------------------------------------------------------------------------------------------
 struct Tile {
@@ -311,9 +488,11 @@ __global__ void __launch_bounds__(NTHREAD, 1) oz_gemm_kernel(const __grid_consta
 {
     using C = Cfg<S>;
     extern __shared__ char smem_raw[];
-    __shared__ __align__(8) unsigned long long full[C::STAGES], empty[C::STAGES], tfull[1], tempty[1], done[1];
+    __shared__ __align__(8) unsigned long long full[C::STAGES], empty[C::STAGES], tfull[1], tempty[1], done[1], ubar[1];
     __shared__ unsigned tmem_sh;
+    __shared__ double red[4 * NENG];
     char *stages = reinterpret_cast<char *>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~(uintptr_t)1023);
+    double *park = reinterpret_cast<double *>(stages + (size_t)C::STAGES * C::STAGE);  // 1024-byte aligned
 
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int nchunks = (P.nks * KSTEP + KC - 1) / KC;
@@ -326,6 +505,7 @@ __global__ void __launch_bounds__(NTHREAD, 1) oz_gemm_kernel(const __grid_consta
         mbar_init(tfull, 1);
         mbar_init(tempty, NREC);  // one arrival per recombination warp
         mbar_init(done, 1);
+        mbar_init(ubar, 1);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     if (warp == 1) {
@@ -337,7 +517,10 @@ __global__ void __launch_bounds__(NTHREAD, 1) oz_gemm_kernel(const __grid_consta
     tc_fence_after();
     const unsigned tmem = tmem_sh;
 
-    if (warp == 0) {
+    // each role's code sits in the branch of its warpgroup's register change
+    if (warp < REC0) {
+      asm volatile("setmaxnreg.dec.sync.aligned.u32 %0;" ::"n"(REG_CTRL));
+      if (warp == 0) {
         if (lane == 0) {  // TMA producer: runs ahead across tiles, bounded by the stage ring
             const unsigned long long pol = policy_evict_last();
             int stage = 0;
@@ -419,12 +602,16 @@ __global__ void __launch_bounds__(NTHREAD, 1) oz_gemm_kernel(const __grid_consta
                 }
                 mma_commit(tfull);  // this tile's sums are complete (or the tile was skipped)
             }
-            mma_commit(done);  // every MMA issued by this thread has completed when `done` flips
-            mbar_wait(done, 0, P.status);
+            if (it > 0) {  // a CTA with no tiles (an energies-only launch) issued nothing to wait for
+                mma_commit(done);  // every MMA issued by this thread has completed when `done` flips
+                mbar_wait(done, 0, P.status);
+            }
         }
         __syncwarp();
-    } else {  // recombination: this warp reads TMEM lanes 32*(warp%4).., columns 32*half..
-        const int qd = warp & 3, half = (warp - 2) >> 2;
+      }
+    } else if (warp < ENG0) {  // recombination: TMEM lanes 32*(warp%4).., columns 32*half..
+        asm volatile("setmaxnreg.inc.sync.aligned.u32 %0;" ::"n"(REG_REC));
+        const int qd = warp & 3, half = (warp - REC0) >> 2;
         constexpr int WC = BN / 2;  // columns per recombination warp
         const int V = P.V;
         const size_t vv = (size_t)V * V;
@@ -479,17 +666,20 @@ __global__ void __launch_bounds__(NTHREAD, 1) oz_gemm_kernel(const __grid_consta
                     const int col = d.n0 + half * WC + c;
                     if (col < 2 * V) {
                         const int ch = col >= V ? 1 : 0, cc = col - ch * V;
-                    {
                         double *dst = fj + (size_t)(rh + 2 * ch) * vv + b + (size_t)cc * V;
+                        const double val = acc[c] * sa * __ldg(eb + col);
+                        // evict-first: read once, by a later launch; keeps the digits in L2
                         if (OZ_F_STREAMING)
-                            __stcs(dst, acc[c] * sa * __ldg(eb + col));  // evict-first: keeps the digits in L2
+                            __stcs(dst, val);
                         else
-                            *dst = acc[c] * sa * __ldg(eb + col);
-                    }
+                            *dst = val;
                     }
                 }
             }
         }
+    } else {  // energy warps: the units of the positions an earlier launch stored
+        asm volatile("setmaxnreg.dec.sync.aligned.u32 %0;" ::"n"(REG_ENG));
+        if (P.enpos > 0) fused_energies(P, park, ubar, red, tid - 32 * ENG0);
     }
     tc_fence_before();
     __syncthreads();
@@ -608,17 +798,6 @@ __global__ void __launch_bounds__(256) oz_slice_kernel(const SliceParams P)
 // SM.  A CTA's four sums go to its own slot of the triple's items (slot index = tile-pair index; the
 // 16-wide pairs fit in the 8 slots of each 32-wide item, and the slots no CTA writes are zero from
 // plan creation), so item_reduce sums them in a fixed order.
-// ------------------------------------------------------------------------------------------------
-constexpr int TW = 16;
-constexpr size_t TSMEM_BYTES = (size_t)16 * TW * (TW + 1) * sizeof(double);
-// TMA form (even nvir): the eight f tiles of one orientation arrive as one 16 x 16 x 8 box with the
-// 128-byte swizzle; both orientations take 32 KB on a 1024-byte boundary.
-constexpr int TBOX = TW * TW * 8;  // doubles of one orientation
-constexpr size_t TSMEM_TMA_BYTES = (size_t)2 * TBOX * sizeof(double) + 1024;
-// 256 threads when the kernel runs alone; 128 (at most 96 registers) to run beside the persistent
-// contraction kernel on the same SMs: 128 x 96 registers and 33-35 KB of shared memory fit in what an
-// oz_gemm_kernel CTA leaves free on its SM.
-
 struct TengyParams {
     CUtensorMap fmap;  // TMA form: fbuf as {nvir rows (contiguous), nvir columns, 8 * npos planes}
     trpdrv_dev_system sys;
@@ -626,41 +805,6 @@ struct TengyParams {
     const double *fbuf;
     int *status;  // bit 1: a wait for the tiles ran out (the item's energies are not written)
 };
-
-struct TengyItem {
-    int i, j, k, pairi, y, b0, c0;
-    bool diag;
-    unsigned ai;
-    long long tt;
-};
-
-// Work item = (16-wide tile pair, batch position); false for positions past the end of the system.
-__device__ __forceinline__ bool tengy_decode(const TengyParams &P, int np, int pairi, int y, TengyItem &it)
-{
-    const trpdrv_dev_system &S = P.sys;
-    const long long pos = P.pos0 + y;  // a position over the records ([a][triple])
-    if (pos >= S.ntriples || S.nt <= 0) return false;
-    it.ai = pos >= S.nt ? (unsigned)pos / (unsigned)S.nt : 0u;  // records < 2^31
-    const long long tpos = pos - (long long)it.ai * S.nt;
-    it.tt = S.order ? (long long)S.order[tpos] : tpos;
-    if (it.tt < 0 || it.tt >= S.nt) return false;
-    const int packed = S.triples[it.tt];
-    it.i = packed & 1023;
-    it.j = (packed >> 10) & 1023;
-    it.k = (packed >> 20) & 1023;
-    const int nb = (S.nvir + TW - 1) / TW;
-    int B = 0, rem = pairi;
-    while (B < nb && rem >= nb - B) {
-        rem -= nb - B;
-        ++B;
-    }
-    it.pairi = pairi;
-    it.y = y;
-    it.b0 = B * TW;
-    it.c0 = (B + rem) * TW;
-    it.diag = rem == 0;
-    return true;
-}
 
 // cp.async form: park f(B,C) (o = 0) and f(C,B) (o = 1) tiles of all eight f, W x (W + 1) doubles
 // each; column q of a tile is contiguous in f.  Every copy of a thread is issued before any is
@@ -689,21 +833,8 @@ __device__ __forceinline__ void tengy_park_cpasync(const TengyParams &P, const T
 template <int TNTHREAD, bool TMA>
 __device__ __forceinline__ void tengy_finish(const TengyParams &P, const TengyItem &it, const double *park, double *red)
 {
-    const trpdrv_dev_system &S = P.sys;
-    const int nvir = S.nvir, tid = threadIdx.x;
-    TengyVecs v;
-    v.eorb = S.eorb;
-    const size_t ao = (size_t)it.ai * S.nocc;  // the a block of the a-dependent vectors
-    v.dintc1 = S.dintc + (ao + it.i) * nvir;
-    v.dintx1 = S.dintx + (ao + it.i) * nvir;
-    v.t1v1 = S.t1v + (ao + it.i) * nvir;
-    v.dintc2 = S.dintc + (ao + it.k) * nvir;
-    v.dintx2 = S.dintx + (ao + it.k) * nvir;
-    v.t1v2 = S.t1v + (ao + it.k) * nvir;
-    v.voff = S.ncor + S.nocc;
-    v.nvir = nvir;
-    // omp/ccsd_trpdrv_omp_cbody.c:126 (a is 1-based, i/j/k here 0-based)
-    v.eaijk = S.eorb[S.a - 1 + it.ai] - (S.eorb[S.ncor + it.i] + S.eorb[S.ncor + it.j] + S.eorb[S.ncor + it.k]);
+    const int tid = threadIdx.x;
+    const TengyVecs v = tengy_vecs(P.sys, it);
     TengySums su = {0.0, 0.0, 0.0, 0.0};
     if (TMA)
         tengy_tile_pair_swz16<TNTHREAD>(park, it.b0, it.c0, it.diag, v, tid, su);
@@ -711,8 +842,7 @@ __device__ __forceinline__ void tengy_finish(const TengyParams &P, const TengyIt
         tengy_tile_pair_factored<TW>(park, it.b0, it.c0, it.diag, v, tid, TNTHREAD, su);
     const TengySums tot = block_sum4(su, red);
     if (tid == 0) {  // block_sum4's result is valid in thread 0
-        double *out =
-            S.partial + ((size_t)((long long)it.ai * S.nt + it.tt) * S.npairs * TRPDRV_FUSED_SLOTS + it.pairi) * 4;
+        double *out = tengy_slot(P.sys, it);
         out[0] = tot.e4i;
         out[1] = tot.e5i;
         out[2] = tot.e4k;
@@ -742,7 +872,7 @@ oz_tengy_kernel(const __grid_constant__ TengyParams P, int np, int npos)
     const long long items = (long long)np * npos;
     for (long long w = blockIdx.x; w < items; w += gridDim.x) {
         TengyItem it;
-        if (!tengy_decode(P, np, (int)(w % np), (int)(w / np), it)) continue;  // uniform over the CTA
+        if (!tengy_decode(P.sys, P.pos0, (int)(w % np), (int)(w / np), it)) continue;  // uniform over the CTA
         if (TMA) {
             if (threadIdx.x == 0) {
                 // the previous item's reads of the park (generic proxy) precede these writes
@@ -767,12 +897,6 @@ oz_tengy_kernel(const __grid_constant__ TengyParams P, int np, int npos)
     }
 }
 
-// number of 16-wide tile pairs (must fit in the npairs * TRPDRV_FUSED_SLOTS slots of a triple)
-static int tengy_pairs(int nvir)
-{
-    const int nb = (nvir + TW - 1) / TW;
-    return nb * (nb + 1) / 2;
-}
 
 // ------------------------------------------------------------------------------------------------
 // host side
@@ -853,9 +977,25 @@ static int launch_gemm(const GemmParams &P, dim3 grid, cudaStream_t st)
 
 using namespace trpdrv;
 
+// Registers per thread the contraction kernels are launched with (read back at init): the setmaxnreg
+// split is valid only when every instantiation has exactly REG_LAUNCH.
+static int g_oz_launch_regs = 0;
+
 extern "C" int trpdrv_oz_slices_supported(int slices) { return slices >= TRPDRV_OZ_MIN_SLICES && slices <= TRPDRV_OZ_MAX_SLICES; }
 
 extern "C" int trpdrv_oz_dp(int nocc, int nvir) { return ((nvir + nocc) + 31) / 32 * 32; }
+
+// Energies inside the contraction launch (TRPDRV_OZ_FUSED_ENERGY=1, read at each call): computed by
+// the kernel's energy warps from f still in L2; needs even nvir (the f tiles are read by TMA).  The
+// default is the separate energy launch, measured 4 % (7 slices) to 14 % (5 slices) faster at
+// (40, 300): the energy work costs the same SM issue and FP64 time either way, and inside the
+// contraction kernel it also slows the MMA warp's issue.
+extern "C" int trpdrv_oz_fused_energy_supported(int nvir)
+{
+    const char *e = getenv("TRPDRV_OZ_FUSED_ENERGY");
+    const int on = e && e[0] == '1';
+    return on && nvir >= 2 && (nvir & 1) == 0 && oz::tengy_tma_enabled();
+}
 
 extern "C" size_t trpdrv_oz_maps_bytes(void) { return 2 * sizeof(CUtensorMap); }
 
@@ -897,10 +1037,22 @@ extern "C" int trpdrv_launch_oz_slices(const trpdrv_dev_system *h_sys, const trp
 }
 
 extern "C" int trpdrv_launch_oz_gemm(const trpdrv_dev_system *h_sys, const trpdrv_oz_system *oz, const void *maps,
-                                     int64_t pos0, int npos, double *fbuf, int *status, int grid, void *stream)
+                                     int64_t pos0, int npos, double *fbuf, int64_t epos0, int enpos,
+                                     const double *efbuf, int *status, int grid, void *stream)
 {
-    if (npos <= 0) return 0;
+    if (npos < 0 || enpos < 0 || (npos == 0 && enpos == 0)) return 0;
     oz::GemmParams P;
+    memset(&P, 0, sizeof(P));
+    if (enpos > 0) {  // energies of an earlier launch's positions, fused into this one
+        if (!trpdrv_oz_fused_energy_supported(h_sys->nvir)) return (int)cudaErrorInvalidValue;
+        P.np = oz::tengy_pairs(h_sys->nvir);
+        if (P.np > h_sys->npairs * TRPDRV_FUSED_SLOTS) return (int)cudaErrorInvalidValue;
+        if ((long long)P.np * enpos > 0x7fffffffLL) return (int)cudaErrorInvalidValue;
+        if (oz::make_map_f64(&P.fmap, efbuf, h_sys->nvir, 8ull * enpos) != 0) return (int)cudaErrorInvalidValue;
+        P.sys = *h_sys;
+        P.epos0 = epos0;
+        P.enpos = enpos;
+    }
     memcpy(&P.mapA, maps, sizeof(CUtensorMap));
     memcpy(&P.mapB, static_cast<const char *>(maps) + sizeof(CUtensorMap), sizeof(CUtensorMap));
     P.ea = oz->ea;
@@ -918,9 +1070,11 @@ extern "C" int trpdrv_launch_oz_gemm(const trpdrv_dev_system *h_sys, const trpdr
     P.ntiles = (2 * oz->nvir + oz::BN - 1) / oz::BN;
     P.tiles = 2 * npos * P.mtiles * P.ntiles;
     P.status = status;
+    const long long work = P.tiles > 0 ? P.tiles : (long long)P.np * enpos;  // an energies-only launch
     if (grid < 1) grid = 1;
-    if (grid > P.tiles) grid = P.tiles;
+    if (grid > work) grid = (int)work;
     cudaStream_t st = (cudaStream_t)stream;
+    if (g_oz_launch_regs != oz::REG_LAUNCH) return (int)cudaErrorInvalidConfiguration;  // split unusable
     switch (oz->slices) {
     case 4: return oz::launch_gemm<4>(P, dim3((unsigned)grid), st);
     case 5: return oz::launch_gemm<5>(P, dim3((unsigned)grid), st);
@@ -962,9 +1116,23 @@ extern "C" int trpdrv_launch_oz_tengy(const trpdrv_dev_system *h_sys, int64_t po
     return (int)cudaGetLastError();
 }
 
+template <int S>
+static int oz_regs(int *all_equal)
+{
+    cudaFuncAttributes a;
+    const cudaError_t e = cudaFuncGetAttributes(&a, oz::oz_gemm_kernel<S>);
+    if (e != cudaSuccess) return (int)e;
+    if (a.numRegs != oz::REG_LAUNCH) *all_equal = 0;
+    return 0;
+}
+
 extern "C" int trpdrv_oz_init(void)
 {
-    int e;
+    int e, regs_ok = 1;
+    if ((e = oz_regs<4>(&regs_ok)) != 0 || (e = oz_regs<5>(&regs_ok)) != 0 || (e = oz_regs<6>(&regs_ok)) != 0 ||
+        (e = oz_regs<7>(&regs_ok)) != 0 || (e = oz_regs<8>(&regs_ok)) != 0)
+        return e;
+    g_oz_launch_regs = regs_ok ? oz::REG_LAUNCH : 0;
     if ((e = oz::set_attr<4>()) != 0) return e;
     if ((e = oz::set_attr<5>()) != 0) return e;
     if ((e = oz::set_attr<6>()) != 0) return e;

@@ -90,10 +90,12 @@ template <int NTHREAD>
 __device__ __forceinline__ void tengy_tile_pair_swz16(const double *park, int b0, int c0, bool diag,
                                                       const TengyVecs &v, int tid, TengySums &su)
 {
-    constexpr int PLANE = 16 * 16, BOX = 8 * PLANE;
-    static_assert(NTHREAD % 16 == 0 && NTHREAD <= 256, "half-warps walk the 16 diagonals");
+    constexpr int PLANE = 16 * 16, BOX = 8 * PLANE, NDIAG = 16 / (NTHREAD / 16);
+    static_assert(NTHREAD % 16 == 0 && NTHREAD <= 256 && 16 % (NTHREAD / 16) == 0, "half-warps walk the 16 diagonals");
     const int r = tid & 15;
-    for (int d = tid >> 4; d < 16; d += NTHREAD / 16) {
+#pragma unroll
+    for (int k = 0; k < NDIAG; ++k) {  // a fixed trip count: the loads of every diagonal issue together
+        const int d = (tid >> 4) + k * (NTHREAD / 16);
         const int q = (r + d) & 15;
         const int b = b0 + r, c = c0 + q;
         if (b < v.nvir && c < v.nvir) {

@@ -108,3 +108,59 @@ def test_target_digits_picks_the_fewest_slices_that_meet_it(T, name, digits):
         ref = np.asarray(g["records"])
         dev = np.max(np.abs(recs[0] - ref)) / np.max(np.abs(ref))
         assert dev > 10.0 ** -(digits + 2)
+
+
+# ------------------------------------------------------------------------------------------------
+# Energies fused into the contraction launch (TRPDRV_OZ_FUSED_ENERGY=1, even nvir): the kernel's energy
+# warps compute each tile pair once every tile of its triple has stored its f.  They walk the same
+# 128-thread diagonals and sum the warps in the same order as the separate energy launch; the two
+# kernels may still contract multiplies and adds into FMAs differently, so the records agree to a
+# few units in the last place (SAME_PATH_RTOL), not bitwise.
+# ------------------------------------------------------------------------------------------------
+SAME_PATH_RTOL = 1e-13
+def _even_goldens():
+    return [n for n in golden_cases() if load_golden(n)["nvir"] % 2 == 0]
+
+
+@pytest.fixture
+def fused_energy(monkeypatch):
+    monkeypatch.setenv("TRPDRV_OZ_FUSED_ENERGY", "1")
+    yield
+    monkeypatch.delenv("TRPDRV_OZ_FUSED_ENERGY")
+
+
+@pytest.mark.parametrize("name", _even_goldens())
+def test_fused_energies_match_reference_golden_and_separate_launch(T, monkeypatch, name):
+    g = load_golden(name)
+    s = system_from_golden(g)
+    e4, e5, recs, launches = _run(T, [s], nkpass=g["nkpass"], slices=7)
+    monkeypatch.setenv("TRPDRV_OZ_FUSED_ENERGY", "1")
+    e4f, e5f, recf, launches_f = _run(T, [s], nkpass=g["nkpass"], slices=7)
+    monkeypatch.delenv("TRPDRV_OZ_FUSED_ENERGY")
+    assert launches_f < launches  # no separate energy launches
+    assert_records_close(recf[0], recs[0], rtol=SAME_PATH_RTOL)
+    assert_total_close(e4f[0], e4[0], rtol=SAME_PATH_RTOL, what="emp4 vs separate launch")
+    assert_total_close(e5f[0], e5[0], rtol=SAME_PATH_RTOL, what="emp5 vs separate launch")
+    assert_records_close(recf[0], g["records"])
+    assert_total_close(e4f[0], g["emp4"], what="emp4")
+    assert_total_close(e5f[0], g["emp5"], what="emp5")
+
+
+def test_fused_energies_batches_and_shards_recombine(T, fused_energy):
+    s = T.synth_system(7, 64, seed=45)
+    rec = _run(T, [s], slices=7, batch=5)[2][0]
+    assert np.array_equal(_run(T, [s], slices=7, batch=64)[2][0], rec)
+    parts = [_run(T, [s], slices=7, rank=r, world=3)[2][0] for r in range(3)]
+    assert np.array_equal(np.concatenate(parts), rec)
+
+
+def test_fused_energies_leave_odd_nvir_on_the_separate_launch(T, monkeypatch):
+    """Odd nvir (the f rows are not 16-byte multiples for TMA): the switch falls back to the
+    separate energy launch and the energies are unchanged."""
+    s = T.synth_system(5, 37, seed=49, ncor=1)
+    base = _run(T, [s], slices=7)
+    monkeypatch.setenv("TRPDRV_OZ_FUSED_ENERGY", "1")
+    fused = _run(T, [s], slices=7)
+    monkeypatch.delenv("TRPDRV_OZ_FUSED_ENERGY")
+    assert fused[3] == base[3]
+    assert np.array_equal(fused[2][0], base[2][0])

@@ -79,6 +79,21 @@ def test_c2_emulated_matches_the_reference(T, slices):
     _check(g, e4[0], e5[0], recs[0], what=f"c2 emulated {slices}")
 
 
+def test_c2_emulated_with_fused_energies_equals_the_separate_launch(T, monkeypatch):
+    """TRPDRV_OZ_FUSED_ENERGY=1: the energies inside the contraction launch agree with the separate
+    launch's to 1e-13 (the kernels may contract multiplies and adds differently) and with the
+    reference at the usual bars."""
+    g = _load("big_c2_o40_v300")["systems"][0]
+    s = _system(T, g)
+    e4, e5, recs, _ = _run(T, [s], mode=T.MODE_EMULATED, slices=7)
+    monkeypatch.setenv("TRPDRV_OZ_FUSED_ENERGY", "1")
+    e4f, e5f, recf, _ = _run(T, [s], mode=T.MODE_EMULATED, slices=7)
+    assert_records_close(np.asarray(recf[0]), np.asarray(recs[0]), rtol=1e-13)
+    assert_total_close(e4f[0], e4[0], rtol=1e-13, what="emp4 vs separate launch")
+    assert_total_close(e5f[0], e5[0], rtol=1e-13, what="emp5 vs separate launch")
+    _check(g, e4f[0], e5f[0], recf[0], what="c2 emulated fused energies")
+
+
 @pytest.mark.parametrize("mode", ["fused", "plain"])
 def test_c3_fp64_matches_the_reference_on_every_triple(T, mode):
     g = _load("big_c3_o30_v400_log")["systems"][0]

@@ -80,10 +80,13 @@ struct ItemCtx {
     double eaijk;
     int ncor, nocc, nvir, b0, c0, diag, nV, nch, state;  // state: 1 work, 0 malformed, -1 end
     int packed, b1;      // packed edge item: pairs (b0, c0) and (b1, c0); b1 < 0 when the second is absent
-    int split, ch0, cstep;  // split item: this half runs chunks ch0, ch0 + cstep, ... (cstep 2, else 1)
-    double *scr;         // split item: [2 halves][64][256] partial f / gT of this item
-    unsigned *cnt;       // split item: arrivals of the two halves
+    // split item (the one-triple system of a split launch): 1 | half << 1 | pair << 2, else 0; this half
+    // runs chunks half, half + 2, ...  One int keeps the context at 128 bytes: at 160 bytes (the split
+    // fields as separate members) the batched kernel measured 6 % slower.
+    int split_tag;
 };
+
+static_assert(sizeof(ItemCtx) == 128, "the item context is kept at 128 bytes (see split_tag)");
 
 // Packed edge items (systems with pack_edge: the last column tile E holds 1..16 valid indices).  The
 // pairs (B, E) and (B + 1, E), B even, run as one item: each family of a chunk gets its own stage
@@ -383,6 +386,9 @@ __device__ __forceinline__ void warp_epilogue(const ItemCtx &cx, const double (&
 // ------------------------------------------------------------------------------------------------
 // producer warp: tickets and item contexts (lane 0), TMA loads (one box per lane)
 // ------------------------------------------------------------------------------------------------
+// SPLIT: the instantiation that also runs split systems (two work items per pair); without it the
+// producer and consumer loops carry no split logic at all.
+template <bool SPLIT>
 __device__ __forceinline__ void producer(const trpdrv_dev_system *__restrict__ sys, int nsys, long long total,
                                          unsigned long long *counter, int *status, const Maps &maps, char *stages,
                                          unsigned long long *full, unsigned long long *empty, ItemCtx *ring, int lane)
@@ -414,8 +420,8 @@ __device__ __forceinline__ void producer(const trpdrv_dev_system *__restrict__ s
         while (s + 1 < nsys && item >= sys[s + 1].item_begin) ++s;
         const trpdrv_dev_system &S = sys[s];
         // a split system has two work items (halves of the contraction) per pair
-        const int hpart = S.split ? (int)((item - S.item_begin) & 1) : 0;
-        const long long local = S.split ? (item - S.item_begin) >> 1 : item - S.item_begin;
+        const int hpart = (SPLIT && S.split) ? (int)((item - S.item_begin) & 1) : 0;
+        const long long local = (SPLIT && S.split) ? (item - S.item_begin) >> 1 : item - S.item_begin;
         const long long qpos = local / S.npairs;  // processing position over the system's records
         const int p = (int)(local - qpos * S.npairs);
         // a index (records are [a][triple], fewer than 2^31: the host checks); no division for a single a
@@ -486,12 +492,8 @@ __device__ __forceinline__ void producer(const trpdrv_dev_system *__restrict__ s
             cx.c0 = C0;
             cx.diag = diag;
             cx.nV = nV;
-            cx.split = S.split;
-            cx.ch0 = S.split ? hpart : 0;
-            cx.cstep = S.split ? 2 : 1;
-            cx.nch = S.split ? (nV + nO - hpart + 1) / 2 : nV + nO;
-            cx.scr = S.split ? S.split_scratch + (size_t)own * 2 * 64 * 256 : nullptr;
-            cx.cnt = S.split ? S.split_count + own : nullptr;
+            cx.split_tag = (SPLIT && S.split) ? 1 | hpart << 1 | (int)own << 2 : 0;
+            cx.nch = (SPLIT && S.split) ? (nV + nO - hpart + 1) / 2 : nV + nO;
             cx.state = 1;
         }
 
@@ -519,8 +521,8 @@ __device__ __forceinline__ void producer(const trpdrv_dev_system *__restrict__ s
                 off = (lane < 16 ? PK_B1B + pp : PK_B3B + pp) * PANEL_BYTES + half * KBOX;
             }
             tb = tb >= 0 ? tb * T : -1;
-            const int pch0 = S.split ? hpart : 0, pstep = S.split ? 2 : 1;
-            const int nsl = 2 * (S.split ? (nV + nO - hpart + 1) / 2 : nV + nO);
+            const int pch0 = (SPLIT && S.split) ? hpart : 0, pstep = (SPLIT && S.split) ? 2 : 1;
+            const int nsl = 2 * ((SPLIT && S.split) ? (nV + nO - hpart + 1) / 2 : nV + nO);
             for (int sl = 0; sl < nsl; ++sl) {
                 if (!mbar_wait(&empty[stage], phase ^ 1, status)) return;
                 const int fam = sl & 1, ch = pch0 + (sl >> 1) * pstep;
@@ -576,7 +578,7 @@ __device__ __forceinline__ void producer(const trpdrv_dev_system *__restrict__ s
         const int pnl = fam * 8 + (slot < 2 ? 0 : slot < 4 ? 2 : slot < 6 ? 4 : 6) + o;
         const bool mine = lane < 28 && (!diag || o == 0);
         const unsigned bytes = (diag ? NPANEL / 2 : NPANEL) * PANEL_BYTES;
-        for (int ch = S.split ? hpart : 0; ch < nV + nO; ch += S.split ? 2 : 1) {
+        for (int ch = (SPLIT && S.split) ? hpart : 0; ch < nV + nO; ch += (SPLIT && S.split) ? 2 : 1) {
             if (!mbar_wait(&empty[stage], phase ^ 1, status)) return;
             if (lane == 0) mbar_arrive_expect_tx(&full[stage], bytes);
             __syncwarp();
@@ -612,12 +614,16 @@ __device__ __forceinline__ void producer(const trpdrv_dev_system *__restrict__ s
 // the first stops there.  Two rounds of the consumer barrier order the writes before the count and
 // broadcast its result; the counter is reset by the second arrival.  Nothing waits for the other CTA.
 // Returns false when a barrier wait ran out (status set).
-__device__ __forceinline__ bool split_combine(const ItemCtx &cx, double (&f)[8][4], double (&gT)[8][4], int warp,
-                                              int lane, unsigned long long *xbar, unsigned &xphase, int *flag,
-                                              int *status, int &fin)
+__device__ __forceinline__ bool split_combine(const trpdrv_dev_system *__restrict__ sys, const ItemCtx &cx,
+                                              double (&f)[8][4], double (&gT)[8][4], int warp, int lane,
+                                              unsigned long long *xbar, unsigned &xphase, int *flag, int *status,
+                                              int &fin)
 {
-    const int tc = warp * 32 + lane;
-    double *mine = cx.scr + (size_t)(cx.ch0 ? 64 * 256 : 0) + tc;
+    const int tc = warp * 32 + lane, half = (cx.split_tag >> 1) & 1;
+    const size_t pair = (size_t)(cx.split_tag >> 2);
+    double *const scr = sys[0].split_scratch + pair * 2 * 64 * 256;  // [2 halves][64][256] of this pair
+    unsigned *const cnt = sys[0].split_count + pair;                 // arrivals of the two halves
+    double *mine = scr + (size_t)(half ? 64 * 256 : 0) + tc;
 #pragma unroll
     for (int x = 0; x < 8; ++x)
 #pragma unroll
@@ -630,7 +636,7 @@ __device__ __forceinline__ bool split_combine(const ItemCtx &cx, double (&f)[8][
     if (lane == 0) mbar_arrive(xbar);
     if (!mbar_wait(xbar, xphase, status)) return false;
     xphase ^= 1;
-    if (tc == 0) *flag = (int)atomicAdd(cx.cnt, 1u);
+    if (tc == 0) *flag = (int)atomicAdd(cnt, 1u);
     __syncwarp();
     if (lane == 0) mbar_arrive(xbar);
     if (!mbar_wait(xbar, xphase, status)) return false;
@@ -638,7 +644,7 @@ __device__ __forceinline__ bool split_combine(const ItemCtx &cx, double (&f)[8][
     fin = *flag != 0;
     if (fin) {
         __threadfence();
-        const double *other = cx.scr + (size_t)(cx.ch0 ? 0 : 64 * 256) + tc;
+        const double *other = scr + (size_t)(half ? 0 : 64 * 256) + tc;
 #pragma unroll
         for (int x = 0; x < 8; ++x)
 #pragma unroll
@@ -646,13 +652,13 @@ __device__ __forceinline__ bool split_combine(const ItemCtx &cx, double (&f)[8][
                 f[x][e] += __ldcg(other + (x * 4 + e) * 256);
                 gT[x][e] += __ldcg(other + (32 + x * 4 + e) * 256);
             }
-        if (tc == 0) *cx.cnt = 0u;
+        if (tc == 0) *cnt = 0u;
     }
     return true;
 }
 
 // ------------------------------------------------------------------------------------------------
-template <int KS>
+template <int KS, bool SPLIT>
 __global__ void __launch_bounds__(NTHREAD, 1)
 fused_tma_kernel(const trpdrv_dev_system *__restrict__ sys, int nsys, long long total, unsigned long long *counter,
                  int *status, const __grid_constant__ Maps maps)
@@ -678,7 +684,7 @@ fused_tma_kernel(const trpdrv_dev_system *__restrict__ sys, int nsys, long long 
 
     if (warp >= NCW) {  // producer warpgroup: its first warp issues everything
         asm volatile("setmaxnreg.dec.sync.aligned.u32 %0;" ::"n"(Regs<KS>::PRODUCER));
-        if (warp == NCW) producer(sys, nsys, total, counter, status, maps, stages, full, empty, ring, lane);
+        if (warp == NCW) producer<SPLIT>(sys, nsys, total, counter, status, maps, stages, full, empty, ring, lane);
         return;
     }
     asm volatile("setmaxnreg.inc.sync.aligned.u32 %0;" ::"n"(Regs<KS>::CONSUMER));
@@ -725,7 +731,7 @@ fused_tma_kernel(const trpdrv_dev_system *__restrict__ sys, int nsys, long long 
             for (int sl = 0; sl < nsl; ++sl) {
                 if (sl > 0 && !mbar_wait(&full[stage], phase, status)) return;
                 const char *st = stages + (size_t)stage * STAGE_BYTES;
-                const int ch = cx.ch0 + (sl >> 1) * cx.cstep;
+                const int ch = SPLIT ? ((cx.split_tag >> 1) & 1) + (sl >> 1) * ((cx.split_tag & 1) + 1) : sl >> 1;
                 const bool ph1 = ch >= pnV;
                 const int kval = ph1 ? cx.nocc - (ch - pnV) * DK : cx.nvir - ch * DK;
                 if (pactive) {
@@ -743,9 +749,9 @@ fused_tma_kernel(const trpdrv_dev_system *__restrict__ sys, int nsys, long long 
                     phase ^= 1;
                 }
             }
-            if (cx.split) {
+            if (SPLIT && (cx.split_tag & 1)) {
                 int fin = 0;
-                if (!split_combine(cx, f, gT, warp, lane, xbar, xphase, split_flag, status, fin)) return;
+                if (!split_combine(sys, cx, f, gT, warp, lane, xbar, xphase, split_flag, status, fin)) return;
                 if (!fin) continue;
             }
             if (pb0 >= 0) {  // this pair's slots: the 4 sub-blocks' sums, zeros in the other 4
@@ -763,7 +769,7 @@ fused_tma_kernel(const trpdrv_dev_system *__restrict__ sys, int nsys, long long 
         const bool diag = cx.diag != 0;
         const int pf = nch > 3 ? nch - 3 : 0;
         for (int c = 0; c < nch; ++c) {
-            const int ch = cx.ch0 + c * cx.cstep;
+            const int ch = SPLIT ? ((cx.split_tag >> 1) & 1) + c * ((cx.split_tag & 1) + 1) : c;
             if (c > 0 && !mbar_wait(&full[stage], phase, status)) return;
             const char *st = stages + (size_t)stage * STAGE_BYTES;
             const bool ph1 = ch >= nV;
@@ -853,9 +859,9 @@ fused_tma_kernel(const trpdrv_dev_system *__restrict__ sys, int nsys, long long 
                 phase ^= 1;
             }
         }
-        if (cx.split) {  // the second half to arrive adds the first's partial sums and finishes the item
+        if (SPLIT && (cx.split_tag & 1)) {  // the second half to arrive adds the first's partial sums and finishes
             int fin = 0;
-            if (!split_combine(cx, f, gT, warp, lane, xbar, xphase, split_flag, status, fin)) return;
+            if (!split_combine(sys, cx, f, gT, warp, lane, xbar, xphase, split_flag, status, fin)) return;
             if (!fin) continue;
         }
         if (diag) {
@@ -980,35 +986,41 @@ extern "C" int trpdrv_tma_prepare(const trpdrv_dev_system *h_sys, int nsys, void
 
 extern "C" int trpdrv_launch_fused_tma(const trpdrv_dev_system *d_sys, int nsys, int64_t total_items,
                                        unsigned long long *counter, int *status, int grid, const void *maps,
-                                       int mma_k, void *stream)
+                                       int mma_k, int split, void *stream)
 {
     if (grid <= 0 || total_items <= 0) return 0;
     if (g_launch_regs != tma::REG_LAUNCH) return (int)cudaErrorInvalidConfiguration;
     const tma::Maps &m = *static_cast<const tma::Maps *>(maps);
-    if (mma_k == 16)
-        tma::fused_tma_kernel<16><<<grid, tma::NTHREAD, tma::SMEM_BYTES, (cudaStream_t)stream>>>(
-            d_sys, nsys, total_items, counter, status, m);
+    cudaStream_t st = (cudaStream_t)stream;
+    if (split && mma_k == 8)
+        tma::fused_tma_kernel<8, true><<<grid, tma::NTHREAD, tma::SMEM_BYTES, st>>>(d_sys, nsys, total_items,
+                                                                                   counter, status, m);
+    else if (split)
+        return (int)cudaErrorInvalidValue;
+    else if (mma_k == 16)
+        tma::fused_tma_kernel<16, false><<<grid, tma::NTHREAD, tma::SMEM_BYTES, st>>>(d_sys, nsys, total_items,
+                                                                                     counter, status, m);
     else if (mma_k == 8)
-        tma::fused_tma_kernel<8><<<grid, tma::NTHREAD, tma::SMEM_BYTES, (cudaStream_t)stream>>>(
-            d_sys, nsys, total_items, counter, status, m);
+        tma::fused_tma_kernel<8, false><<<grid, tma::NTHREAD, tma::SMEM_BYTES, st>>>(d_sys, nsys, total_items,
+                                                                                    counter, status, m);
     else
         return (int)cudaErrorInvalidValue;
     return (int)cudaGetLastError();
 }
 
-// Both instantiations must be launched with REG_LAUNCH registers per thread (the setmaxnreg split
+// Every instantiation must be launched with REG_LAUNCH registers per thread (the setmaxnreg split
 // assumes it); g_launch_regs holds the common value, or 0 when they differ.
 extern "C" int trpdrv_fused_tma_init(void)
 {
-    cudaFuncAttributes f8, f16;
-    cudaError_t e = cudaFuncGetAttributes(&f8, tma::fused_tma_kernel<8>);
-    if (e == cudaSuccess) e = cudaFuncGetAttributes(&f16, tma::fused_tma_kernel<16>);
+    cudaFuncAttributes a[3];
+    cudaError_t e = cudaFuncGetAttributes(&a[0], tma::fused_tma_kernel<8, false>);
+    if (e == cudaSuccess) e = cudaFuncGetAttributes(&a[1], tma::fused_tma_kernel<16, false>);
+    if (e == cudaSuccess) e = cudaFuncGetAttributes(&a[2], tma::fused_tma_kernel<8, true>);
     if (e != cudaSuccess) return (int)e;
-    g_launch_regs = f8.numRegs == f16.numRegs ? f8.numRegs : 0;
-    e = cudaFuncSetAttribute(tma::fused_tma_kernel<8>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)tma::SMEM_BYTES);
-    if (e == cudaSuccess)
-        e = cudaFuncSetAttribute(tma::fused_tma_kernel<16>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)tma::SMEM_BYTES);
+    g_launch_regs = a[0].numRegs == a[1].numRegs && a[0].numRegs == a[2].numRegs ? a[0].numRegs : 0;
+    const cudaFuncAttribute dyn = cudaFuncAttributeMaxDynamicSharedMemorySize;
+    e = cudaFuncSetAttribute(tma::fused_tma_kernel<8, false>, dyn, (int)tma::SMEM_BYTES);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(tma::fused_tma_kernel<16, false>, dyn, (int)tma::SMEM_BYTES);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(tma::fused_tma_kernel<8, true>, dyn, (int)tma::SMEM_BYTES);
     return (int)e;
 }

@@ -640,7 +640,7 @@ static int enqueue_fused(trpdrv_plan *p, cudaStream_t st, int capturing)
     if (p->total_items > 0) {
         if (p->use_tma)
             LAUNCH_TRY(trpdrv_launch_fused_tma(p->d_dev, p->nsys, p->total_items, p->d_counter, p->d_status,
-                                               p->grid_tma, p->tma_maps, p->tma_mma_k, st));
+                                               p->grid_tma, p->tma_maps, p->tma_mma_k, 0, st));
         else
             LAUNCH_TRY(trpdrv_launch_fused(p->d_dev, p->nsys, p->total_items, p->d_counter, p->d_status, p->grid,
                                            p->vec2, p->opt.mma_k, st));
@@ -1065,7 +1065,7 @@ int trpdrv_plan_upload_execute(trpdrv_plan *p, const trpdrv_system *host, int ch
         const int grid = (int64_t)cap < n ? cap : (int)n;
         if (n <= 0 || rc != TRPDRV_OK) continue;
         int e = p->use_tma ? trpdrv_launch_fused_tma(p->d_dev, p->nsys, sp[c].end, p->d_chunk_first + c, p->d_status,
-                                                     grid, p->tma_maps, p->tma_mma_k, p->stream)
+                                                     grid, p->tma_maps, p->tma_mma_k, 0, p->stream)
                            : trpdrv_launch_fused(p->d_dev, p->nsys, sp[c].end, p->d_chunk_first + c, p->d_status,
                                                  grid, p->vec2, p->opt.mma_k, p->stream);
         if (e) rc = fail(TRPDRV_ERR_CUDA, "fused launch of span %d: %s", c, cudaGetErrorString((cudaError_t)e));
@@ -1334,8 +1334,10 @@ static int tune_elapsed(trpdrv_plan *p, float *ms)
     return TRPDRV_OK;
 }
 
-/* estimated device time of one execution with candidate c: each system timed on a sample (after one
- * untimed run of the same sample) and scaled to its full work */
+/* estimated device time of one execution with candidate c: each system timed on a sample (the best of
+ * TUNE_REPS runs of the same sample, the first of which also warms the caches) and scaled to its full
+ * work; candidates within a few percent of each other need the minimum to be told apart */
+#define TUNE_REPS 3
 static int tune_time(trpdrv_plan *p, const trpdrv_tune_candidate *c, double *est)
 {
     cudaStream_t st = p->stream;
@@ -1352,36 +1354,40 @@ static int tune_time(trpdrv_plan *p, const trpdrv_tune_candidate *c, double *est
             const unsigned long long first = (unsigned long long)d->item_begin;
             int grid = c->staging == 2 ? p->nsm : c->ctas_per_sm * p->nsm;
             if (grid > sample) grid = (int)sample;
-            for (int rep = 0; rep < 2; ++rep) {
+            if (c->staging == 2) TRY(tune_set_edge_pack(p, c->edge_pack));
+            float best = 0.0f;
+            for (int rep = 0; rep < TUNE_REPS; ++rep) {
                 CUDA_TRY(cudaMemcpyAsync(p->d_counter, &first, sizeof first, cudaMemcpyHostToDevice, st));
                 CUDA_TRY(cudaStreamSynchronize(st)); /* `first` is a host stack value */
                 CUDA_TRY(cudaEventRecord(p->ev0, st));
-                if (c->staging == 2) TRY(tune_set_edge_pack(p, c->edge_pack));
                 if (c->staging == 2)
                     LAUNCH_TRY(trpdrv_launch_fused_tma(p->d_dev, p->nsys, d->item_begin + sample, p->d_counter,
-                                                       p->d_status, grid, p->tma_maps, c->mma_k, st));
+                                                       p->d_status, grid, p->tma_maps, c->mma_k, 0, st));
                 else
                     LAUNCH_TRY(trpdrv_launch_fused(p->d_dev, p->nsys, d->item_begin + sample, p->d_counter,
                                                    p->d_status, grid, p->vec2, c->mma_k, st));
                 CUDA_TRY(cudaEventRecord(p->ev1, st));
                 TRY(tune_elapsed(p, &ms));
+                if (rep == 0 || ms < best) best = ms;
             }
-            *est += (double)ms * (double)items / (double)sample;
+            *est += (double)best * (double)items / (double)sample;
         } else {
             const sysbuf *b = &p->s[q];
             /* four launch pairs of the largest batch, so every candidate is timed over several launches */
             const int64_t want = 4 * (int64_t)TUNE_MAX_BATCH;
             const int64_t n = d->ntriples < want ? d->ntriples : want;
             LAUNCH_TRY(trpdrv_launch_oz_slices(d, &b->oz, st));
-            for (int rep = 0; rep < 2; ++rep) {
+            float best = 0.0f;
+            for (int rep = 0; rep < TUNE_REPS; ++rep) {
                 int64_t bi = 0;
                 CUDA_TRY(cudaEventRecord(p->ev0, st));
                 TRY(emulated_batches(p, d, b, 0, n, c->batch, st, &bi, NULL));
                 TRY(emulated_join(p, st, bi));
                 CUDA_TRY(cudaEventRecord(p->ev1, st));
                 TRY(tune_elapsed(p, &ms));
+                if (rep == 0 || ms < best) best = ms;
             }
-            *est += (double)ms * (double)d->ntriples / (double)n;
+            *est += (double)best * (double)d->ntriples / (double)n;
         }
     }
     return TRPDRV_OK;
@@ -2115,7 +2121,7 @@ static int body_fused(int ncor, int nocc, int nvir, int a, int i, int j, int k, 
     const int grid = items < g_dif.nsm ? items : g_dif.nsm;
     LAUNCH_TRY(trpdrv_launch_fused_tma((const trpdrv_dev_system *)g_dif.d_block, 1, items,
                                        (unsigned long long *)(g_dif.d_io + nslot), (int *)(g_dif.d_io + nslot + 1),
-                                       grid, g_dif.maps, 8, st));
+                                       grid, g_dif.maps, 8, 1, st));
     CUDA_TRY(cudaMemcpyAsync(g_dif.h_io, g_dif.d_io, sizeof(double) * (nslot + 2), cudaMemcpyDeviceToHost, st));
     CUDA_TRY(cudaStreamSynchronize(st));
     int status = 0;

@@ -80,7 +80,7 @@ size_t trpdrv_tma_maps_bytes(void);
 int trpdrv_tma_prepare(const trpdrv_dev_system *h_sys, int nsys, void *maps_out);
 int trpdrv_launch_fused_tma(const trpdrv_dev_system *d_sys, int nsys, int64_t total_items,
                             unsigned long long *counter, int *status, int grid, const void *maps,
-                            int mma_k, void *stream);
+                            int mma_k, int split, void *stream);
 int trpdrv_fused_tma_init(void);
 
 /* Emulated-FP64 (Ozaki int8) form, ozaki.cu.  Per system: digit slices of the A operands

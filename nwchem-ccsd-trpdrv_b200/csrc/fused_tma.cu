@@ -728,12 +728,15 @@ fused_tma_kernel(const trpdrv_dev_system *__restrict__ sys, int nsys, long long 
             const int pb0 = pp ? cx.b1 : cx.b0;
             const bool pactive = pb0 >= 0 && cx.c0 + pcs * 8 < cx.nvir;
             const int nsl = 2 * cx.nch, pnV = cx.nV;
+            // per-item values in registers: every field read after a wait would be reloaded from the ring
+            const int inocc = cx.nocc, invir = cx.nvir;
+            const int ich0 = SPLIT ? (cx.split_tag >> 1) & 1 : 0, istep = SPLIT ? (cx.split_tag & 1) + 1 : 1;
             for (int sl = 0; sl < nsl; ++sl) {
                 if (sl > 0 && !mbar_wait(&full[stage], phase, status)) return;
                 const char *st = stages + (size_t)stage * STAGE_BYTES;
-                const int ch = SPLIT ? ((cx.split_tag >> 1) & 1) + (sl >> 1) * ((cx.split_tag & 1) + 1) : sl >> 1;
+                const int ch = ich0 + (sl >> 1) * istep;
                 const bool ph1 = ch >= pnV;
-                const int kval = ph1 ? cx.nocc - (ch - pnV) * DK : cx.nvir - ch * DK;
+                const int kval = ph1 ? inocc - (ch - pnV) * DK : invir - ch * DK;
                 if (pactive) {
                     // m16n8k8 here in both kernels: the packed path's extra fragment registers would
                     // push the k16 kernel's MMA warps past their register budget
@@ -765,16 +768,19 @@ fused_tma_kernel(const trpdrv_dev_system *__restrict__ sys, int nsys, long long 
             continue;
         }
         const int nch = cx.nch, nV = cx.nV;
+        // per-item values in registers: every field read after a wait would be reloaded from the ring
+        const int inocc = cx.nocc, invir = cx.nvir;
+        const int ich0 = SPLIT ? (cx.split_tag >> 1) & 1 : 0, istep = SPLIT ? (cx.split_tag & 1) + 1 : 1;
         const bool active = (cx.b0 + rx0 < cx.nvir) && (cx.c0 + cx0 < cx.nvir);
         const bool diag = cx.diag != 0;
         const int pf = nch > 3 ? nch - 3 : 0;
         for (int c = 0; c < nch; ++c) {
-            const int ch = SPLIT ? ((cx.split_tag >> 1) & 1) + c * ((cx.split_tag & 1) + 1) : c;
+            const int ch = ich0 + c * istep;
             if (c > 0 && !mbar_wait(&full[stage], phase, status)) return;
             const char *st = stages + (size_t)stage * STAGE_BYTES;
             const bool ph1 = ch >= nV;
             // the second k-step of a chunk is skipped when it lies entirely in the zero padding
-            const int kval = ph1 ? cx.nocc - (ch - nV) * DK : cx.nvir - ch * DK;
+            const int kval = ph1 ? inocc - (ch - nV) * DK : invir - ch * DK;
             if (c == pf) prefetch_epilogue(cx, lane);
             if (KS == 16 && active && kval > 8) {
                 // one m16n8k16 per product: the fragments of both k-steps of the chunk side by side

@@ -187,7 +187,7 @@ typedef struct trpdrv_options {
                          16-byte aligned tensors, <= 8 systems), else cp.async; 1 = cp.async; 2 = TMA
                          or fail with TRPDRV_ERR_UNSUPPORTED */
     int slices;       /* EMULATED: base-128 digits per operand element, 4..8; 0 = default (7) */
-    int batch;        /* EMULATED: triples whose f share one device buffer per launch pair; 0 = default (32) */
+    int batch;        /* EMULATED: triples whose f share one device buffer per launch pair; 0 = default (64) */
     int a_count;      /* full (T) sweep: every system covers the virtual indices a .. a + a_count - 1 (1-based,
                          all within the basis).  The a-dependent tensors (trpdrv_tensor_a_dependent: jvv,
                          kvv, dintc, dintx, t1v) then hold a_count consecutive blocks, a-major; the others

@@ -169,7 +169,7 @@ static int pack_triple(int i, int j, int k) { return (i - 1) | ((j - 1) << 10) |
 /* plans                                                                                        */
 /* ------------------------------------------------------------------------------------------ */
 
-#define TUNE_MAX_BATCH 32 /* largest emulated batch the autotuner tries */
+#define TUNE_MAX_BATCH 64 /* largest emulated batch the autotuner tries */
 
 typedef struct sysbuf {
     trpdrv_system shape;
@@ -238,7 +238,7 @@ void trpdrv_options_default(trpdrv_options *opt)
     opt->use_graph = 1;
     opt->mma_k = 8;
     opt->slices = 7;
-    opt->batch = 32;
+    opt->batch = 64;
 }
 
 static void plan_free(trpdrv_plan *p)
@@ -460,7 +460,7 @@ int trpdrv_plan_create(trpdrv_plan **plan, const trpdrv_system *shape, int nsys,
         return fail(TRPDRV_ERR_ARG, "target_digits %d: must be 0..15", o.target_digits);
     if (o.slices == 0) o.slices = 7;
     if (o.mode == TRPDRV_MODE_EMULATED && o.target_digits > 0) o.slices = 8; /* room for any choice */
-    if (o.batch == 0) o.batch = 32;
+    if (o.batch == 0) o.batch = 64;
     if (!trpdrv_oz_slices_supported(o.slices))
         return fail(TRPDRV_ERR_ARG, "slices %d: must be %d..%d", o.slices, TRPDRV_OZ_MIN_SLICES, TRPDRV_OZ_MAX_SLICES);
     if (o.batch < 1 || o.batch > 4096) return fail(TRPDRV_ERR_ARG, "batch %d: must be 1..4096", o.batch);
@@ -1576,7 +1576,7 @@ int trpdrv_plan_autotune(trpdrv_plan *p, trpdrv_tune_result *result)
             if (occ > 1 && n < 8) c[n++] = (trpdrv_tune_candidate){1, 8, 1, 0, 0, 0.0};
         }
     } else {
-        static const int batches[4] = {4, 8, 16, 32};
+        static const int batches[4] = {8, 16, 32, 64};
         for (int k = 0; k < 4; ++k)
             if (batches[k] <= p->fbuf_batch) c[n++] = (trpdrv_tune_candidate){0, 0, 0, batches[k], 0, 0.0};
     }

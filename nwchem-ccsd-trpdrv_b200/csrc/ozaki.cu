@@ -219,9 +219,6 @@ enum { COL_DISCARD = 0, COL_FILL = 1, COL_USE = 2, COL_LASTUSE = 3 };
 #ifndef OZ_DIGIT_EVICT_LAST
 #define OZ_DIGIT_EVICT_LAST 1
 #endif
-#ifndef OZ_F_LOAD_EVICT_FIRST
-#define OZ_F_LOAD_EVICT_FIRST 1
-#endif
 
 __device__ __forceinline__ void mma_i8(unsigned d, unsigned long long a, unsigned long long b, int accumulate,
                                        int col = COL_DISCARD)
@@ -309,21 +306,12 @@ struct TengyItem {
     long long tt;
 };
 
-// Work item = (16-wide tile pair, batch position y after pos0); false for positions past the end of
-// the system.
-__device__ __forceinline__ bool tengy_decode(const trpdrv_dev_system &S, long long pos0, int pairi, int y,
-                                             TengyItem &it)
+// Geometry of work item (16-wide tile pair, batch position y after pos0), from indices alone; false for
+// positions past the end of the system.
+__device__ __forceinline__ bool tengy_geom(const trpdrv_dev_system &S, long long pos0, int pairi, int y,
+                                           TengyItem &it)
 {
-    const long long pos = pos0 + y;  // a position over the records ([a][triple])
-    if (pos >= S.ntriples || S.nt <= 0) return false;
-    it.ai = pos >= S.nt ? (unsigned)pos / (unsigned)S.nt : 0u;  // records < 2^31
-    const long long tpos = pos - (long long)it.ai * S.nt;
-    it.tt = S.order ? (long long)S.order[tpos] : tpos;
-    if (it.tt < 0 || it.tt >= S.nt) return false;
-    const int packed = S.triples[it.tt];
-    it.i = packed & 1023;
-    it.j = (packed >> 10) & 1023;
-    it.k = (packed >> 20) & 1023;
+    if (pos0 + y >= S.ntriples || S.nt <= 0) return false;
     const int nb = (S.nvir + TW - 1) / TW;
     int B = 0, rem = pairi;
     while (B < nb && rem >= nb - B) {
@@ -336,6 +324,27 @@ __device__ __forceinline__ bool tengy_decode(const trpdrv_dev_system &S, long lo
     it.c0 = (B + rem) * TW;
     it.diag = rem == 0;
     return true;
+}
+
+// The item's triple (its record and indices); false for a malformed queue entry.
+__device__ __forceinline__ bool tengy_triple(const trpdrv_dev_system &S, long long pos0, TengyItem &it)
+{
+    const long long pos = pos0 + it.y;  // a position over the records ([a][triple])
+    it.ai = pos >= S.nt ? (unsigned)pos / (unsigned)S.nt : 0u;  // records < 2^31
+    const long long tpos = pos - (long long)it.ai * S.nt;
+    it.tt = S.order ? (long long)S.order[tpos] : tpos;
+    if (it.tt < 0 || it.tt >= S.nt) return false;
+    const int packed = S.triples[it.tt];
+    it.i = packed & 1023;
+    it.j = (packed >> 10) & 1023;
+    it.k = (packed >> 20) & 1023;
+    return true;
+}
+
+__device__ __forceinline__ bool tengy_decode(const trpdrv_dev_system &S, long long pos0, int pairi, int y,
+                                             TengyItem &it)
+{
+    return tengy_geom(S, pos0, pairi, y, it) && tengy_triple(S, pos0, it);
 }
 
 // The vectors and eaijk of an item's triple.
@@ -356,6 +365,22 @@ __device__ __forceinline__ TengyVecs tengy_vecs(const trpdrv_dev_system &S, cons
     // omp/ccsd_trpdrv_omp_cbody.c:126 (a is 1-based, i/j/k here 0-based)
     v.eaijk = S.eorb[S.a - 1 + it.ai] - (S.eorb[S.ncor + it.i] + S.eorb[S.ncor + it.j] + S.eorb[S.ncor + it.k]);
     return v;
+}
+
+// The per-index vectors of an item in shared memory, rows of 16: t1v(i), t1v(k), dintx(i), dintx(k),
+// dintc(i), dintc(k), e_virt at b0 + r (rows 0 .. 6), then the same at c0 + q (rows 7 .. 13); zero
+// past nvir.  Loaded by the CTA while the item's f tiles are in flight.
+constexpr int TVROWS = 14;
+__device__ __forceinline__ void tengy_stage_vecs(const TengyVecs &v, const TengyItem &it, double *vsh, int tid,
+                                                 int nthreads)
+{
+    for (int idx = tid; idx < TVROWS * TW; idx += nthreads) {
+        const int row = idx / TW, x = idx % TW, side = row / 7, kind = row % 7;
+        const int n = (side ? it.c0 : it.b0) + x;
+        const double *src = kind == 0 ? v.t1v1 : kind == 1 ? v.t1v2 : kind == 2 ? v.dintx1 : kind == 3 ? v.dintx2
+                          : kind == 4 ? v.dintc1 : kind == 5 ? v.dintc2 : v.eorb + v.voff;
+        vsh[idx] = n < v.nvir ? __ldg(src + n) : 0.0;
+    }
 }
 
 // The item's four energy slots (e4i, e5i, e4k, e5k).
@@ -829,17 +854,14 @@ __device__ __forceinline__ void tengy_park_cpasync(const TengyParams &P, const T
     __syncthreads();
 }
 
-// Energies of one item from its parked tiles (either layout), summed over the CTA into its slot.
-template <int TNTHREAD, bool TMA>
+// Energies of one item from its tiles parked by cp.async, summed over the CTA into its slot.
+template <int TNTHREAD>
 __device__ __forceinline__ void tengy_finish(const TengyParams &P, const TengyItem &it, const double *park, double *red)
 {
     const int tid = threadIdx.x;
     const TengyVecs v = tengy_vecs(P.sys, it);
     TengySums su = {0.0, 0.0, 0.0, 0.0};
-    if (TMA)
-        tengy_tile_pair_swz16<TNTHREAD>(park, it.b0, it.c0, it.diag, v, tid, su);
-    else
-        tengy_tile_pair_factored<TW>(park, it.b0, it.c0, it.diag, v, tid, TNTHREAD, su);
+    tengy_tile_pair_factored<TW>(park, it.b0, it.c0, it.diag, v, tid, TNTHREAD, su);
     const TengySums tot = block_sum4(su, red);
     if (tid == 0) {  // block_sum4's result is valid in thread 0
         double *out = tengy_slot(P.sys, it);
@@ -872,28 +894,46 @@ oz_tengy_kernel(const __grid_constant__ TengyParams P, int np, int npos)
     const long long items = (long long)np * npos;
     for (long long w = blockIdx.x; w < items; w += gridDim.x) {
         TengyItem it;
-        if (!tengy_decode(P.sys, P.pos0, (int)(w % np), (int)(w / np), it)) continue;  // uniform over the CTA
-        if (TMA) {
+        if (TMA) {  // the tiles' coordinates need no loads: copies first, the triple and vectors meanwhile
+            __shared__ double vsh[TVROWS * TW];
+            if (!tengy_geom(P.sys, P.pos0, (int)(w % np), (int)(w / np), it)) continue;  // uniform over the CTA
             if (threadIdx.x == 0) {
-                // the previous item's reads of the park (generic proxy) precede these writes
                 asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
                 mbar_arrive_expect_tx(tbar, (it.diag ? 1u : 2u) * (unsigned)(TBOX * sizeof(double)));
-                if (OZ_F_LOAD_EVICT_FIRST) {
-                    const unsigned long long pol = policy_evict_first();
-                    tma_load_3d_hint(park, &P.fmap, tbar, it.b0, it.c0, it.y * 8, pol);
-                    if (!it.diag) tma_load_3d_hint(park + TBOX, &P.fmap, tbar, it.c0, it.b0, it.y * 8, pol);
-                } else {
-                    tma_load_3d(park, &P.fmap, tbar, it.b0, it.c0, it.y * 8);
-                    if (!it.diag) tma_load_3d(park + TBOX, &P.fmap, tbar, it.c0, it.b0, it.y * 8);
-                }
+                const unsigned long long pol = policy_evict_first();
+                tma_load_3d_hint(park, &P.fmap, tbar, it.b0, it.c0, it.y * 8, pol);
+                if (!it.diag) tma_load_3d_hint(park + TBOX, &P.fmap, tbar, it.c0, it.b0, it.y * 8, pol);
+            }
+            const bool valid = tengy_triple(P.sys, P.pos0, it);  // the same in every thread
+            TengyVecs v;
+            if (valid) {
+                v = tengy_vecs(P.sys, it);
+                tengy_stage_vecs(v, it, vsh, threadIdx.x, TNTHREAD);
             }
             const bool ok = mbar_wait(tbar, phase, P.status);
             phase ^= 1;
             if (__syncthreads_or(!ok)) return;  // status bit 1 is set
-        } else {
-            tengy_park_cpasync<TNTHREAD>(P, it, park);
+            if (!valid) {
+                __syncthreads();  // the park is free again
+                continue;
+            }
+            TengySums su = {0.0, 0.0, 0.0, 0.0};
+            tengy_tile_pair_swz16_sv<TNTHREAD>(park, vsh, it.b0, it.c0, it.diag, v.nvir, v.eaijk, threadIdx.x, su);
+            const TengySums tot = block_sum4(su, red);
+            if (threadIdx.x == 0) {
+                double *out = tengy_slot(P.sys, it);
+                out[0] = tot.e4i;
+                out[1] = tot.e5i;
+                out[2] = tot.e4k;
+                out[3] = tot.e5k;
+            }
+            __syncthreads();  // the park, the vectors and the reduction scratch are reused by the next item
+            continue;
         }
-        tengy_finish<TNTHREAD, TMA>(P, it, park, red);
+        // cp.async form (odd nvir)
+        if (!tengy_decode(P.sys, P.pos0, (int)(w % np), (int)(w / np), it)) continue;  // uniform over the CTA
+        tengy_park_cpasync<TNTHREAD>(P, it, park);
+        tengy_finish<TNTHREAD>(P, it, park, red);
     }
 }
 

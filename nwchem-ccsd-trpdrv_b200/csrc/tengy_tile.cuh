@@ -117,6 +117,39 @@ __device__ __forceinline__ void tengy_tile_pair_swz16(const double *park, int b0
     }
 }
 
+// tengy_tile_pair_swz16 with the per-index vectors read from a shared table (rows of 16: t1v(i),
+// t1v(k), dintx(i), dintx(k), dintc(i), dintc(k), e_virt at b0 + r, then the same seven at c0 + q).
+template <int NTHREAD>
+__device__ __forceinline__ void tengy_tile_pair_swz16_sv(const double *park, const double *vsh, int b0, int c0,
+                                                         bool diag, int nvir, double eaijk, int tid, TengySums &su)
+{
+    constexpr int PLANE = 16 * 16, BOX = 8 * PLANE, NDIAG = 16 / (NTHREAD / 16);
+    static_assert(NTHREAD % 16 == 0 && NTHREAD <= 256 && 16 % (NTHREAD / 16) == 0, "half-warps walk the 16 diagonals");
+    const int r = tid & 15;
+    const double *vb = vsh, *vc = vsh + 7 * 16;  // row x of a side at [x * 16 + index]
+#pragma unroll
+    for (int k = 0; k < NDIAG; ++k) {
+        const int d = (tid >> 4) + k * (NTHREAD / 16);
+        const int q = (r + d) & 15;
+        if (b0 + r < nvir && c0 + q < nvir) {
+            const double *bcT = park + q * 16 + swz128(r, q);                       // f_x(B + r, C + q)
+            const double *cbT = park + (diag ? 0 : BOX) + r * 16 + swz128(q, r);    // f_x(C + q, B + r)
+            double fbc[8], fcb[8];
+#pragma unroll
+            for (int f = 0; f < 8; ++f) {
+                fbc[f] = bcT[f * PLANE];
+                fcb[f] = cbT[f * PLANE];
+            }
+            const double denom = -1.0 / (vb[6 * 16 + r] + vc[6 * 16 + q] + eaijk);
+            tengy_term_factored(fbc, fcb, denom, vb[0 * 16 + r], vb[1 * 16 + r], vc[2 * 16 + q], vc[3 * 16 + q],
+                                vc[4 * 16 + q], vc[5 * 16 + q], su);
+            if (!diag)
+                tengy_term_factored(fcb, fbc, denom, vc[0 * 16 + q], vc[1 * 16 + q], vb[2 * 16 + r], vb[3 * 16 + r],
+                                    vb[4 * 16 + r], vb[5 * 16 + r], su);
+        }
+    }
+}
+
 __device__ __forceinline__ void tengy_tile_pair(const double *park, int b0, int c0, bool diag,
                                                 const TengyVecs &v, int tid, int nthreads, TengySums &su)
 {

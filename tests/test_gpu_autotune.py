@@ -64,7 +64,7 @@ def test_emulated_autotune_picks_a_batch_and_results_do_not_change(T):
     with T.Plan([s], mode=T.MODE_EMULATED, slices=7) as p:
         p.upload()
         r = p.autotune()
-        assert [c["batch"] for c in r["candidates"]] == [4, 8, 16, 32]
+        assert [c["batch"] for c in r["candidates"]] == [8, 16, 32, 64]
         e4, e5, recs = _energies(p)
     assert np.array_equal(recs[0], rrec[0])  # the batch size changes no arithmetic
 

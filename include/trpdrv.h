@@ -344,7 +344,10 @@ int trpdrv_synth_fill(int tensor, int ncor, int nocc, int nvir, uint64_t seed, i
 #define TRPDRV_NOALLOC_MAX_NOCC 64
 typedef struct trpdrv_body_device_args {
     int ncor, nocc, nvir;
-    int a, i, j, k;  /* 1-based, as in the reference body */
+    int a, i, j, k;  /* 1-based, as in the reference body.  a is accepted over 1 .. ncor + nocc + nvir
+                        like the reference body's (the reference driver itself passes a = 1,
+                        omp/test.c:162); a physical sweep passes virtual indices,
+                        ncor + nocc < a <= ncor + nocc + nvir, which keep every denominator negative */
     const double *eorb;
     const double *tij, *tkj, *tia, *tka, *xia, *xka, *jia, *jka, *kia, *kka;
     const double *jij, *jkj, *kij, *kkj;

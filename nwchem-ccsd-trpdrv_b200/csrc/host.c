@@ -211,7 +211,7 @@ struct trpdrv_plan {
     int tma_mma_k;      /* FP64 MMA shape of the TMA kernel: 8 (m16n8k8) or 16 (m16n8k16) */
     double *d_fbuf;     /* emulated form: f of two batches of triples [2][fbuf_batch][8][nvir][nvir] */
     size_t fbuf_half;   /* doubles in one of the two halves */
-    cudaStream_t aux_stream;          /* emulated form: energies of batch n beside the products of n + 1 */
+    cudaStream_t aux_stream;          /* emulated form: energies of batch n, ordered after its products only */
     cudaEvent_t ev_gemm[2], ev_tengy[2];
     int fbuf_batch;     /* triples d_fbuf holds (>= opt.batch, and room for the autotuner's batches) */
     int tuned_staging;  /* FUSED staging chosen by the autotuner (1 cp.async, 2 TMA), 0 = none */
@@ -712,7 +712,7 @@ static int emulated_join(trpdrv_plan *p, cudaStream_t st, int64_t bi)
 }
 
 /* Emulated form: slice every operand once per execution, then per batch of `batch` triples (in the
- * processing order) one contraction launch writing their f and one energy launch beside the next. */
+ * processing order) one contraction launch writing their f and one energy launch on the second stream. */
 static int enqueue_emulated(trpdrv_plan *p, cudaStream_t st, int capturing)
 {
     int64_t launches = 0, bi = 0;

@@ -113,8 +113,8 @@ int trpdrv_launch_oz_gemm(const trpdrv_dev_system *h_sys, const trpdrv_oz_system
                           int64_t pos0, int npos, double *fbuf, int64_t epos0, int enpos, const double *efbuf,
                           int *status, int grid, void *stream);
 int trpdrv_oz_fused_energy_supported(int nvir);
-/* threads: 256 to run alone, 128 to run beside the contraction kernel (emulated plans overlap the
- * energies of one batch with the next batch's products on a second stream).  Even nvir: the tiles
+/* threads: 128 (what the plans launch) or 256.  Emulated plans launch the energies of one batch on a
+ * second stream, ordered only after that batch's products.  Even nvir: the tiles
  * arrive by TMA (fbuf 16-byte aligned), with a bounded wait that sets *status bit 1 when it runs out;
  * odd nvir (or TRPDRV_OZ_TENGY_TMA=0): cp.async copies. */
 int trpdrv_launch_oz_tengy(const trpdrv_dev_system *h_sys, int64_t pos0, int npos, const double *fbuf,

@@ -294,9 +294,10 @@ constexpr size_t TSMEM_BYTES = (size_t)16 * TW * (TW + 1) * sizeof(double);
 // 128-byte swizzle; both orientations take 32 KB on a 1024-byte boundary.
 constexpr int TBOX = TW * TW * 8;  // doubles of one orientation
 constexpr size_t TSMEM_TMA_BYTES = (size_t)2 * TBOX * sizeof(double) + 1024;
-// 256 threads when the kernel runs alone; 128 (at most 96 registers) to run beside the persistent
-// contraction kernel on the same SMs: 128 x 96 registers and 33-35 KB of shared memory fit in what an
-// oz_gemm_kernel CTA leaves free on its SM.
+// The plans launch 128-thread CTAs (at most 96 registers, five per SM); 256 is the other size the
+// launcher accepts.  The energies of one batch are launched on a second stream after its contraction
+// launch; since the contraction kernel holds every register of its SMs (512 threads x 128), they run
+// on the SMs it has left, between its launches.
 
 
 struct TengyItem {
@@ -1141,7 +1142,7 @@ extern "C" int trpdrv_launch_oz_tengy(const trpdrv_dev_system *h_sys, int64_t po
     P.fbuf = fbuf;
     P.status = status;
     const bool tma = oz::tengy_tma_enabled() && oz::make_map_f64(&P.fmap, fbuf, h_sys->nvir, 8ull * npos) == 0;
-    // one CTA per item: a launch of one CTA per SM beside the contraction kernel (each CTA looping
+    // one CTA per item: a launch of one CTA per SM (each CTA looping
     // over many items) was measured 30 % slower overall, too little memory parallelism per SM
     cudaStream_t st = (cudaStream_t)stream;
     const unsigned grid = (unsigned)items;

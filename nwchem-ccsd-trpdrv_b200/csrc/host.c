@@ -658,12 +658,13 @@ static int enqueue_fused(trpdrv_plan *p, cudaStream_t st, int capturing)
 }
 
 /* Emulated form, positions [pos0, pos1) of one system in batches of `batch`; *bi counts batches over a
- * whole execution (it picks the half of d_fbuf a batch's f goes to).  Default: each batch's contraction
- * launch writes its f into one half, and its energies run on the auxiliary stream (128-thread CTAs)
- * while the next batch's products go to the other half; a half is reused only after the energies that
- * read it.  TRPDRV_OZ_FUSED_ENERGY=1 (even nvir): each contraction launch's energy warps compute the
- * energies of the previous batch, from the half the previous launch (on the same stream) filled, and
- * an energies-only launch closes the system.  Finish with emulated_join. */
+ * whole execution (it picks the half of d_fbuf a batch's f goes to).  Even nvir (the default): each
+ * contraction launch writes its batch's f into one half while its energy warps compute the energies of
+ * the previous batch from the other half, which the previous launch (on the same stream) filled; an
+ * energies-only launch closes the system.  Odd nvir, or TRPDRV_OZ_FUSED_ENERGY=0: each batch's
+ * energies run as a separate launch on the auxiliary stream (128-thread CTAs) while the next batch's
+ * products go to the other half; a half is reused only after the energies that read it.  Finish with
+ * emulated_join. */
 static int emulated_batches(trpdrv_plan *p, const trpdrv_dev_system *d, const sysbuf *b, int64_t pos0, int64_t pos1,
                             int batch, cudaStream_t st, int64_t *bi, int64_t *launches)
 {

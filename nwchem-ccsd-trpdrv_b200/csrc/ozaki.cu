@@ -421,11 +421,12 @@ __device__ __forceinline__ bool eng_bar_or(bool p)
 
 // One unit's energies, by the energy threads (te = 0 .. NENG_THREADS - 1); false if the wait for its
 // tiles ran out (status bit 1 set).
-__device__ __forceinline__ bool fused_unit(const GemmParams &P, int u, double *park, unsigned long long *ubar,
-                                           unsigned &uphase, double *red, int te)
+__device__ __forceinline__ bool fused_unit(const GemmParams &P, int u, double *park, double *vsh,
+                                           unsigned long long *ubar, unsigned &uphase, double *red, int te)
 {
     TengyItem it;
-    if (!tengy_decode(P.sys, P.epos0, u % P.np, u / P.np, it)) return true;  // same outcome in every thread
+    if (!tengy_geom(P.sys, P.epos0, u % P.np, u / P.np, it)) return true;  // same outcome in every thread
+    // the tiles' coordinates need no loads: copies first, the triple and the vectors while they land
     if (te == 0) {
         // this park's previous reads (generic proxy) before the tensor-copy writes
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
@@ -434,12 +435,21 @@ __device__ __forceinline__ bool fused_unit(const GemmParams &P, int u, double *p
         tma_load_3d_hint(park, &P.fmap, ubar, it.b0, it.c0, it.y * 8, pol);
         if (!it.diag) tma_load_3d_hint(park + PARK_BYTES / 16u, &P.fmap, ubar, it.c0, it.b0, it.y * 8, pol);
     }
+    const bool valid = tengy_triple(P.sys, P.epos0, it);  // the same in every thread
+    TengyVecs v;
+    if (valid) {
+        v = tengy_vecs(P.sys, it);
+        tengy_stage_vecs(v, it, vsh, te, NENG_THREADS);
+    }
     const bool ok = mbar_wait(ubar, uphase, P.status);
     uphase ^= 1u;
-    if (eng_bar_or(!ok)) return false;
-    const TengyVecs v = tengy_vecs(P.sys, it);
+    if (eng_bar_or(!ok)) return false;  // also: the vector table is complete
+    if (!valid) {
+        eng_bar();  // the park and the table are free again
+        return true;
+    }
     TengySums su = {0.0, 0.0, 0.0, 0.0};
-    tengy_tile_pair_swz16<NENG_THREADS>(park, it.b0, it.c0, it.diag, v, te, su);
+    tengy_tile_pair_swz16_sv<NENG_THREADS>(park, vsh, it.b0, it.c0, it.diag, v.nvir, v.eaijk, te, su);
     su.e4i = warp_sum(su.e4i);
     su.e5i = warp_sum(su.e5i);
     su.e4k = warp_sum(su.e4k);
@@ -471,9 +481,10 @@ __device__ __forceinline__ void fused_energies(const GemmParams &P, double *park
                                                double *red, int te)
 {
     const unsigned total = (unsigned)P.enpos * (unsigned)P.np;
+    __shared__ double vsh[TVROWS * TW];
     unsigned uphase = 0;
     for (unsigned u = blockIdx.x; u < total; u += gridDim.x)
-        if (!fused_unit(P, (int)u, park, ubar, uphase, red, te)) return;
+        if (!fused_unit(P, (int)u, park, vsh, ubar, uphase, red, te)) return;
 }
 
 // ------------------------------------------------------------------------------------------------
@@ -1026,15 +1037,14 @@ extern "C" int trpdrv_oz_slices_supported(int slices) { return slices >= TRPDRV_
 
 extern "C" int trpdrv_oz_dp(int nocc, int nvir) { return ((nvir + nocc) + 31) / 32 * 32; }
 
-// Energies inside the contraction launch (TRPDRV_OZ_FUSED_ENERGY=1, read at each call): computed by
-// the kernel's energy warps from f still in L2; needs even nvir (the f tiles are read by TMA).  The
-// default is the separate energy launch, measured 4 % (7 slices) to 14 % (5 slices) faster at
-// (40, 300): the energy work costs the same SM issue and FP64 time either way, and inside the
-// contraction kernel it also slows the MMA warp's issue.
+// Energies inside the contraction launch (the default for even nvir: the f tiles are read by TMA): the
+// kernel's energy warps compute the previous batch's energies while the tensor cores run this batch's
+// products; 1.3 % faster than the separate energy launch at (40, 300), 3.4 % at (30, 400), 7 slices.
+// TRPDRV_OZ_FUSED_ENERGY=0 (read at each call) selects the separate launch for every nvir.
 extern "C" int trpdrv_oz_fused_energy_supported(int nvir)
 {
     const char *e = getenv("TRPDRV_OZ_FUSED_ENERGY");
-    const int on = e && e[0] == '1';
+    const int on = !(e && e[0] == '0');
     return on && nvir >= 2 && (nvir & 1) == 0 && oz::tengy_tma_enabled();
 }
 

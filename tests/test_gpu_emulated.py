@@ -111,31 +111,33 @@ def test_target_digits_picks_the_fewest_slices_that_meet_it(T, name, digits):
 
 
 # ------------------------------------------------------------------------------------------------
-# Energies fused into the contraction launch (TRPDRV_OZ_FUSED_ENERGY=1, even nvir): the kernel's energy
-# warps compute each tile pair once every tile of its triple has stored its f.  They walk the same
-# 128-thread diagonals and sum the warps in the same order as the separate energy launch; the two
-# kernels may still contract multiplies and adds into FMAs differently, so the records agree to a
-# few units in the last place (SAME_PATH_RTOL), not bitwise.
+# Energies inside the contraction launch (the default for even nvir): the kernel's energy warps compute
+# the previous batch's tile pairs.  TRPDRV_OZ_FUSED_ENERGY=0 selects the separate energy launch; both
+# walk the same 128-thread diagonals and sum the warps in the same order, but the two kernels may
+# contract multiplies and adds into FMAs differently, so the records agree to a few units in the last
+# place (SAME_PATH_RTOL), not bitwise.
 # ------------------------------------------------------------------------------------------------
 SAME_PATH_RTOL = 1e-13
+
+
 def _even_goldens():
     return [n for n in golden_cases() if load_golden(n)["nvir"] % 2 == 0]
 
 
 @pytest.fixture
 def fused_energy(monkeypatch):
-    monkeypatch.setenv("TRPDRV_OZ_FUSED_ENERGY", "1")
+    monkeypatch.delenv("TRPDRV_OZ_FUSED_ENERGY", raising=False)  # the default
     yield
-    monkeypatch.delenv("TRPDRV_OZ_FUSED_ENERGY")
 
 
 @pytest.mark.parametrize("name", _even_goldens())
 def test_fused_energies_match_reference_golden_and_separate_launch(T, monkeypatch, name):
     g = load_golden(name)
     s = system_from_golden(g)
-    e4, e5, recs, launches = _run(T, [s], nkpass=g["nkpass"], slices=7)
-    monkeypatch.setenv("TRPDRV_OZ_FUSED_ENERGY", "1")
+    monkeypatch.delenv("TRPDRV_OZ_FUSED_ENERGY", raising=False)
     e4f, e5f, recf, launches_f = _run(T, [s], nkpass=g["nkpass"], slices=7)
+    monkeypatch.setenv("TRPDRV_OZ_FUSED_ENERGY", "0")
+    e4, e5, recs, launches = _run(T, [s], nkpass=g["nkpass"], slices=7)
     monkeypatch.delenv("TRPDRV_OZ_FUSED_ENERGY")
     assert launches_f <= launches  # the energies ride in the contraction launches (plus one per system)
     assert_records_close(recf[0], recs[0], rtol=SAME_PATH_RTOL)
@@ -144,6 +146,7 @@ def test_fused_energies_match_reference_golden_and_separate_launch(T, monkeypatc
     assert_records_close(recf[0], g["records"])
     assert_total_close(e4f[0], g["emp4"], what="emp4")
     assert_total_close(e5f[0], g["emp5"], what="emp5")
+    assert_records_close(recs[0], g["records"])  # the separate launch meets the bars too
 
 
 def test_fused_energies_batches_and_shards_recombine(T, fused_energy):
@@ -155,12 +158,13 @@ def test_fused_energies_batches_and_shards_recombine(T, fused_energy):
 
 
 def test_fused_energies_leave_odd_nvir_on_the_separate_launch(T, monkeypatch):
-    """Odd nvir (the f rows are not 16-byte multiples for TMA): the switch falls back to the
-    separate energy launch and the energies are unchanged."""
+    """Odd nvir (the f rows are not 16-byte multiples for TMA): the default runs the separate energy
+    launch, exactly as TRPDRV_OZ_FUSED_ENERGY=0 does."""
     s = T.synth_system(5, 37, seed=49, ncor=1)
+    monkeypatch.delenv("TRPDRV_OZ_FUSED_ENERGY", raising=False)
     base = _run(T, [s], slices=7)
-    monkeypatch.setenv("TRPDRV_OZ_FUSED_ENERGY", "1")
-    fused = _run(T, [s], slices=7)
+    monkeypatch.setenv("TRPDRV_OZ_FUSED_ENERGY", "0")
+    sep = _run(T, [s], slices=7)
     monkeypatch.delenv("TRPDRV_OZ_FUSED_ENERGY")
-    assert fused[3] == base[3]
-    assert np.array_equal(fused[2][0], base[2][0])
+    assert sep[3] == base[3]
+    assert np.array_equal(sep[2][0], base[2][0])

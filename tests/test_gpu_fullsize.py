@@ -80,13 +80,14 @@ def test_c2_emulated_matches_the_reference(T, slices):
 
 
 def test_c2_emulated_with_fused_energies_equals_the_separate_launch(T, monkeypatch):
-    """TRPDRV_OZ_FUSED_ENERGY=1: the energies inside the contraction launch agree with the separate
-    launch's to 1e-13 (the kernels may contract multiplies and adds differently) and with the
-    reference at the usual bars."""
+    """The energies inside the contraction launch (the default) agree with the separate launch's
+    (TRPDRV_OZ_FUSED_ENERGY=0) to 1e-13 (the kernels may contract multiplies and adds differently) and
+    with the reference at the usual bars."""
     g = _load("big_c2_o40_v300")["systems"][0]
     s = _system(T, g)
+    monkeypatch.setenv("TRPDRV_OZ_FUSED_ENERGY", "0")
     e4, e5, recs, _ = _run(T, [s], mode=T.MODE_EMULATED, slices=7)
-    monkeypatch.setenv("TRPDRV_OZ_FUSED_ENERGY", "1")
+    monkeypatch.delenv("TRPDRV_OZ_FUSED_ENERGY")
     e4f, e5f, recf, _ = _run(T, [s], mode=T.MODE_EMULATED, slices=7)
     assert_records_close(np.asarray(recf[0]), np.asarray(recs[0]), rtol=1e-13)
     assert_total_close(e4f[0], e4[0], rtol=1e-13, what="emp4 vs separate launch")

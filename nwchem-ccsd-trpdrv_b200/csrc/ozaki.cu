@@ -170,15 +170,6 @@ __device__ __forceinline__ void tma_load_3d_hint(void *dst, const CUtensorMap *m
         : "memory");
 }
 
-__device__ __forceinline__ void tma_load_3d(void *dst, const CUtensorMap *map, unsigned long long *bar, int x, int y,
-                                            int z)
-{
-    asm volatile(
-        "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4, %5}], [%2];"
-        ::"r"(saddr(dst)), "l"(map), "r"(saddr(bar)), "r"(x), "r"(y), "r"(z)
-        : "memory");
-}
-
 __device__ __forceinline__ void tmem_alloc(unsigned *dst, unsigned ncols)
 {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(saddr(dst)), "r"(ncols)
@@ -210,15 +201,6 @@ __device__ __forceinline__ unsigned long long sdesc_sw64(const void *p)
 // A-operand collector buffer use of one MMA: the first MMA of a run that shares its A tile fills the
 // buffer, the following ones read A from it instead of shared memory, the last one releases it.
 enum { COL_DISCARD = 0, COL_FILL = 1, COL_USE = 2, COL_LASTUSE = 3 };
-#ifndef OZ_COLLECTOR
-#define OZ_COLLECTOR 1
-#endif
-#ifndef OZ_F_STREAMING
-#define OZ_F_STREAMING 1
-#endif
-#ifndef OZ_DIGIT_EVICT_LAST
-#define OZ_DIGIT_EVICT_LAST 1
-#endif
 
 __device__ __forceinline__ void mma_i8(unsigned d, unsigned long long a, unsigned long long b, int accumulate,
                                        int col = COL_DISCARD)
@@ -576,18 +558,13 @@ __global__ void __launch_bounds__(NTHREAD, 1) oz_gemm_kernel(const __grid_consta
                     }
                     mbar_arrive_expect_tx(&full[stage], C::STAGE);
                     char *sA = stages + (size_t)stage * C::STAGE, *sB = sA + S * SLICE_A;
+                    // the digit planes are reused by the tiles and triples that share them: evict_last
 #pragma unroll
                     for (int p = 0; p < S; ++p)
-                        if (OZ_DIGIT_EVICT_LAST)
-                            tma_load_3d_hint(sA + p * SLICE_A, &P.mapA, &full[stage], kc * KC, d.m0, d.planeA * S + p, pol);
-                        else
-                            tma_load_3d(sA + p * SLICE_A, &P.mapA, &full[stage], kc * KC, d.m0, d.planeA * S + p);
+                        tma_load_3d_hint(sA + p * SLICE_A, &P.mapA, &full[stage], kc * KC, d.m0, d.planeA * S + p, pol);
 #pragma unroll
                     for (int q = 0; q < S; ++q)
-                        if (OZ_DIGIT_EVICT_LAST)
-                            tma_load_3d_hint(sB + q * SLICE_B, &P.mapB, &full[stage], kc * KC, d.n0, d.planeB * S + q, pol);
-                        else
-                            tma_load_3d(sB + q * SLICE_B, &P.mapB, &full[stage], kc * KC, d.n0, d.planeB * S + q);
+                        tma_load_3d_hint(sB + q * SLICE_B, &P.mapB, &full[stage], kc * KC, d.n0, d.planeB * S + q, pol);
                     if (++stage == C::STAGES) {
                         stage = 0;
                         phase ^= 1;
@@ -627,7 +604,7 @@ __global__ void __launch_bounds__(NTHREAD, 1) oz_gemm_kernel(const __grid_consta
                                         mma_i8(tmem + (unsigned)((p + q) * BN),
                                                dA + (unsigned long long)(p * (SLICE_A >> 4) + ks * (KSTEP >> 4)),
                                                dB + (unsigned long long)(q * (SLICE_B >> 4) + ks * (KSTEP >> 4)),
-                                               (kg > 0 || p > 0) ? 1 : 0, OZ_COLLECTOR ? collector_op(q, S - p) : COL_DISCARD);
+                                               (kg > 0 || p > 0) ? 1 : 0, collector_op(q, S - p));
                             }
                         }
                         mma_commit(&empty[stage]);  // the stage is free once these MMAs have read it
@@ -705,11 +682,7 @@ __global__ void __launch_bounds__(NTHREAD, 1) oz_gemm_kernel(const __grid_consta
                         const int ch = col >= V ? 1 : 0, cc = col - ch * V;
                         double *dst = fj + (size_t)(rh + 2 * ch) * vv + b + (size_t)cc * V;
                         const double val = acc[c] * sa * __ldg(eb + col);
-                        // evict-first: read once, by a later launch; keeps the digits in L2
-                        if (OZ_F_STREAMING)
-                            __stcs(dst, val);
-                        else
-                            *dst = val;
+                        __stcs(dst, val);  // evict-first: read once, by a later launch; keeps the digits in L2
                     }
                 }
             }

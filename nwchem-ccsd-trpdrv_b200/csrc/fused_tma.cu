@@ -7,7 +7,7 @@
 //
 //  * one producer thread takes work tickets, writes each item's context to a ring in shared memory
 //    and issues, per chunk of DK contraction indices, one or two cp.async.bulk.tensor loads per
-//    panel (no cluster multicast) that complete on the stage's "full" mbarrier;
+//    panel (each CTA loads its own copy) that complete on the stage's "full" mbarrier;
 //  * eight consumer warps wait on "full", run the m16n8k8 DMMAs straight from the staged panels and
 //    release the stage through its "empty" mbarrier; no CTA-wide barrier in the main loop.
 //

@@ -374,6 +374,16 @@ int trpdrv_unregister_host(const void *ptr);
  * call repeatedly. */
 void trpdrv_finalize(void);
 
+/* Failure-detection self-test.  Every mbarrier wait inside the TMA FP64 kernel and the int8
+ * emulated kernel (stage fills, stage releases, accumulator handoffs) gives up after a time limit
+ * (4 s), sets an error bit in the launch's status word and returns, so a stalled pipeline ends as
+ * TRPDRV_ERR_DEVICE instead of a hung device.  This call runs
+ * that same bounded wait on an mbarrier that nothing completes, with the given limit (seconds, in
+ * (0, 10]), on the current device: *status receives the kernel's status word (2 = the wait gave
+ * up, as it must; 4 = it reported a phase that never completed) and *elapsed_seconds how long the
+ * wait lasted.  The device stays usable afterwards.  No counterpart in the reference. */
+int trpdrv_selftest_bounded_wait(double limit_seconds, int *status, double *elapsed_seconds);
+
 #ifdef __cplusplus
 }
 #endif

@@ -140,7 +140,8 @@ __device__ __forceinline__ bool mbar_try_wait(unsigned long long *b, unsigned pa
 // Bounded wait for the phase with the given parity; false (and status bit 1) when it runs out.
 // try_wait itself suspends the warp for a while in hardware; the clock is read only every 256
 // failed polls so that waiting warps take few issue slots from the MMA warps of their scheduler.
-__device__ __forceinline__ bool mbar_wait(unsigned long long *b, unsigned parity, int *status)
+__device__ __forceinline__ bool mbar_wait_for(unsigned long long *b, unsigned parity, int *status,
+                                              unsigned long long limit_ns)
 {
     if (mbar_try_wait(b, parity)) return true;
     const unsigned long long t0 = globaltimer();
@@ -148,11 +149,31 @@ __device__ __forceinline__ bool mbar_wait(unsigned long long *b, unsigned parity
 #pragma unroll 1
         for (int spin = 0; spin < 256; ++spin)
             if (mbar_try_wait(b, parity)) return true;
-        if (globaltimer() - t0 > WAIT_LIMIT_NS) {
+        if (globaltimer() - t0 > limit_ns) {
             atomicOr(status, 2);
             return false;
         }
     }
+}
+
+__device__ __forceinline__ bool mbar_wait(unsigned long long *b, unsigned parity, int *status)
+{
+    return mbar_wait_for(b, parity, status, WAIT_LIMIT_NS);
+}
+
+// Self-test of the bounded waits: one thread waits, with the given limit, on an mbarrier that
+// nothing completes; the wait must give up, set status bit 1 and return (elapsed_ns: how long it took).
+__global__ void bounded_wait_selftest_kernel(unsigned long long limit_ns, int *status,
+                                             unsigned long long *elapsed_ns)
+{
+    __shared__ __align__(8) unsigned long long bar;
+    if (threadIdx.x != 0) return;
+    mbar_init(&bar, 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    const unsigned long long t0 = globaltimer();
+    const bool completed = mbar_wait_for(&bar, 0u, status, limit_ns);
+    *elapsed_ns = globaltimer() - t0;
+    if (completed) atomicOr(status, 4);  // a phase nothing arrived on reported complete
 }
 
 __device__ __forceinline__ void tma_load_3d(void *dst, const CUtensorMap *map, unsigned long long *bar, int x, int y,
@@ -1011,6 +1032,13 @@ extern "C" int trpdrv_launch_fused_tma(const trpdrv_dev_system *d_sys, int nsys,
                                                                                     counter, status, m);
     else
         return (int)cudaErrorInvalidValue;
+    return (int)cudaGetLastError();
+}
+
+extern "C" int trpdrv_launch_wait_selftest(unsigned long long limit_ns, int *status, unsigned long long *elapsed_ns,
+                                           void *stream)
+{
+    tma::bounded_wait_selftest_kernel<<<1, 32, 0, (cudaStream_t)stream>>>(limit_ns, status, elapsed_ns);
     return (int)cudaGetLastError();
 }
 

@@ -1783,6 +1783,32 @@ int trpdrv_unregister_host(const void *ptr)
     return rc;
 }
 
+int trpdrv_selftest_bounded_wait(double limit_seconds, int *status, double *elapsed_seconds)
+{
+    if (!status || !elapsed_seconds) return fail(TRPDRV_ERR_ARG, "selftest: NULL output pointer");
+    if (!(limit_seconds > 0.0 && limit_seconds <= 10.0))
+        return fail(TRPDRV_ERR_ARG, "selftest: limit %g s outside (0, 10]", limit_seconds);
+    int dev = 0;
+    TRY(ensure_device(-1, &dev, NULL));
+    int *d_status = NULL;
+    unsigned long long *d_el = NULL, el = 0;
+    int h_status = 0;
+    cudaError_t e = cudaMalloc((void **)&d_status, sizeof(int));
+    if (e == cudaSuccess) e = cudaMalloc((void **)&d_el, sizeof(unsigned long long));
+    if (e == cudaSuccess) e = cudaMemset(d_status, 0, sizeof(int));
+    if (e == cudaSuccess)
+        e = (cudaError_t)trpdrv_launch_wait_selftest((unsigned long long)(limit_seconds * 1e9), d_status, d_el, NULL);
+    if (e == cudaSuccess) e = cudaDeviceSynchronize();
+    if (e == cudaSuccess) e = cudaMemcpy(&h_status, d_status, sizeof(int), cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess) e = cudaMemcpy(&el, d_el, sizeof el, cudaMemcpyDeviceToHost);
+    if (d_status) cudaFree(d_status);
+    if (d_el) cudaFree(d_el);
+    if (e != cudaSuccess) return fail(TRPDRV_ERR_CUDA, "selftest: %s", cudaGetErrorString(e));
+    *status = h_status;
+    *elapsed_seconds = (double)el * 1e-9;
+    return TRPDRV_OK;
+}
+
 void trpdrv_finalize(void)
 {
     pthread_mutex_lock(&g_di_mu);

@@ -82,6 +82,11 @@ int trpdrv_launch_fused_tma(const trpdrv_dev_system *d_sys, int nsys, int64_t to
                             unsigned long long *counter, int *status, int grid, const void *maps,
                             int mma_k, int split, void *stream);
 int trpdrv_fused_tma_init(void);
+/* One thread waits, with the production bounded wait and the given limit, on an mbarrier that
+ * nothing completes: sets bit 1 of *status when the wait gives up (bit 2 if it wrongly completes)
+ * and stores how long it waited. */
+int trpdrv_launch_wait_selftest(unsigned long long limit_ns, int *status, unsigned long long *elapsed_ns,
+                                void *stream);
 
 /* Emulated-FP64 (Ozaki int8) form, ozaki.cu.  Per system: digit slices of the A operands
  * sa [nocc][slices][2 nvir][dp] and of the B operands sb [nocc*nocc][slices][2 nvir][dp] (int8,

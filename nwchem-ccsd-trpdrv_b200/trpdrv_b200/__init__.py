@@ -131,6 +131,7 @@ _proto("trpdrv_finalize", None, [])
 _proto("trpdrv_register_host", C.c_int, [C.c_void_p, C.c_size_t])
 _proto("trpdrv_refresh_host", C.c_int, [C.c_void_p])
 _proto("trpdrv_unregister_host", C.c_int, [C.c_void_p])
+_proto("trpdrv_selftest_bounded_wait", C.c_int, [C.c_double, _ip, _dp])
 _body_args = [_dp] * 9 + [_ip] * 3 + [_dp] * 2 + [_ip] * 5 + [_dp] * 20
 for _n in ("ccsd_trpdrv_omp_cbody_", "ccsd_trpdrv_omp_fbody_", "ccsd_trpdrv_cbody_", "ccsd_trpdrv_opencl_"):
     _proto(_n, None, _body_args)
@@ -357,6 +358,14 @@ def refresh_host(arr: np.ndarray):
 
 def unregister_host(arr: np.ndarray):
     _check(lib.trpdrv_unregister_host(C.c_void_p(arr.ctypes.data)))
+
+
+def selftest_bounded_wait(limit_seconds: float = 0.05) -> tuple[int, float]:
+    """trpdrv_selftest_bounded_wait: runs the kernels' bounded mbarrier wait on a barrier that nothing
+    completes; returns (status word, seconds waited).  A correct wait gives up: status 2."""
+    st, el = C.c_int(0), C.c_double(0.0)
+    _check(lib.trpdrv_selftest_bounded_wait(float(limit_seconds), C.byref(st), C.byref(el)))
+    return st.value, el.value
 
 
 def register_system(s: "System"):

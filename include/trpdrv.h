@@ -187,7 +187,8 @@ typedef struct trpdrv_options {
                          16-byte aligned tensors, <= 8 systems), else cp.async; 1 = cp.async; 2 = TMA
                          or fail with TRPDRV_ERR_UNSUPPORTED */
     int slices;       /* EMULATED: base-128 digits per operand element, 4..8; 0 = default (7) */
-    int batch;        /* EMULATED: triples whose f share one device buffer per launch pair; 0 = default (64) */
+    int batch;        /* EMULATED: triples per contraction launch (their f fill one half of a double
+                         buffer that the energy stage reads back); 0 = default (64) */
     int a_count;      /* full (T) sweep: every system covers the virtual indices a .. a + a_count - 1 (1-based,
                          all within the basis).  The a-dependent tensors (trpdrv_tensor_a_dependent: jvv,
                          kvv, dintc, dintx, t1v) then hold a_count consecutive blocks, a-major; the others
@@ -246,7 +247,7 @@ int trpdrv_plan_destroy(trpdrv_plan *plan);
 /* Autotuner: times every compiled variant of the plan's mode on a sample of the plan's own work and
  * keeps the fastest (FUSED: TMA vs cp.async staging, FP64 MMA shape (TMA m16n8k8 / m16n8k16, cp.async
  * m16n8k8 / m16n8k4), edge tile shape (TMA: packed 2 x 32x16 or 32x32 items), CTAs per SM;
- * EMULATED: triples per launch pair, 4 / 8 / 16 / 32).  Needs a bound plan (after upload or bind); each
+ * EMULATED: triples per launch, 8 / 16 / 32 / 64).  Needs a bound plan (after upload or bind); each
  * system is sampled (about 1/8 of its fused items, 64 triples in the emulated form) and the per-
  * system times are scaled to its full work.  EMULATED plans with target_digits first pick the fewest
  * slices (4..8) that meet the accuracy target on the same sample.  The choice is cached per device and set of shapes for
@@ -259,7 +260,7 @@ typedef struct trpdrv_tune_candidate {
     int staging;          /* FUSED: 1 cp.async, 2 TMA; 0 otherwise */
     int mma_k;            /* FUSED: FP64 MMA shape k (TMA: 8 or 16; cp.async: 4 or 8) */
     int ctas_per_sm;      /* FUSED cp.async grid */
-    int batch;            /* EMULATED: triples per launch pair */
+    int batch;            /* EMULATED: triples per contraction launch */
     int edge_pack;        /* FUSED TMA: 1 = where the last tile holds at most 16 virtual indices, its tile
                              pairs run two to a work item (2 x 32x16 tiles); 0 = one 32x32 pair per item */
     double ms_estimate;   /* estimated device time of one execution with this candidate */

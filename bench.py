@@ -86,6 +86,9 @@ def parse():
     ap.add_argument("--profile", action="store_true",
                     help="the timed plan only (c2/c4: fused FP64; c3: emulated, 7 slices), no probes, e2e, plain "
                          "or CPU legs: the command profiled with ncu")
+    ap.add_argument("--probe-int8", action="store_true",
+                    help="print the tcgen05 int8 issue-probe table (N = 64/128/256; one SM, CTA pair, stage "
+                         "handshake) as one JSON line and exit")
     args = ap.parse_args()
     if args.profile:
         args.no_cpu_baseline = args.no_plain = True
@@ -350,14 +353,48 @@ def probe_fp64_peak(kind, device):
     return out.value
 
 
+def probe_int8_peak(n, device, flags=0):
+    """TOPS of the int8 issue-rate probe (lib/libtrpdrv_probe.so): tcgen05.mma.kind::i8 K=32 with the given
+    N, digit-like shared-memory operands in the emulated form's order; flags 0 = one issuing thread per
+    SM (M=128), 1 = CTA pairs (cta_group::2, M=256), 2 = one SM behind the contraction kernel's two-stage
+    stage handshake."""
+    import ctypes as C
+    lib = C.CDLL(os.path.join(ROOT, "nwchem-ccsd-trpdrv_b200", "lib", "libtrpdrv_probe.so"))
+    lib.trpdrv_probe_int8_rate.argtypes = [C.c_int, C.c_int, C.c_int, C.POINTER(C.c_double)]
+    lib.trpdrv_probe_int8_rate.restype = C.c_int
+    out = C.c_double()
+    rc = lib.trpdrv_probe_int8_rate(device, n, flags, C.byref(out))
+    if rc:
+        raise RuntimeError(f"int8 probe N={n} flags={flags} failed with status {rc}")
+    return out.value
+
+
+def run_int8_probe_table():
+    """--probe-int8: the issue rate of every probe form on GPU 0, with cycles per instruction per SM."""
+    import torch
+    props = torch.cuda.get_device_properties(0)
+    clock_hz = 1.965e9
+    rows = []
+    for flags, form in ((0, "one SM, M=128"), (1, "CTA pair, M=256"), (2, "one SM, M=128, stage handshake")):
+        for n in (64, 128, 256):
+            tops = probe_int8_peak(n, 0, flags)
+            # per SM and instruction: 128 rows x N x 32 multiply-adds, 2 operations each
+            cyc = 2.0 * 128 * n * 32 * props.multi_processor_count / (tops * 1e12) * clock_hz
+            rows.append({"form": form, "n": n, "tops": round(tops, 1), "cycles_per_instruction_at_1965mhz": round(cyc, 1)})
+    print(json.dumps({"int8_issue_probe": rows, "device": props.name, "sms": props.multi_processor_count}), flush=True)
+
+
 def measure_peaks(T, R, skip):
-    """FP64: the library's probes (DMMA m16n8k4/k8/k16, DFMA) and cuBLAS DGEMM 8192^3; int8: cuBLASLt
-    int8 GEMM 8192^3 (torch._int_mm), the denominator of the emulated form's tensor-pipe fraction."""
+    """FP64: the library's probes (DMMA m16n8k4/k8/k16, DFMA) and cuBLAS DGEMM 8192^3.  int8: cuBLASLt int8
+    GEMM 8192^3 (torch._int_mm) and the library's tcgen05 int8 issue probe at N = 64 (the emulated form's
+    instruction) and N = 256; the larger of cuBLASLt and the N = 256 probe is the denominator of the
+    emulated form's tensor-pipe fraction."""
     torch = R.torch
-    probe, cublas_dgemm, int8 = {1: 0.0, 2: 0.0, 3: 0.0, 4: 0.0}, 0.0, None
+    probe, cublas_dgemm, int8, int8_mma = {1: 0.0, 2: 0.0, 3: 0.0, 4: 0.0}, 0.0, None, {}
     if skip:
-        return probe, cublas_dgemm, int8
+        return probe, cublas_dgemm, int8, int8_mma
     probe = {k: probe_fp64_peak(k, R.local) for k in (1, 2, 3, 4)}
+    int8_mma = {n: probe_int8_peak(n, R.local) for n in (64, 256)}
 
     def best_of(fn, flop, reps=3):
         fn()
@@ -379,7 +416,7 @@ def measure_peaks(T, R, skip):
         del ai
     except Exception:
         int8 = None
-    return probe, cublas_dgemm, int8
+    return probe, cublas_dgemm, int8, int8_mma
 
 
 def time_plan(T, R, plan, steps, warmup):
@@ -446,9 +483,11 @@ def emulated_ops_per_triple(nocc, nvir, slices):
     return 2 * (2 * nvir) ** 2 * (nvir + nocc) * 2 * slices * (slices + 1) / 2
 
 
-def emulated_sweep(T, R, systems, ref_e4, ref_e5, steps, warmup, slice_list, int8_peak, fp64_peak=None):
+def emulated_sweep(T, R, systems, ref_e4, ref_e5, steps, warmup, slice_list, int8_peak, fp64_peak=None,
+                   int8_n64=None):
     """The emulated form on the same systems for each slice count: triples/s, FP64-equivalent TFLOP/s,
-    int8 tensor-pipe rate and its error against the native FP64 fused result."""
+    int8 tensor-pipe rate (against the device's int8 peak, and against the issue rate of the N = 64
+    instruction the form uses) and its error against the native FP64 fused result."""
     out = {}
     n_all = R.mult * sum(T.count_triples(s.nocc) for s in systems)  # every rank's triples
     flop = R.mult * sum(T.count_triples(s.nocc) * T.triple_flops(s.nocc, s.nvir) for s in systems)
@@ -465,6 +504,7 @@ def emulated_sweep(T, R, systems, ref_e4, ref_e5, steps, warmup, slice_list, int
         out[str(sl)] = {"value": n_all / sec, "unit": "triples/s", "ms_per_step": 1e3 * sec,
                         "tflops_fp64_equiv": flop / sec / 1e12, "kernel_ms": kms, "gpu_launches": launches,
                         "int8_tops": int8_tops, "int8_frac": (int8_tops / int8_peak) if int8_peak else None,
+                        "int8_frac_of_n64_issue": (int8_tops / int8_n64) if int8_n64 else None,
                         "emp4_rel_err_vs_fp64": r4, "emp5_rel_err_vs_fp64": r5,
                         "fp64_roofline_frac": (flop / sec / 1e12) / fp64_peak if fp64_peak else None,
                         "batch": tune["candidates"][tune["chosen"]]["batch"]}
@@ -723,7 +763,10 @@ def run_b200_arm(args):
     n_all = R.mult * sum(T.count_triples(s.nocc) for s in systems)
     flop_all = R.mult * sum(T.count_triples(s.nocc) * T.triple_flops(s.nocc, s.nvir) for s in systems)
 
-    probe, cublas_dgemm, int8_peak = measure_peaks(T, R, args.profile)
+    probe, cublas_dgemm, int8_cublaslt, int8_mma = measure_peaks(T, R, args.profile)
+    int8_peak = max([v for v in (int8_cublaslt, int8_mma.get(256)) if v] or [0.0]) or None
+    int8_peaks = {"cublaslt_8192": int8_cublaslt, "mma_probe_m128n64": int8_mma.get(64),
+                  "mma_probe_m128n256": int8_mma.get(256)}
     peak = max(max(probe.values()), cublas_dgemm) or 1.0
     fp64_probe = {"dmma_m16n8k4": probe[1], "dmma_m16n8k8": probe[2], "dmma_m16n8k16": probe[3],
                   "dfma": probe[4], "cublas_dgemm_8192": cublas_dgemm}
@@ -778,7 +821,8 @@ def run_b200_arm(args):
             clocks = ClockSampler(R.local)
             clocks.start()
             time.sleep(0.3)
-        emulated = emulated_sweep(T, R, systems, e4, e5, args.steps, args.warmup, SLICES, int8_peak, peak)
+        emulated = emulated_sweep(T, R, systems, e4, e5, args.steps, args.warmup, SLICES, int8_peak, peak,
+                                  int8_mma.get(64))
         if args.workload == "c3":
             ck = clocks.stop()
     emu_e2e_sec = None
@@ -827,16 +871,18 @@ def run_b200_arm(args):
             "tflops_fp64_equiv": flop_all / wsec / 1e12,
             "roofline": {"bound": "tensor", "achieved": emu["int8_tops"] if emu else None, "peak": int8_peak,
                          "unit": "TOPS (int8)", "frac": emu["int8_frac"] if emu else None, "traffic": None,
-                         "peak_source": "cuBLASLt int8 GEMM 8192^3 (torch._int_mm) measured live on this device; "
-                                        "achieved = algorithmic int8 operations of the digit-pair products over the "
-                                        "whole step (slicing, products and FP64 energies)",
+                         "peak_source": "measured live on this device: max of cuBLASLt int8 GEMM 8192^3 "
+                                        "(torch._int_mm) and the tcgen05 int8 issue probe at M=128 N=256 "
+                                        "(lib/libtrpdrv_probe.so); achieved = algorithmic int8 operations of the "
+                                        "digit-pair products over the whole step (slicing, products and FP64 "
+                                        "energies)",
                          "kernel_ms": emu["kernel_ms"] if emu else None},
             "fp64_fused": {"value": n_all / sec, "unit": "triples/s", "ms_per_step": 1e3 * sec,
                            "tflops_fp64_equiv": flop_all / sec / 1e12, "roofline_frac": achieved / peak,
                            "emp4": e4[0], "emp5": e5[0]},
             "speedup_vs_fp64_fused": (value / (n_all / sec)),
             "emulated_slices": emulated,
-            "int8_peak_tops": int8_peak, "fp64_probe_tflops": fp64_probe,
+            "int8_peak_tops": int8_peak, "int8_peaks_tops": int8_peaks, "fp64_probe_tflops": fp64_probe,
             "e2e": {"value": (n_all / emu_e2e_sec) if emu_e2e_sec else None, "unit": "triples/s",
                     "h2d_bytes_per_step": in_bytes, "d2h_bytes_per_step": 16,
                     "path": "trpdrv_plan_upload (pinned host) + trpdrv_plan_execute + trpdrv_plan_energies"},
@@ -890,14 +936,17 @@ def run_b200_arm(args):
                                                         "speedup_vs_fp64_fused": tgt["value"] / value,
                                                         "speedup_vs_plain": (tgt["value"] / R.world / plain["value"])
                                                         if plain else None},
-                                    "int8_peak_tops": int8_peak, "slices": emulated}
+                                    "int8_peak_tops": int8_peak, "int8_peaks_tops": int8_peaks,
+                                    "slices": emulated}
     print(json.dumps(line), flush=True)
     R.close()
 
 
 def main():
     args = parse()
-    if args.impl == "reference":
+    if args.probe_int8:
+        run_int8_probe_table()
+    elif args.impl == "reference":
         run_reference_arm(args)
     else:
         run_b200_arm(args)

@@ -20,7 +20,8 @@ nocc=40, nvir=300 (32,800 triples, 16.06 TFLOP per step), seeded synthetic input
   the same workload's triples; rank 0 only.
   The default line also carries `emulated`: the emulated-FP64 form (Ozaki int8 digit slices on the
   tcgen05 tensor cores, TRPDRV_MODE_EMULATED) on the same inputs for 5..8 slices, with its speedup over
-  the native FP64 fused kernel and its error against it.
+  the native FP64 fused kernel, its error against it and its int8 rate against the device's int8 peak
+  (the larger of cuBLASLt's int8 GEMM and the library's tcgen05 issue probe at N = 256).
 --workload c3: the emulated form at nocc=30, nvir=400 with log-uniform integral magnitudes in
   [1e-6, 1]: `value` = triples/s of the emulated form (7 slices), beside the native FP64 fused kernel
   on the same system and the slice sweep with its errors.
@@ -29,6 +30,8 @@ nocc=40, nvir=300 (32,800 triples, 16.06 TFLOP per step), seeded synthetic input
 --workload c4: six systems of uneven size, (8,80) (12,150) (16,220) (24,310) (32,380) (40,450), in
   one fused FP64 launch: `value` = aggregate triples/s; per-system energies checked against
   single-system plans; compared with one plain FP64 launch pair per triple, serially per system.
+--probe-int8: the tcgen05 int8 issue-probe table (N = 64 / 128 / 256 for one SM, a CTA pair and the
+  contraction kernel's stage handshake) as one JSON line; nothing else runs.
 With torchrun (N > 1) every rank runs the whole workload for its own virtual index a (weak scaling: the
 a loop of the full (T) is what partitions into independent units; `value` counts the triples of all
 ranks), and one NCCL all-reduce of the energies per step sums the ranks' (T) contributions.  With
